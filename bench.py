@@ -1,0 +1,325 @@
+"""Benchmark of the GSpaRC training step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step"): the per-receiver training step of train.py:364-566 on
+the 20,000-Gaussian synthetic scene -- forward render of one 90x360
+spectrum (preprocess, binning, sort, blend), L1 + fused SSIM + confidence
+loss, the full hand-written adjoint, Adam.  Each step uses the next receiver
+of a pool; targets are spectra of a second seeded scene at those receivers.
+Synthetic data (no dataset in the container).
+
+value: steps/s with inputs resident in HBM, per-step CUDA events on the
+compute stream, L2 flushed (256 MiB write) between steps outside the events.
+e2e: the same step through SplatTrainer with the receiver's target spectrum,
+view matrix and position copied from pinned host memory every step and the
+loss read back to the host, inside the timed region.
+N > 1: one process per GPU (torchrun), receivers sharded, Gaussians
+replicated, gradients all-reduced over NCCL every step (weak scaling).
+--impl reference: the CPU restatement of the same step (oracle/) on the
+host, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gsparc-wirelessgaussiansplatting_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, ROOT)
+
+METRIC = "train steps/s & spectra/s on 1 B200: batched BF16 vs plain FP32, ΔSSIM≤1e-3"
+UNIT = "train steps/s"
+P_GAUSS = 20000
+POOL = 16
+WORKLOAD = ("cfg1_train_20k: per-receiver training step (forward+SSIM/L1/confidence loss+adjoint+Adam), "
+            "P=20000 Gaussians uniform in a 10x3x8 m room, 90x360 spectrum, 16x16 tiles, per-Gaussian 3-32-2 "
+            "emission MLP, FP32")
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during a timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.samples.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[1]))
+                mx = float(s[2])
+                for n, v in zip(names, s[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist_setup():
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    group = None
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        group = dist.group.WORLD
+    return world, rank, local, group
+
+
+def run_reference(args):
+    """CPU restatement of the step (oracle/train_step.py), timed on the host."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import numpy as np
+    from gsparc_b200 import scenes
+    from oracle import raster as oraster
+    from oracle.train_step import OracleTrainer
+    sc = scenes.make_scene(P_GAUSS, scenes.SEED_SCENE)
+    tg = scenes.make_scene(P_GAUSS, scenes.SEED_TARGET)
+    rxs = scenes.make_receivers(POOL)
+    tm, ts, tq, to = tg.activated()
+    n_tgt = min(POOL, args.warmup + args.steps)
+    targets = [oraster.render(tm, ts, tq, to, tg.mlp, scenes.view_matrix(rxs[i]), scenes.TX_POS, rxs[i], 90,
+                              360)["out"][0] for i in range(n_tgt)]
+    tr = OracleTrainer(sc)
+    # bounded sample: at most ~150 s of timed CPU work
+    for i in range(min(args.warmup, 1)):
+        tr.step(scenes.view_matrix(rxs[i % n_tgt]), rxs[i % n_tgt], scenes.TX_POS, targets[i % n_tgt])
+    times = []
+    budget = 150.0
+    for i in range(args.steps):
+        j = i % n_tgt
+        t0 = time.perf_counter()
+        tr.step(scenes.view_matrix(rxs[j]), rxs[j], scenes.TX_POS, targets[j])
+        times.append(time.perf_counter() - t0)
+        if sum(times) > budget:
+            break
+    v = len(times) / sum(times)
+    ncores = int(os.environ.get("OMP_NUM_THREADS", "0")) or 1
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": len(times), "warmup": min(args.warmup, 1), "ms_per_step": 1000.0 / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "gaussians": P_GAUSS, "receivers_per_step": 1, "spectrum": "90x360",
+                       "implementation": "CPU restatement of the reference path (oracle/train_step.py, numpy)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": ncores, "kind": "port",
+                             "sample": f"{len(times)} of {args.steps} requested steps (capped at {budget:.0f} s)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from gsparc_b200 import _lib, raster, scenes
+    from gsparc_b200.trainer import SplatTrainer
+
+    world, rank, local, group = _dist_setup()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    sc = scenes.make_scene(P_GAUSS, scenes.SEED_SCENE)
+    tg = scenes.make_scene(P_GAUSS, scenes.SEED_TARGET)
+    rxs = scenes.make_receivers(POOL * world)[rank * POOL:(rank + 1) * POOL]   # receivers sharded over ranks
+    views = scenes.view_matrices(rxs)
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
+    tx = t(scenes.TX_POS)
+    views_d, rxs_d = t(views), t(rxs)
+    tm, ts, tq, to = tg.activated()
+    with torch.no_grad():
+        targets_d, _, _, _ = raster.forward(t(tm), t(tg.mlp), t(to.reshape(-1)), t(ts), t(tq), 90, 360, 1.0,
+                                            views_d, tx, rxs_d)
+    targets_h = targets_d.cpu().pin_memory()
+    views_h = torch.tensor(views).pin_memory()
+    rxs_h = torch.tensor(rxs).pin_memory()
+    trainer = SplatTrainer(sc, device=dev, group=group)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def dev_step(i):
+        j = i % POOL
+        return trainer.step(views_d[j], rxs_d[j], tx, targets_d[j])
+
+    tgt_buf = torch.empty((90, 360), dtype=torch.float32, device=dev)
+    view_buf = torch.empty((4, 4), dtype=torch.float32, device=dev)
+    rx_buf = torch.empty(3, dtype=torch.float32, device=dev)
+    loss_h = torch.empty((), dtype=torch.float32).pin_memory()
+
+    def host_step(i):
+        j = i % POOL
+        tgt_buf.copy_(targets_h[j], non_blocking=True)
+        view_buf.copy_(views_h[j], non_blocking=True)
+        rx_buf.copy_(rxs_h[j], non_blocking=True)
+        loss = trainer.step(view_buf, rx_buf, tx, tgt_buf)
+        loss_h.copy_(loss, non_blocking=True)
+        stream.synchronize()
+        return float(loss_h)
+
+    def timed(fn, steps):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        if group is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for i in range(steps):
+            flush.zero_()                     # L2 flush outside the timed events
+            evs[i][0].record(stream)
+            fn(i)
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        if group is not None:
+            dist.barrier()
+        tot = sum(a.elapsed_time(b) for a, b in evs) / 1000.0
+        tt = torch.tensor([tot], dtype=torch.float64, device=dev)
+        if group is not None:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt)
+
+    for i in range(args.warmup):
+        dev_step(i)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        sec = timed(dev_step, args.steps)
+    value = args.steps * world / sec
+    # end to end through the public API with host buffers
+    for i in range(min(args.warmup, 3)):
+        host_step(i)
+    e2e_sec = timed(host_step, args.steps)
+    e2e = args.steps * world / e2e_sec
+    h2d = (90 * 360 + 16 + 3) * 4
+    # per-kernel device times over a third pass of the same steps
+    with _lib.KernelTimer() as kt:
+        for i in range(args.steps):
+            dev_step(i)
+        torch.cuda.synchronize()
+    ktimes = {k: v for k, v in kt.results().items() if v[1] > 0}
+    launches = sum(c for _, c in ktimes.values())
+    dom = max(ktimes, key=lambda k: ktimes[k][0])
+    dom_ms = ktimes[dom][0] / ktimes[dom][1]
+    # algorithmic bytes per launch of the dominant kernel
+    with torch.no_grad():
+        _, _, _, st = raster.forward(trainer.centre, trainer.emission_mlps(), torch.sigmoid(trainer.opacity_logit),
+                                     torch.exp(trainer.log_scale), torch.nn.functional.normalize(trainer.rotation),
+                                     90, 360, 1.0, views_d[0], tx, rxs_d[0])
+    K = st.num_rendered
+    vis = int((raster.state_views(st)["radii"] > 0).sum())
+    npix = 90 * 360
+    alg = {
+        "blend_backward_kernel": K * 36 + npix * 16 + vis * 40,
+        "blend_forward_kernel": K * 36 + npix * 16,
+        "preprocess_kernel": P_GAUSS * 44 + vis * 776 + P_GAUSS * 44,
+        "segment_sort_kernel": K * 8 + K * 4 + 138 * 8,
+        "scatter_kernel": vis * 20 + K * 8,
+        "emission_backward_kernel": vis * (776 + 12 + 8) + P_GAUSS * 776,
+        "geometry_backward_kernel": vis * (12 + 40 + 24 + 24 + 24) + P_GAUSS * 64,
+        "ssim_forward_kernel": npix * 8 + npix * 16,
+        "ssim_backward_kernel": npix * (8 + 16 + 4),
+    }
+    peak, peak_kind = _peaks()
+    achieved = alg.get(dom, 0) / (dom_ms / 1000.0) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic_per_launch.json")) as f:
+            traffic = json.load(f).get(dom)
+    except Exception:
+        pass
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import raster as oraster
+        from oracle.train_step import OracleTrainer
+        otr = OracleTrainer(sc)
+        tgt0 = targets_d[0].cpu().numpy()
+        t0 = time.perf_counter()
+        otr.step(views[0], rxs[0], scenes.TX_POS, tgt0)
+        dt = time.perf_counter() - t0
+        cpu_base = {"value": 1.0 / dt, "unit": UNIT, "cores": 1, "kind": "port",
+                    "sample": "1 full training step of the same workload (numpy restatement, single thread)"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000.0 * sec / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "gaussians": P_GAUSS, "receivers_per_step": 1,
+                           "spectrum": "90x360", "tiles": "16x16", "instances_K": K,
+                           "l2": "flushed between steps (256 MiB write, outside the timed events)",
+                           "parallelism": f"dp{world} (receivers sharded, gradients all-reduced)"},
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
+                "gpu_launches": launches // args.steps * args.steps,
+                "clocks": clk.summary(),
+                "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                             "avg_launch_ms": dom_ms, "algorithmic_bytes": alg.get(dom)},
+                "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(ktimes.items())},
+                "cpu_baseline": cpu_base}
+        print(json.dumps(line))
+    if group is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,257 @@
+// Binning: per-(receiver, tile) segments sorted by depth.
+//
+// The reference duplicates one (tile << 32 | depth bits, gaussian id) pair per
+// touched tile in Gaussian order and stable-radix-sorts all of them with CUB
+// (rasterizer_impl.cu:102-143, :293-300), then finds tile boundaries
+// (:149-171).  The sorted order it produces is: by tile, then by depth bits,
+// then by Gaussian id (stability over an id-ordered input).
+//
+// Here the tile counts come from the preprocess histogram, so the segment
+// boundaries (= the reference's tile ranges) are known after one scan.  Each
+// instance is scattered straight into its segment as a 64-bit key
+// (depth bits << 32 | gaussian id); the keys are unique, so sorting each
+// segment by that key reproduces the reference order exactly without any
+// stability requirement.  Segments are sorted independently, one CTA each,
+// in shared memory (bitonic network) with a merge-path fallback for segments
+// larger than shared memory.  Traffic is one scatter write plus one read and
+// one write per instance, instead of 5 radix passes over the whole list.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace gsparc {
+
+// ---- scan of per-segment counts -> ranges, cursors, K ----------------------
+// One block; n = R*T segments (a few thousand at most for a spectrum batch).
+__global__ void __launch_bounds__(1024)
+scan_segments_kernel(int n, const uint32_t* __restrict__ counts, uint2* __restrict__ ranges,
+                     uint32_t* __restrict__ cursor, ImageHeader* __restrict__ hdr) {
+  __shared__ unsigned long long warp_tot[32];
+  __shared__ unsigned long long carry;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += 1024 * 4) {
+    // each thread owns 4 consecutive segments of this chunk
+    uint32_t c[4];
+    unsigned long long local = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int i = base + tid * 4 + k;
+      c[k] = i < n ? counts[i] : 0u;
+      local += c[k];
+    }
+    // inclusive warp scan of `local`
+    unsigned long long incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      unsigned long long w = warp_tot[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long v = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += v;
+      }
+      warp_tot[lane] = w;   // inclusive over warps
+    }
+    __syncthreads();
+    unsigned long long start = carry + (wid ? warp_tot[wid - 1] : 0ull) + (incl - local);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int i = base + tid * 4 + k;
+      if (i < n) {
+        // empty tiles keep the reference's zeroed range (rasterizer_impl.cu:303)
+        ranges[i] = c[k] ? make_uint2((uint32_t)start, (uint32_t)(start + c[k])) : make_uint2(0u, 0u);
+        cursor[i] = (uint32_t)start;
+        start += c[k];
+      }
+    }
+    __syncthreads();
+    if (tid == 0) carry += warp_tot[31];
+    __syncthreads();
+  }
+  if (tid == 0) hdr->num_rendered = carry;
+}
+
+// Flags a capacity overflow before any kernel writes into the binning arena.
+__global__ void check_capacity_kernel(ImageHeader* hdr, unsigned long long capacity) {
+  hdr->capacity = capacity;
+  if (hdr->num_rendered > capacity) atomic_or_error(hdr, kErrCapacity);
+}
+
+// ---- scatter instances into their segments ---------------------------------
+// grid (ceil(P/256), R).  Block-aggregated reservation: shared counters per
+// tile, one global atomic per (block, tile), then shared-atomic slots.
+__global__ void __launch_bounds__(256)
+scatter_kernel(int P, TileGrid grid, GeomView geo, uint32_t* __restrict__ cursor,
+               const ImageHeader* __restrict__ hdr, unsigned long long* __restrict__ keys) {
+  if (hdr->error) return;
+  extern __shared__ uint32_t sh[];
+  uint32_t* cnt = sh;
+  uint32_t* base = sh + grid.T;
+  const int r = blockIdx.y;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int t = threadIdx.x; t < grid.T; t += blockDim.x) cnt[t] = 0;
+  __syncthreads();
+  int x0 = 0, y0 = 0, x1 = 0, y1 = 0;
+  bool vis = false;
+  unsigned long long lowkey = 0;
+  if (g < P) {
+    const size_t rg = (size_t)r * P + g;
+    const int rad = geo.radii[rg];
+    if (rad > 0) {
+      vis = true;
+      const float2 xy = geo.means2D[rg];
+      tile_rect(xy.x, xy.y, rad, grid, x0, y0, x1, y1);
+      lowkey = ((unsigned long long)__float_as_uint(geo.depth[rg]) << 32) | (unsigned long long)(uint32_t)g;
+      for (int ty = y0; ty < y1; ++ty)
+        for (int tx = x0; tx < x1; ++tx) atomicAdd(&cnt[ty * grid.gx + tx], 1u);
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < grid.T; t += blockDim.x) {
+    const uint32_t c = cnt[t];
+    base[t] = c ? atomicAdd(&cursor[(size_t)r * grid.T + t], c) : 0u;
+  }
+  __syncthreads();
+  if (vis) {
+    for (int ty = y0; ty < y1; ++ty)
+      for (int tx = x0; tx < x1; ++tx) {
+        const uint32_t pos = atomicAdd(&base[ty * grid.gx + tx], 1u);
+        keys[pos] = lowkey;
+      }
+  }
+}
+
+// ---- per-segment sort -------------------------------------------------------
+constexpr int kSortThreads = 512;
+constexpr int kSortCap = 8192;   // keys per shared-memory sort (64 KB)
+
+__device__ __forceinline__ void bitonic_sort_shared(unsigned long long* s, int npad) {
+  for (int k = 2; k <= npad; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < (npad >> 1); i += blockDim.x) {
+        const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));   // j is a power of two
+        const int hi = lo + j;
+        const bool up = (lo & k) == 0;
+        const unsigned long long a = s[lo], b = s[hi];
+        if ((a > b) == up) { s[lo] = b; s[hi] = a; }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__device__ __forceinline__ int next_pow2(int n) {
+  int p = 1;
+  while (p < n) p <<= 1;
+  return p;
+}
+
+// Merge two sorted runs a[0:na), b[0:nb) into out[0:na+nb) with one CTA
+// (merge path partitioning; keys are unique).
+__device__ void merge_runs_cta(const unsigned long long* __restrict__ a, int na,
+                               const unsigned long long* __restrict__ b, int nb,
+                               unsigned long long* __restrict__ out) {
+  const int total = na + nb;
+  const int per = (total + blockDim.x - 1) / blockDim.x;
+  const int d = min(total, (int)threadIdx.x * per);
+  const int dend = min(total, d + per);
+  int lo = max(0, d - nb), hi = min(d, na);
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] < b[d - mid - 1]) lo = mid + 1;
+    else hi = mid;
+  }
+  int i = lo, j = d - lo;
+  for (int o = d; o < dend; ++o) {
+    const bool take_a = (j >= nb) || (i < na && a[i] < b[j]);
+    out[o] = take_a ? a[i++] : b[j++];
+  }
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+segment_sort_kernel(const uint2* __restrict__ ranges, const ImageHeader* __restrict__ hdr,
+                    unsigned long long* __restrict__ keys, unsigned long long* __restrict__ keys_alt,
+                    uint32_t* __restrict__ point_list) {
+  if (hdr->error) return;
+  extern __shared__ unsigned long long skeys[];
+  const uint2 rg = ranges[blockIdx.x];
+  const int n = (int)(rg.y - rg.x);
+  if (n <= 0) return;
+  unsigned long long* seg = keys + rg.x;
+  if (n == 1) {
+    if (threadIdx.x == 0) point_list[rg.x] = (uint32_t)seg[0];
+    return;
+  }
+  if (n <= kSortCap) {
+    const int npad = next_pow2(n);
+    for (int i = threadIdx.x; i < npad; i += blockDim.x) skeys[i] = i < n ? seg[i] : ~0ull;
+    __syncthreads();
+    bitonic_sort_shared(skeys, npad);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) point_list[rg.x + i] = (uint32_t)skeys[i];
+    return;
+  }
+  // large segment: sort kSortCap-sized chunks in shared memory, then merge
+  // pairs of runs through global memory, ping-ponging keys <-> keys_alt
+  for (int c0 = 0; c0 < n; c0 += kSortCap) {
+    const int cn = min(kSortCap, n - c0);
+    for (int i = threadIdx.x; i < kSortCap; i += blockDim.x) skeys[i] = i < cn ? seg[c0 + i] : ~0ull;
+    __syncthreads();
+    bitonic_sort_shared(skeys, kSortCap);
+    for (int i = threadIdx.x; i < cn; i += blockDim.x) seg[c0 + i] = skeys[i];
+    __syncthreads();
+  }
+  unsigned long long* src = seg;
+  unsigned long long* dst = keys_alt + rg.x;
+  for (int width = kSortCap; width < n; width <<= 1) {
+    for (int lo = 0; lo < n; lo += 2 * width) {
+      const int na = min(width, n - lo);
+      const int nb = max(0, min(width, n - lo - width));
+      merge_runs_cta(src + lo, na, src + lo + na, nb, dst + lo);
+    }
+    __syncthreads();
+    unsigned long long* t = src; src = dst; dst = t;
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) point_list[rg.x + i] = (uint32_t)src[i];
+}
+
+cudaError_t launch_scan_segments(int n, const uint32_t* counts, uint2* ranges, uint32_t* cursor,
+                                 ImageHeader* hdr, cudaStream_t stream) {
+  scan_segments_kernel<<<1, 1024, 0, stream>>>(n, counts, ranges, cursor, hdr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_check_capacity(ImageView img, unsigned long long capacity, cudaStream_t stream) {
+  check_capacity_kernel<<<1, 1, 0, stream>>>(img.hdr, capacity);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(int P, int R, const TileGrid& grid, const GeomView& geo, ImageView img, BinningView bin,
+                           cudaStream_t stream) {
+  if (P == 0 || R == 0) return cudaSuccess;
+  const size_t smem = 2 * (size_t)grid.T * sizeof(uint32_t);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  scatter_kernel<<<dim3((P + 255) / 256, R), 256, smem, stream>>>(P, grid, geo, img.cursor, img.hdr, bin.keys);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_segment_sort(int R, const TileGrid& grid, ImageView img, BinningView bin, cudaStream_t stream) {
+  const size_t sort_smem = (size_t)kSortCap * sizeof(unsigned long long);
+  cudaError_t e = cudaFuncSetAttribute(segment_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem);
+  if (e != cudaSuccess) return e;
+  const int nseg = R * grid.T;
+  if (nseg > 0)
+    segment_sort_kernel<<<nseg, kSortThreads, sort_smem, stream>>>(img.ranges, img.hdr, bin.keys, bin.keys_alt,
+                                                                  bin.point_list);
+  return cudaGetLastError();
+}
+
+}  // namespace gsparc

@@ -1,0 +1,374 @@
+// extern "C" entry points: argument checks, arena carving and launch order.
+//
+// Launch sequence of one forward (all on the caller's stream):
+//   memset(header, counts) -> preprocess(+tile histogram) -> scan   [prepare]
+//   capacity check -> scatter -> segment sort -> blend              [render]
+// and of one backward:
+//   memset(accumulated grads) -> blend adjoint -> geometry adjoint
+//   -> emission-MLP adjoint.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace gsparc;
+
+namespace {
+
+thread_local char g_detail[256] = "";
+
+int cuda_fail(cudaError_t e, const char* where) {
+  std::snprintf(g_detail, sizeof(g_detail), "%s: %s", where, cudaGetErrorString(e));
+  return GSPARC_ERR_CUDA;
+}
+
+int invalid(const char* what) {
+  std::snprintf(g_detail, sizeof(g_detail), "invalid argument: %s", what);
+  return GSPARC_ERR_INVALID;
+}
+
+bool valid_tile(int th, int tw) {
+  return th * tw == kBlendThreads && (th == 8 || th == 16 || th == 32) && (tw == 8 || tw == 16 || tw == 32);
+}
+
+#define GS_CHECK(call, where)                 \
+  do {                                        \
+    cudaError_t e_ = (call);                  \
+    if (e_ != cudaSuccess) return cuda_fail(e_, where); \
+  } while (0)
+
+// ---- optional per-kernel timing (CUDA events around each launch) ----------
+enum KernelId {
+  KID_PREPROCESS, KID_SCAN, KID_CHECK, KID_SCATTER, KID_SEGSORT, KID_BLEND_FWD, KID_BLEND_BWD,
+  KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_COUNT
+};
+const char* const kKernelNames[KID_COUNT] = {
+    "preprocess_kernel", "scan_segments_kernel", "check_capacity_kernel", "scatter_kernel",
+    "segment_sort_kernel", "blend_forward_kernel", "blend_backward_kernel", "geometry_backward_kernel",
+    "emission_backward_kernel", "ssim_forward_kernel", "ssim_backward_kernel", "mark_visible_kernel"};
+
+struct PendingTiming {
+  int id;
+  cudaEvent_t a, b;
+};
+std::mutex g_tmu;
+bool g_timing = false;
+std::vector<PendingTiming> g_pending;
+std::vector<cudaEvent_t> g_event_pool;
+double g_ms[KID_COUNT] = {0};
+long long g_launches[KID_COUNT] = {0};
+
+cudaEvent_t pool_event() {
+  if (!g_event_pool.empty()) {
+    cudaEvent_t e = g_event_pool.back();
+    g_event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Records an event pair around one launch when timing is enabled.
+struct Timed {
+  int id;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr;
+  Timed(int id_, cudaStream_t s_) : id(id_), s(s_) {
+    if (!g_timing) return;
+    std::lock_guard<std::mutex> lk(g_tmu);
+    a = pool_event();
+    cudaEventRecord(a, s);
+  }
+  ~Timed() {
+    if (!a) return;
+    std::lock_guard<std::mutex> lk(g_tmu);
+    cudaEvent_t b = pool_event();
+    cudaEventRecord(b, s);
+    g_pending.push_back({id, a, b});
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int gsparc_abi_version(void) { return 1; }
+
+const char* gsparc_status_string(int status) {
+  switch (status) {
+    case GSPARC_OK: return "ok";
+    case GSPARC_ERR_INVALID: return "invalid argument";
+    case GSPARC_ERR_CUDA: return "CUDA error";
+    case GSPARC_ERR_CAPACITY: return "binning capacity exceeded";
+    case GSPARC_ERR_DEVICE: return "device error word set";
+    default: return "unknown status";
+  }
+}
+
+const char* gsparc_last_error_detail(void) { return g_detail; }
+
+size_t gsparc_geom_state_bytes(int P, int R) {
+  if (P < 0 || R < 0) return 0;
+  return carve_geom(nullptr, (size_t)P, (size_t)R, nullptr);
+}
+
+size_t gsparc_image_state_bytes(int R, int H, int W, int tile_h, int tile_w) {
+  if (R < 0 || H <= 0 || W <= 0 || !valid_tile(tile_h, tile_w)) return 0;
+  TileGrid g(H, W, tile_h, tile_w);
+  return carve_image(nullptr, (size_t)R, (size_t)g.T, (size_t)H * W, nullptr);
+}
+
+size_t gsparc_binning_state_bytes(long long capacity) {
+  if (capacity < 0) return 0;
+  return carve_binning(nullptr, (size_t)capacity, nullptr);
+}
+
+int gsparc_geom_state_layout(int P, int R, size_t* o) {
+  if (P < 0 || R < 0 || !o) return invalid("geom layout");
+  GeomView v;
+  char* base = (char*)(uintptr_t)4096;   // any non-null base; offsets are relative
+  carve_geom(base, (size_t)P, (size_t)R, &v);
+  o[0] = (char*)v.means2D - base; o[1] = (char*)v.depth - base; o[2] = (char*)v.radii - base;
+  o[3] = (char*)v.conic_opacity - base; o[4] = (char*)v.signal - base; o[5] = (char*)v.cov3D - base;
+  return GSPARC_OK;
+}
+
+int gsparc_image_state_layout(int R, int H, int W, int tile_h, int tile_w, size_t* o) {
+  if (R < 0 || H <= 0 || W <= 0 || !valid_tile(tile_h, tile_w) || !o) return invalid("image layout");
+  TileGrid g(H, W, tile_h, tile_w);
+  ImageView v;
+  char* base = (char*)(uintptr_t)4096;
+  carve_image(base, (size_t)R, (size_t)g.T, (size_t)H * W, &v);
+  o[0] = (char*)v.hdr - base; o[1] = (char*)v.ranges - base; o[2] = (char*)v.counts - base;
+  o[3] = (char*)v.cursor - base; o[4] = (char*)v.final_T - base; o[5] = (char*)v.n_contrib - base;
+  return GSPARC_OK;
+}
+
+int gsparc_binning_state_layout(long long capacity, size_t* o) {
+  if (capacity < 0 || !o) return invalid("binning layout");
+  BinningView v;
+  char* base = (char*)(uintptr_t)4096;
+  carve_binning(base, (size_t)capacity, &v);
+  o[0] = (char*)v.keys - base; o[1] = (char*)v.keys_alt - base; o[2] = (char*)v.point_list - base;
+  return GSPARC_OK;
+}
+
+int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w, float scale_modifier,
+                             const float* means3D, const float* emission_mlps, const float* opacities,
+                             const float* scales, const float* rotations, const float* viewmatrices,
+                             const float* tx_pos, const float* rx_pos, int* radii_out, void* geom_state,
+                             void* image_state, long long* num_rendered, void* stream) {
+  if (P < 0 || R < 1 || H <= 0 || W <= 0) return invalid("sizes (need P >= 0, R >= 1, H, W > 0)");
+  if (!valid_tile(tile_h, tile_w)) return invalid("tile shape must be 16x16, 8x32 or 32x8");
+  if (!image_state || !viewmatrices || !tx_pos || !rx_pos) return invalid("null state or receiver pointer");
+  if (P > 0 && (!geom_state || !means3D || !emission_mlps || !opacities || !scales || !rotations))
+    return invalid("null Gaussian pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  TileGrid grid(H, W, tile_h, tile_w);
+  GeomView geo{};
+  if (geom_state) carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
+  ImageView img;
+  carve_image((char*)image_state, (size_t)R, (size_t)grid.T, (size_t)H * W, &img);
+  GS_CHECK(cudaMemsetAsync(img.hdr, 0, sizeof(ImageHeader), s), "memset header");
+  GS_CHECK(cudaMemsetAsync(img.counts, 0, (size_t)R * grid.T * sizeof(uint32_t), s), "memset counts");
+  {
+    Timed t(KID_PREPROCESS, s);
+    GS_CHECK(launch_preprocess(P, R, H, W, grid, scale_modifier, means3D, emission_mlps, opacities, scales,
+                               rotations, viewmatrices, tx_pos, rx_pos, geo, radii_out, img.counts, s),
+             "preprocess");
+  }
+  {
+    Timed t(KID_SCAN, s);
+    GS_CHECK(launch_scan_segments(R * grid.T, img.counts, img.ranges, img.cursor, img.hdr, s), "scan");
+  }
+  if (num_rendered) {
+    unsigned long long k = 0;
+    GS_CHECK(cudaMemcpyAsync(&k, &img.hdr->num_rendered, sizeof(k), cudaMemcpyDeviceToHost, s), "read K");
+    GS_CHECK(cudaStreamSynchronize(s), "sync K");
+    *num_rendered = (long long)k;
+  }
+  return GSPARC_OK;
+}
+
+int gsparc_rasterize_render(int P, int R, int H, int W, int tile_h, int tile_w, const void* geom_state,
+                            void* image_state, void* binning_state, long long capacity, float* out_real,
+                            float* out_imag, void* stream) {
+  if (P < 0 || R < 1 || H <= 0 || W <= 0 || capacity < 0) return invalid("sizes");
+  if (!valid_tile(tile_h, tile_w)) return invalid("tile shape must be 16x16, 8x32 or 32x8");
+  if (!image_state || !out_real || !out_imag) return invalid("null image state or output");
+  if (capacity > 0 && !binning_state) return invalid("null binning state");
+  if (P > 0 && !geom_state) return invalid("null geometry state");
+  cudaStream_t s = (cudaStream_t)stream;
+  TileGrid grid(H, W, tile_h, tile_w);
+  GeomView geo{};
+  if (geom_state) carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
+  ImageView img;
+  carve_image((char*)image_state, (size_t)R, (size_t)grid.T, (size_t)H * W, &img);
+  BinningView bin{};
+  carve_binning((char*)binning_state, (size_t)capacity, &bin);
+  {
+    Timed t(KID_CHECK, s);
+    GS_CHECK(launch_check_capacity(img, (unsigned long long)capacity, s), "capacity check");
+  }
+  {
+    Timed t(KID_SCATTER, s);
+    GS_CHECK(launch_scatter(P, R, grid, geo, img, bin, s), "scatter");
+  }
+  {
+    Timed t(KID_SEGSORT, s);
+    GS_CHECK(launch_segment_sort(R, grid, img, bin, s), "segment sort");
+  }
+  {
+    Timed t(KID_BLEND_FWD, s);
+    GS_CHECK(launch_blend_forward(P, R, H, W, grid, geo, img, bin, out_real, out_imag, s), "blend forward");
+  }
+  return GSPARC_OK;
+}
+
+int gsparc_read_status(const void* image_state, long long* num_rendered, unsigned int* error_word, void* stream) {
+  if (!image_state) return invalid("null image state");
+  cudaStream_t s = (cudaStream_t)stream;
+  ImageHeader h;
+  GS_CHECK(cudaMemcpyAsync(&h, image_state, 16, cudaMemcpyDeviceToHost, s), "read header");
+  GS_CHECK(cudaStreamSynchronize(s), "sync header");
+  if (num_rendered) *num_rendered = (long long)h.num_rendered;
+  if (error_word) *error_word = h.error;
+  if (h.error & kErrCapacity) return GSPARC_ERR_CAPACITY;
+  if (h.error) return GSPARC_ERR_DEVICE;
+  return GSPARC_OK;
+}
+
+int gsparc_rasterize_backward(int P, int R, int H, int W, int tile_h, int tile_w, float scale_modifier,
+                              unsigned int grad_mode, const float* means3D, const float* emission_mlps,
+                              const float* scales, const float* rotations, const float* viewmatrices,
+                              const float* tx_pos, const float* rx_pos, const void* geom_state,
+                              const void* image_state, const void* binning_state, long long binning_capacity,
+                              const float* dL_dout_real, const float* dL_dout_imag, float* dL_dmeans2D,
+                              float* dL_dconic, float* dL_dsignal, float* dL_dopacity, float* dL_dmeans3D,
+                              float* dL_dcov3D, float* dL_dscales, float* dL_drotations, float* dL_demission_mlps,
+                              void* stream) {
+  if (P < 0 || R < 1 || H <= 0 || W <= 0 || binning_capacity < 0) return invalid("sizes");
+  if (!valid_tile(tile_h, tile_w)) return invalid("tile shape must be 16x16, 8x32 or 32x8");
+  if (grad_mode != GSPARC_GRAD_REFERENCE && grad_mode != GSPARC_GRAD_EXACT) return invalid("grad_mode");
+  if (!image_state || !dL_dout_real || !dL_dout_imag || !viewmatrices || !tx_pos || !rx_pos)
+    return invalid("null image state, upstream gradient or receiver pointer");
+  if (P == 0) return GSPARC_OK;
+  if (!geom_state || !means3D || !emission_mlps || !scales || !rotations || !dL_dmeans2D || !dL_dconic ||
+      !dL_dsignal || !dL_dopacity || !dL_dmeans3D || !dL_dcov3D || !dL_dscales || !dL_drotations ||
+      !dL_demission_mlps)
+    return invalid("null Gaussian input or gradient output");
+  if (binning_capacity > 0 && !binning_state) return invalid("null binning state");
+  cudaStream_t s = (cudaStream_t)stream;
+  TileGrid grid(H, W, tile_h, tile_w);
+  GeomView geo;
+  carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
+  ImageView img;
+  carve_image((char*)image_state, (size_t)R, (size_t)grid.T, (size_t)H * W, &img);
+  BinningView bin{};
+  carve_binning((char*)binning_state, (size_t)binning_capacity, &bin);
+  const size_t rp = (size_t)R * P;
+  GS_CHECK(cudaMemsetAsync(dL_dmeans2D, 0, rp * 3 * sizeof(float), s), "memset dmeans2D");
+  GS_CHECK(cudaMemsetAsync(dL_dconic, 0, rp * 4 * sizeof(float), s), "memset dconic");
+  GS_CHECK(cudaMemsetAsync(dL_dsignal, 0, rp * 2 * sizeof(float), s), "memset dsignal");
+  GS_CHECK(cudaMemsetAsync(dL_dopacity, 0, (size_t)P * sizeof(float), s), "memset dopacity");
+  {
+    Timed t(KID_BLEND_BWD, s);
+    GS_CHECK(launch_blend_backward(P, R, H, W, grid, grad_mode, geo, img, bin, dL_dout_real, dL_dout_imag,
+                                   dL_dmeans2D, dL_dconic, dL_dsignal, dL_dopacity, s),
+             "blend backward");
+  }
+  {
+    Timed t(KID_GEOM_BWD, s);
+    GS_CHECK(launch_geometry_backward(P, R, H, W, scale_modifier, grad_mode, means3D, scales, rotations,
+                                      viewmatrices, geo, dL_dmeans2D, dL_dconic, dL_dmeans3D, dL_dcov3D, dL_dscales,
+                                      dL_drotations, s),
+             "geometry backward");
+  }
+  {
+    Timed t(KID_MLP_BWD, s);
+    GS_CHECK(launch_emission_backward(P, R, means3D, emission_mlps, tx_pos, rx_pos, geo.radii, dL_dsignal,
+                                      dL_demission_mlps, dL_dmeans3D, s),
+             "emission backward");
+  }
+  return GSPARC_OK;
+}
+
+int gsparc_mark_visible(int P, const float* means3D, const float* viewmatrix, uint8_t* present, void* stream) {
+  if (P < 0) return invalid("P");
+  if (P == 0) return GSPARC_OK;
+  if (!means3D || !viewmatrix || !present) return invalid("null pointer");
+  Timed t(KID_MARK_VISIBLE, (cudaStream_t)stream);
+  GS_CHECK(launch_mark_visible(P, means3D, viewmatrix, present, (cudaStream_t)stream), "mark visible");
+  return GSPARC_OK;
+}
+
+int gsparc_ssim_forward(int B, int CH, int H, int W, float C1, float C2, const float* img1, const float* img2,
+                        float* ssim_map, float* dm_dmu1, float* dm_dsigma1_sq, float* dm_dsigma12, void* stream) {
+  if (B < 0 || CH < 0 || H < 0 || W < 0) return invalid("sizes");
+  if ((size_t)B * CH * H * W == 0) return GSPARC_OK;
+  if (!img1 || !img2 || !ssim_map) return invalid("null image or map");
+  const bool any_d = dm_dmu1 || dm_dsigma1_sq || dm_dsigma12;
+  const bool all_d = dm_dmu1 && dm_dsigma1_sq && dm_dsigma12;
+  if (any_d && !all_d) return invalid("derivative maps must be all NULL or all non-NULL");
+  Timed t(KID_SSIM_FWD, (cudaStream_t)stream);
+  GS_CHECK(launch_ssim_forward(B * CH, H, W, C1, C2, img1, img2, ssim_map, dm_dmu1, dm_dsigma1_sq, dm_dsigma12,
+                               (cudaStream_t)stream),
+           "ssim forward");
+  return GSPARC_OK;
+}
+
+int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float C2, const float* img1, const float* img2,
+                         const float* dL_dmap, const float* dm_dmu1, const float* dm_dsigma1_sq,
+                         const float* dm_dsigma12, float* dL_dimg1, void* stream) {
+  (void)C1;
+  (void)C2;
+  if (B < 0 || CH < 0 || H < 0 || W < 0) return invalid("sizes");
+  if ((size_t)B * CH * H * W == 0) return GSPARC_OK;
+  if (!img1 || !img2 || !dL_dmap || !dm_dmu1 || !dm_dsigma1_sq || !dm_dsigma12 || !dL_dimg1)
+    return invalid("null pointer");
+  Timed t(KID_SSIM_BWD, (cudaStream_t)stream);
+  GS_CHECK(launch_ssim_backward(B * CH, H, W, img1, img2, dL_dmap, dm_dmu1, dm_dsigma1_sq, dm_dsigma12, dL_dimg1,
+                                (cudaStream_t)stream),
+           "ssim backward");
+  return GSPARC_OK;
+}
+
+// ---- per-kernel timing ------------------------------------------------------
+
+int gsparc_timing_enable(int on) {
+  std::lock_guard<std::mutex> lk(g_tmu);
+  g_timing = on != 0;
+  return GSPARC_OK;
+}
+
+int gsparc_timing_kernel_count(void) { return KID_COUNT; }
+
+const char* gsparc_timing_kernel_name(int id) { return (id >= 0 && id < KID_COUNT) ? kKernelNames[id] : ""; }
+
+int gsparc_timing_read(double* total_ms, long long* launches, int n, int reset) {
+  std::lock_guard<std::mutex> lk(g_tmu);
+  for (auto& p : g_pending) {
+    GS_CHECK(cudaEventSynchronize(p.b), "timing sync");
+    float ms = 0.f;
+    GS_CHECK(cudaEventElapsedTime(&ms, p.a, p.b), "timing elapsed");
+    g_ms[p.id] += ms;
+    g_launches[p.id] += 1;
+    g_event_pool.push_back(p.a);
+    g_event_pool.push_back(p.b);
+  }
+  g_pending.clear();
+  for (int i = 0; i < n && i < KID_COUNT; ++i) {
+    if (total_ms) total_ms[i] = g_ms[i];
+    if (launches) launches[i] = g_launches[i];
+  }
+  if (reset) {
+    for (int i = 0; i < KID_COUNT; ++i) { g_ms[i] = 0.0; g_launches[i] = 0; }
+  }
+  return GSPARC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,269 @@
+// Shared device helpers and state layouts for the sm_100a splatting kernels.
+//
+// Layout in HBM (all receiver-major, structure-of-arrays, 256-byte aligned):
+//   geometry state  [R][P]  means2D float2 | depth f32 | radii i32 |
+//                           conic_opacity float4 | signal float2 (real, imag)
+//                   [P]     cov3D 6 x f32 (receiver independent)
+//   image state     header (K, error word) | ranges uint2[R*T] |
+//                   counts u32[R*T] | cursor u32[R*T] |
+//                   final_T f32[R*H*W] | n_contrib u32[R*H*W]
+//   binning state   keys u64[Kcap] | keys_alt u64[Kcap] | point_list u32[Kcap]
+// R = receivers per launch, P = Gaussians, T = tiles per receiver.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/gsparc_b200.h"
+
+namespace gsparc {
+
+// 1/pi and 2/pi: the same decimal constants as glibc's M_1_PIf32 / M_2_PIf32
+// (which the reference uses, auxiliary.h:109-110), rounded to float.
+constexpr float kInvPi = 0.318309886183790671537767526745028724f;
+constexpr float kTwoInvPi = 0.636619772367581343075535053490057448f;
+
+constexpr int kBlendThreads = 256;       // pixels per tile (16x16, 8x32 or 32x8)
+constexpr int kMlpIn = 3;                // emission MLP input: receiver position
+constexpr int kMlpHidden = 32;
+constexpr int kMlpOut = 2;               // (real, imag)
+constexpr int kMlpFloats = kMlpIn * kMlpHidden + kMlpHidden + kMlpOut * kMlpHidden + kMlpOut;
+
+// error word bits (image state header)
+constexpr uint32_t kErrCapacity = 1u << 0;   // K exceeded the binning capacity
+constexpr uint32_t kErrSegment = 1u << 1;    // a tile segment exceeded the sort limit
+
+struct ImageHeader {
+  unsigned long long num_rendered;   // K, written by the scan kernel
+  unsigned int error;                // error bits, OR-ed by kernels
+  unsigned int pad;
+  unsigned long long capacity;       // binning capacity the render was given
+  unsigned long long reserved[29];   // pad to 256 bytes
+};
+static_assert(sizeof(ImageHeader) == 256, "header is one 256-byte block");
+
+__host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct TileGrid {
+  int tile_h, tile_w, gx, gy, T;
+  __host__ __device__ TileGrid(int H, int W, int th, int tw)
+      : tile_h(th), tile_w(tw), gx((W + tw - 1) / tw), gy((H + th - 1) / th), T(gx * gy) {}
+};
+
+struct GeomView {
+  float2* means2D;
+  float* depth;
+  int* radii;
+  float4* conic_opacity;
+  float2* signal;
+  float* cov3D;
+};
+
+struct ImageView {
+  ImageHeader* hdr;
+  uint2* ranges;
+  uint32_t* counts;
+  uint32_t* cursor;
+  float* final_T;
+  uint32_t* n_contrib;
+};
+
+struct BinningView {
+  unsigned long long* keys;
+  unsigned long long* keys_alt;
+  uint32_t* point_list;
+};
+
+// Host/device carving of the three caller-provided arenas.  The sizes are the
+// exact byte counts the gsparc_*_state_bytes() entry points report.
+__host__ __device__ inline size_t carve_geom(char* base, size_t P, size_t R, GeomView* v) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) { char* p = base ? base + off : nullptr; off = align_up(off + bytes, 256); return p; };
+  size_t n = P * R;
+  char* a = take(n * sizeof(float2));
+  char* b = take(n * sizeof(float));
+  char* c = take(n * sizeof(int));
+  char* d = take(n * sizeof(float4));
+  char* e = take(n * sizeof(float2));
+  char* f = take(P * 6 * sizeof(float));
+  if (v) {
+    v->means2D = (float2*)a; v->depth = (float*)b; v->radii = (int*)c;
+    v->conic_opacity = (float4*)d; v->signal = (float2*)e; v->cov3D = (float*)f;
+  }
+  return off;
+}
+
+__host__ __device__ inline size_t carve_image(char* base, size_t R, size_t T, size_t npix, ImageView* v) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) { char* p = base ? base + off : nullptr; off = align_up(off + bytes, 256); return p; };
+  char* h = take(sizeof(ImageHeader));
+  char* a = take(R * T * sizeof(uint2));
+  char* b = take(R * T * sizeof(uint32_t));
+  char* c = take(R * T * sizeof(uint32_t));
+  char* d = take(R * npix * sizeof(float));
+  char* e = take(R * npix * sizeof(uint32_t));
+  if (v) {
+    v->hdr = (ImageHeader*)h; v->ranges = (uint2*)a; v->counts = (uint32_t*)b;
+    v->cursor = (uint32_t*)c; v->final_T = (float*)d; v->n_contrib = (uint32_t*)e;
+  }
+  return off;
+}
+
+__host__ __device__ inline size_t carve_binning(char* base, size_t K, BinningView* v) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) { char* p = base ? base + off : nullptr; off = align_up(off + bytes, 256); return p; };
+  char* a = take(K * sizeof(unsigned long long));
+  char* b = take(K * sizeof(unsigned long long));
+  char* c = take(K * sizeof(uint32_t));
+  if (v) { v->keys = (unsigned long long*)a; v->keys_alt = (unsigned long long*)b; v->point_list = (uint32_t*)c; }
+  return off;
+}
+
+// ---------------------------------------------------------------------------
+// Projection math.  The float expression order of every helper below is kept
+// identical to the reference kernels (cited per function) so the integer
+// outputs that depend on it -- radii, tile rectangles, depth key bits -- come
+// out bit-identical under the same compiler and default -fmad.
+// ---------------------------------------------------------------------------
+
+// world -> receiver frame, matrix stored transposed (auxiliary.h:38-46)
+__device__ __forceinline__ float3 view_point(const float3& p, const float* m) {
+  float3 t = {
+      m[0] * p.x + m[4] * p.y + m[8] * p.z + m[12],
+      m[1] * p.x + m[5] * p.y + m[9] * p.z + m[13],
+      m[2] * p.x + m[6] * p.y + m[10] * p.z + m[14],
+  };
+  return t;
+}
+
+// transpose of the rotation part applied to a vector (auxiliary.h:117-125)
+__device__ __forceinline__ float3 view_vec_T(const float3& v, const float* m) {
+  float3 t = {
+      m[0] * v.x + m[1] * v.y + m[2] * v.z,
+      m[4] * v.x + m[5] * v.y + m[6] * v.z,
+      m[8] * v.x + m[9] * v.y + m[10] * v.z,
+  };
+  return t;
+}
+
+// pixel coordinate of a normalised hemisphere coordinate; evaluated in double
+// because the reference's literals are doubles (auxiliary.h:10-13)
+__device__ __forceinline__ float ndc_to_pixel(float v, int S) {
+  return (float)((((double)v + 1.0) * S - 1.0) * 0.5);
+}
+
+// tile rectangle touched by a footprint of the given radius, clamped to the
+// grid (no azimuth wrap), (auxiliary.h:14-24)
+__device__ __forceinline__ void tile_rect(float px, float py, int radius, const TileGrid& g,
+                                          int& x0, int& y0, int& x1, int& y1) {
+  const float bx = (float)g.tile_w, by = (float)g.tile_h;
+  x0 = min(g.gx, max(0, (int)((px - radius) / bx)));
+  y0 = min(g.gy, max(0, (int)((py - radius) / by)));
+  x1 = min(g.gx, max(0, (int)((px + radius + bx - 1) / bx)));
+  y1 = min(g.gy, max(0, (int)((py + radius + by - 1) / by)));
+}
+
+// small column-major 3x3 matrix with GLM's element convention: c[col][row]
+struct Mat3 {
+  float c[3][3];
+};
+
+// GLM-convention product: (A*B)[j][i] = sum_k A[k][i] * B[j][k], k ascending
+__device__ __forceinline__ Mat3 mat_mul(const Mat3& A, const Mat3& B) {
+  Mat3 o;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      o.c[j][i] = A.c[0][i] * B.c[j][0] + A.c[1][i] * B.c[j][1] + A.c[2][i] * B.c[j][2];
+  return o;
+}
+
+__device__ __forceinline__ Mat3 mat_T(const Mat3& A) {
+  Mat3 o;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) o.c[j][i] = A.c[i][j];
+  return o;
+}
+
+// rotation matrix of a (normalised) quaternion q = (r, x, y, z), columns as
+// the reference's mat3 constructor (forward.cu:131-138)
+__device__ __forceinline__ Mat3 quat_to_rot(const float4 q) {
+  const float r = q.x, x = q.y, y = q.z, z = q.w;
+  Mat3 R;
+  R.c[0][0] = 1.f - 2.f * (y * y + z * z); R.c[0][1] = 2.f * (x * y - r * z); R.c[0][2] = 2.f * (x * z + r * y);
+  R.c[1][0] = 2.f * (x * y + r * z); R.c[1][1] = 1.f - 2.f * (x * x + z * z); R.c[1][2] = 2.f * (y * z - r * x);
+  R.c[2][0] = 2.f * (x * z - r * y); R.c[2][1] = 2.f * (y * z + r * x); R.c[2][2] = 1.f - 2.f * (x * x + y * y);
+  return R;
+}
+
+// M = S * R with S = diag(s) (forward.cu:126-140)
+__device__ __forceinline__ Mat3 scale_rot(const float3 s, const Mat3& R) {
+  Mat3 S;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) S.c[j][i] = 0.0f;
+  S.c[0][0] = s.x; S.c[1][1] = s.y; S.c[2][2] = s.z;
+  return mat_mul(S, R);
+}
+
+// view rotation as the reference builds it from the flat matrix (forward.cu:104-107)
+__device__ __forceinline__ Mat3 view_rot(const float* m) {
+  Mat3 W;
+  W.c[0][0] = m[0]; W.c[0][1] = m[4]; W.c[0][2] = m[8];
+  W.c[1][0] = m[1]; W.c[1][1] = m[5]; W.c[1][2] = m[9];
+  W.c[2][0] = m[2]; W.c[2][1] = m[6]; W.c[2][2] = m[10];
+  return W;
+}
+
+__device__ __forceinline__ Mat3 sym_from6(const float* v) {
+  Mat3 V;
+  V.c[0][0] = v[0]; V.c[0][1] = v[1]; V.c[0][2] = v[2];
+  V.c[1][0] = v[1]; V.c[1][1] = v[3]; V.c[1][2] = v[4];
+  V.c[2][0] = v[2]; V.c[2][1] = v[4]; V.c[2][2] = v[5];
+  return V;
+}
+
+// Equirectangular projection Jacobian rows (forward.cu:82-102).  x_scale is
+// 1 in the forward; the reference backward multiplies the azimuth row by 0.5
+// (backward.cu:172-173), reproduced when the reference-compatible gradient
+// mode is selected.
+struct ProjJac {
+  float J00, J02, J10, J11, J12;
+  float trxztrxz, trxztrxz_inv, trxz, trxz_inv, trtr, trtr_inv, W_div_2pi, H_div_pi;
+};
+
+__device__ __forceinline__ ProjJac proj_jacobian(const float3 t, int width, int height) {
+  ProjJac j;
+  j.trxztrxz = t.x * t.x + t.z * t.z;
+  j.trxztrxz_inv = 1.0f / (j.trxztrxz + 1e-7f);
+  j.trxz = sqrtf(j.trxztrxz);
+  j.trxz_inv = 1.0f / (j.trxz + 1e-7f);
+  j.trtr = j.trxztrxz + t.y * t.y;
+  j.trtr_inv = 1.0f / (j.trtr + 1e-7f);
+  j.W_div_2pi = width * 0.5f * kInvPi;
+  j.H_div_pi = height * kInvPi;
+  j.J00 = j.W_div_2pi * t.z * j.trxztrxz_inv;
+  j.J02 = -j.W_div_2pi * t.x * j.trxztrxz_inv;
+  j.J10 = -j.H_div_pi * t.x * t.y * j.trxz_inv * j.trtr_inv;
+  j.J11 = j.H_div_pi * j.trxz * j.trtr_inv;
+  j.J12 = -j.H_div_pi * t.z * t.y * j.trxz_inv * j.trtr_inv;
+  return j;
+}
+
+__device__ __forceinline__ Mat3 jac_mat(float J00, float J02, float J10, float J11, float J12) {
+  Mat3 J;
+  J.c[0][0] = J00; J.c[0][1] = 0.0f; J.c[0][2] = J02;
+  J.c[1][0] = J10; J.c[1][1] = J11; J.c[1][2] = J12;
+  J.c[2][0] = 0.0f; J.c[2][1] = 0.0f; J.c[2][2] = 0.0f;
+  return J;
+}
+
+__device__ __forceinline__ void atomic_or_error(ImageHeader* hdr, uint32_t bits) {
+  atomicOr(&hdr->error, bits);
+}
+
+}  // namespace gsparc

@@ -1,0 +1,53 @@
+// Host-side launch wrappers shared between the kernel files and the C ABI.
+#pragma once
+
+#include "common.cuh"
+
+namespace gsparc {
+
+cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, float mod, const float* means3D,
+                              const float* mlp, const float* opacities, const float* scales,
+                              const float* rotations, const float* views, const float* tx_pos,
+                              const float* rx_pos, const GeomView& geo, int* radii_out, uint32_t* counts,
+                              cudaStream_t stream);
+
+cudaError_t launch_mark_visible(int P, const float* means3D, const float* view, uint8_t* present,
+                                cudaStream_t stream);
+
+cudaError_t launch_scan_segments(int n, const uint32_t* counts, uint2* ranges, uint32_t* cursor, ImageHeader* hdr,
+                                 cudaStream_t stream);
+
+cudaError_t launch_check_capacity(ImageView img, unsigned long long capacity, cudaStream_t stream);
+
+cudaError_t launch_scatter(int P, int R, const TileGrid& grid, const GeomView& geo, ImageView img, BinningView bin,
+                           cudaStream_t stream);
+
+cudaError_t launch_segment_sort(int R, const TileGrid& grid, ImageView img, BinningView bin, cudaStream_t stream);
+
+cudaError_t launch_blend_forward(int P, int R, int H, int W, const TileGrid& grid, const GeomView& geo,
+                                 const ImageView& img, const BinningView& bin, float* out_real, float* out_imag,
+                                 cudaStream_t stream);
+
+cudaError_t launch_blend_backward(int P, int R, int H, int W, const TileGrid& grid, unsigned grad_mode,
+                                  const GeomView& geo, const ImageView& img, const BinningView& bin,
+                                  const float* dL_dout_real, const float* dL_dout_imag, float* dmean2D,
+                                  float* dconic, float* dsig, float* dopac, cudaStream_t stream);
+
+cudaError_t launch_geometry_backward(int P, int R, int H, int W, float mod, unsigned grad_mode,
+                                     const float* means3D, const float* scales, const float* rotations,
+                                     const float* views, const GeomView& geo, const float* dmean2D,
+                                     const float* dconic, float* dL_dmeans3D, float* dL_dcov3D, float* dL_dscales,
+                                     float* dL_drot, cudaStream_t stream);
+
+cudaError_t launch_emission_backward(int P, int R, const float* means3D, const float* mlp, const float* tx_pos,
+                                     const float* rx_pos, const int* radii, const float* dsig, float* dL_dmlp,
+                                     float* dL_dmeans3D, cudaStream_t stream);
+
+cudaError_t launch_ssim_forward(int planes, int H, int W, float C1, float C2, const float* img1, const float* img2,
+                                float* map, float* dmu1, float* ds11, float* ds12, cudaStream_t stream);
+
+cudaError_t launch_ssim_backward(int planes, int H, int W, const float* img1, const float* img2, const float* dL_dmap,
+                                 const float* dmu1, const float* ds11, const float* ds12, float* dL_dimg1,
+                                 cudaStream_t stream);
+
+}  // namespace gsparc

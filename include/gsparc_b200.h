@@ -1,0 +1,201 @@
+/*
+ * gsparc_b200.h -- C ABI of the sm_100a equirectangular RF splatting path.
+ *
+ * Plain device pointers, sizes and a CUDA stream (passed as void*, i.e. a
+ * cudaStream_t; NULL = the legacy default stream).  No allocation happens
+ * inside any entry point: the caller owns every buffer, including the three
+ * opaque state arenas sized by the *_state_bytes() queries, exactly as the
+ * reference's torch extension owns its geometry / binning / image byte
+ * buffers (cuda_kernel_rasterize/rasterize_points.cu:24-30, :69-74).
+ *
+ * Every entry point returns a gsparc_status code; kernel launches are
+ * asynchronous on the given stream unless stated otherwise.
+ *
+ * Batching: R receivers are rendered per call.  Per-receiver tensors are laid
+ * out receiver-major ([R,3] positions, [R,16] view matrices, [R,H,W] spectra,
+ * [R,P] radii).  R = 1 is the reference's per-receiver call.
+ */
+#ifndef GSPARC_B200_H_
+#define GSPARC_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GSPARC_API __attribute__((visibility("default")))
+#else
+#define GSPARC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gsparc_status {
+  GSPARC_OK = 0,
+  GSPARC_ERR_INVALID = 1,   /* bad size, tile shape or null pointer */
+  GSPARC_ERR_CUDA = 2,      /* a CUDA runtime call or launch failed */
+  GSPARC_ERR_CAPACITY = 3,  /* duplicated instances exceeded the binning capacity */
+  GSPARC_ERR_DEVICE = 4     /* a kernel raised a bit in the device error word */
+} gsparc_status;
+
+/* Gradient modes for gsparc_rasterize_backward. */
+#define GSPARC_GRAD_REFERENCE 0u /* reproduce the reference backward bit-for-bit in
+                                    structure: halved azimuth Jacobian row
+                                    (backward.cu:172-173), real-only alpha
+                                    gradient (backward.cu:577,587) */
+#define GSPARC_GRAD_EXACT 1u     /* true derivative of the forward */
+
+/* Version of this ABI (bumped on any signature change). */
+GSPARC_API int gsparc_abi_version(void);
+
+/* Human-readable text for a status code. */
+GSPARC_API const char* gsparc_status_string(int status);
+
+/* Detail of the last failure on the calling host thread (CUDA error text or
+ * the argument that was rejected).  Not part of the reference interface. */
+GSPARC_API const char* gsparc_last_error_detail(void);
+
+/* ---- arena sizing ------------------------------------------------------- */
+
+/* Geometry arena: per-(receiver, Gaussian) preprocess results and cov3D.
+ * Replaces GeometryState / required<GeometryState> (rasterizer_impl.cu:60-76,
+ * rasterizer_impl.h:44-74). */
+GSPARC_API size_t gsparc_geom_state_bytes(int P, int R);
+
+/* Image arena: K, error word, tile ranges/counts, final T and contributor
+ * counts.  Replaces ImageState (rasterizer_impl.cu:78-85). */
+GSPARC_API size_t gsparc_image_state_bytes(int R, int H, int W, int tile_h, int tile_w);
+
+/* Binning arena for `capacity` duplicated (Gaussian, tile) instances.
+ * Replaces BinningState (rasterizer_impl.cu:87-100). */
+GSPARC_API size_t gsparc_binning_state_bytes(long long capacity);
+
+/* Byte offsets of the sub-arrays inside each arena (for inspection / tests).
+ * geom:    means2D, depth, radii, conic_opacity, signal, cov3D   (6 entries)
+ * image:   header, ranges, counts, cursor, final_T, n_contrib    (6 entries)
+ * binning: keys, keys_alt, point_list                            (3 entries) */
+GSPARC_API int gsparc_geom_state_layout(int P, int R, size_t* offsets6);
+GSPARC_API int gsparc_image_state_layout(int R, int H, int W, int tile_h, int tile_w, size_t* offsets6);
+GSPARC_API int gsparc_binning_state_layout(long long capacity, size_t* offsets3);
+
+/* ---- forward ------------------------------------------------------------ */
+
+/* Stage 1 of the forward: per-(receiver, Gaussian) preprocess (range cull,
+ * equirectangular projection, cov3D, 2D conic, radius, tile rectangle,
+ * per-Gaussian emission MLP, depth), per-tile instance counts, prefix scan and
+ * tile ranges.  Replaces FORWARD::preprocess + cub::DeviceScan::InclusiveSum
+ * + the num_rendered readback of Rasterizer::forward
+ * (rasterizer_impl.cu:227-274; forward.cu:252-327).
+ *
+ * means3D [P,3], emission_mlps [194*P] (layout of EmissionMLPs.get_all_params,
+ * gaussian.py:565-572), opacities [P] (activated), scales [P,3] (activated),
+ * rotations [P,4] (normalised, (w,x,y,z)), viewmatrices [R,16] (transposed
+ * world->receiver, as built by preprocess_data.py:177-202), tx_pos [3],
+ * rx_pos [R,3].  radii_out [R,P] may be NULL.
+ *
+ * When num_rendered is non-NULL, K is copied to the host and the stream is
+ * synchronised (the reference's blocking readback, rasterizer_impl.cu:274);
+ * pass NULL to stay asynchronous (CUDA-graph capture). */
+GSPARC_API int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w,
+                             float scale_modifier, const float* means3D,
+                             const float* emission_mlps, const float* opacities,
+                             const float* scales, const float* rotations,
+                             const float* viewmatrices, const float* tx_pos,
+                             const float* rx_pos, int* radii_out, void* geom_state,
+                             void* image_state, long long* num_rendered, void* stream);
+
+/* Stage 2 of the forward: duplicate instances into per-(receiver, tile)
+ * segments, sort every segment by (depth bits, Gaussian id) -- the order the
+ * reference's stable radix sort on (tile | depth) produces -- and blend each
+ * tile front to back.  Replaces duplicateWithKeys, cub::DeviceRadixSort,
+ * identifyTileRanges and FORWARD::render (rasterizer_impl.cu:276-331,
+ * forward.cu:151-249).  out_real / out_imag are [R,H,W] (one channel).
+ * If K exceeds `capacity` the device error word gets the capacity bit and the
+ * outputs are left unwritten; gsparc_read_status reports it. */
+GSPARC_API int gsparc_rasterize_render(int P, int R, int H, int W, int tile_h, int tile_w,
+                            const void* geom_state, void* image_state, void* binning_state,
+                            long long capacity, float* out_real, float* out_imag,
+                            void* stream);
+
+/* Synchronises the stream and reads K and the device error word of the last
+ * forward that used `image_state`.  Returns GSPARC_ERR_CAPACITY or
+ * GSPARC_ERR_DEVICE when the error word is set. */
+GSPARC_API int gsparc_read_status(const void* image_state, long long* num_rendered,
+                       unsigned int* error_word, void* stream);
+
+/* ---- backward ----------------------------------------------------------- */
+
+/* Full adjoint of the forward.  Replaces Rasterizer::backward
+ * (rasterizer_impl.cu:339-442): reverse-order blend adjoint recomputing T
+ * from the saved final T and contributor count (backward.cu:442-616), conic /
+ * projection / cov3D adjoint (backward.cu:124-371) and the emission-MLP
+ * backward (backward.cu:9-118).
+ *
+ * Inputs as for the forward, plus the arenas of that forward, the binning
+ * capacity the render was given (the reference passes num_rendered,
+ * rasterize_points.cu:124) and dL_dout_real / dL_dout_imag [R,H,W].  Outputs (all overwritten):
+ *   dL_dmeans2D [R,P,3], dL_dconic [R,P,4] (slots x,y,-,w), dL_dsignal [R,P,2],
+ *   dL_dopacity [P] (summed over receivers), dL_dmeans3D [P,3],
+ *   dL_dcov3D [P,6], dL_dscales [P,3], dL_drotations [P,4],
+ *   dL_demission_mlps [194*P].
+ * grad_mode is GSPARC_GRAD_REFERENCE or GSPARC_GRAD_EXACT. */
+GSPARC_API int gsparc_rasterize_backward(int P, int R, int H, int W, int tile_h, int tile_w,
+                              float scale_modifier, unsigned int grad_mode,
+                              const float* means3D, const float* emission_mlps,
+                              const float* scales, const float* rotations,
+                              const float* viewmatrices, const float* tx_pos,
+                              const float* rx_pos, const void* geom_state,
+                              const void* image_state, const void* binning_state,
+                              long long binning_capacity, const float* dL_dout_real, const float* dL_dout_imag,
+                              float* dL_dmeans2D, float* dL_dconic, float* dL_dsignal,
+                              float* dL_dopacity, float* dL_dmeans3D, float* dL_dcov3D,
+                              float* dL_dscales, float* dL_drotations,
+                              float* dL_demission_mlps, void* stream);
+
+/* Range cull only: present[i] = |view * means3D[i]|^2 > 0.04.  Replaces
+ * markVisible / checkFrustum (rasterize_points.cu:203-221,
+ * rasterizer_impl.cu:173-202).  present is [P] bytes (0/1). */
+GSPARC_API int gsparc_mark_visible(int P, const float* means3D, const float* viewmatrix,
+                        uint8_t* present, void* stream);
+
+/* ---- fused SSIM --------------------------------------------------------- */
+
+/* SSIM map with an 11x11 Gaussian window (sigma 1.5), zero "same" padding, and
+ * -- when the three derivative pointers are non-NULL -- the partial
+ * derivatives the backward needs.  Replaces fusedssim / fusedssimCUDA
+ * (fused-ssim/ssim.cu:187-286, :368-404).  Images are [B,CH,H,W] float32. */
+GSPARC_API int gsparc_ssim_forward(int B, int CH, int H, int W, float C1, float C2,
+                        const float* img1, const float* img2, float* ssim_map,
+                        float* dm_dmu1, float* dm_dsigma1_sq, float* dm_dsigma12,
+                        void* stream);
+
+/* dL/dimg1 from dL/dmap and the forward's partial derivatives.  Replaces
+ * fusedssim_backward / fusedssim_backwardCUDA (fused-ssim/ssim.cu:288-366,
+ * :406-444). */
+GSPARC_API int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float C2,
+                         const float* img1, const float* img2, const float* dL_dmap,
+                         const float* dm_dmu1, const float* dm_dsigma1_sq,
+                         const float* dm_dsigma12, float* dL_dimg1, void* stream);
+
+/* ---- per-kernel timing (tracing; no counterpart in the reference, which
+ * only times whole renders with time.time(), train.py:673-677) ------------ */
+
+/* Enable/disable CUDA-event timing around every kernel launch of this
+ * library (off by default; adds two event records per launch). */
+GSPARC_API int gsparc_timing_enable(int on);
+
+/* Number of timed kernel kinds, and the name of kind `id`. */
+GSPARC_API int gsparc_timing_kernel_count(void);
+GSPARC_API const char* gsparc_timing_kernel_name(int id);
+
+/* Waits for the recorded events and returns, per kernel kind, the summed
+ * device milliseconds and the launch count since the last reset (arrays of
+ * n entries, either may be NULL).  reset != 0 clears the totals. */
+GSPARC_API int gsparc_timing_read(double* total_ms, long long* launches, int n, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSPARC_B200_H_ */

@@ -1,0 +1,166 @@
+"""CPU tests of the oracle itself: pinned against the reference's golden
+vectors where they exist, and against its own FP64 finite differences."""
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import fd, raster, ssim as ossim
+from gsparc_b200 import scenes
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _golden_cases():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg
+
+
+@pytest.mark.parametrize("case", ["uniform_90x360", "blobs_90x360", "uniform_b2c3_37x53"])
+def test_ssim_oracle_matches_reference_conv_ssim(case):
+    """Oracle SSIM value and gradient vs the reference's utils.ssim (golden
+    vectors made by tests/golden/make_golden.py).  Tolerance: the reference
+    test's torch.isclose defaults (rtol 1e-5) for the value; rtol 1e-4 plus
+    atol 1e-5 * max|grad| for the per-pixel gradient (FP32 autograd vs FP64
+    oracle)."""
+    mg = _golden_cases()
+    g = np.load(os.path.join(GOLDEN, "ssim_golden.npz"))
+    shape, kind, seed = [(s, k, sd) for (n, s, k, sd) in mg.CASES if n == case][0]
+    a, b = mg.golden_inputs(shape, kind, seed)
+    val = ossim.fused_ssim(a, b)
+    grad = ossim.fused_ssim_grad(a, b)
+    assert np.isclose(val, g[case + "/value"], rtol=1e-5, atol=1e-8)
+    gg = g[case + "/grad"]
+    np.testing.assert_allclose(grad, gg, rtol=1e-4, atol=1e-5 * np.abs(gg).max())
+
+
+def test_ssim_window_constants_match_utils_formula():
+    """The kernel's window constants equal the float32 evaluation of
+    utils.py:116-124 (gaussian(11, 1.5) / sum in float32)."""
+    import math
+    src = open(os.path.join(os.path.dirname(GOLDEN), "..", "gsparc-wirelessgaussiansplatting_b200", "csrc",
+                            "ssim.cu")).read()
+    body = src[src.index("kSsimWin[11]"):]
+    body = body[body.index("{") + 1:body.index("}")]
+    consts = np.array([float(x.strip().rstrip("f")) for x in body.split(",")], dtype=np.float32)
+    t = torch.tensor([math.exp(-(x - 5) ** 2 / float(2 * 1.5 ** 2)) for x in range(11)], dtype=torch.float32)
+    t = t / t.sum()
+    assert np.array_equal(consts, t.numpy())
+
+
+def _small_scene(P=60, seed=5, H=18, W=72):
+    sc = scenes.make_scene(P, seed=seed)
+    m, s, q, o = sc.activated()
+    rx = scenes.make_receivers(1, seed=seed + 100)[0]
+    v = scenes.view_matrix(rx)
+    return dict(means=m, scales=s, rots=q, opac=o, mlp=sc.mlp, view=v, tx=scenes.TX_POS, rx=rx, H=H, W=W)
+
+
+def test_oracle_fp32_close_to_fp64():
+    sc = _small_scene(P=400, H=45, W=180)
+    args = (sc["means"], sc["scales"], sc["rots"], sc["opac"], sc["mlp"], sc["view"], sc["tx"], sc["rx"],
+            sc["H"], sc["W"])
+    f32 = raster.render(*args, dtype=np.float32)
+    f64 = raster.render(*args, dtype=np.float64)
+    same = f32["n_contrib"] == f64["n_contrib"]
+    assert same.mean() > 0.99
+    peak = np.abs(f64["out"]).max()
+    err = np.abs(f32["out"] - f64["out"])[:, same].max()
+    assert err <= 1e-4 * peak
+
+
+def test_bin_and_sort_properties():
+    sc = _small_scene(P=300, H=45, W=180)
+    pre = raster.preprocess(sc["means"], sc["scales"], sc["rots"], sc["opac"], sc["mlp"], sc["view"], sc["tx"],
+                            sc["rx"], sc["H"], sc["W"])
+    keys, vals, ranges = raster.bin_and_sort(pre["means2D"], pre["depth"], pre["radii"], sc["H"], sc["W"])
+    assert keys.size == pre["tiles_touched"].sum()
+    assert np.all(np.diff(keys.astype(np.uint64)) >= 0)
+    counts = np.bincount(vals, minlength=sc["means"].shape[0])
+    np.testing.assert_array_equal(counts, pre["tiles_touched"])
+    for t in range(ranges.shape[0]):
+        s, e = ranges[t]
+        if e > s:
+            assert np.all((keys[s:e] >> np.uint64(32)) == t)
+
+
+@pytest.mark.parametrize("seed", [5, 6])
+def test_oracle_exact_adjoint_matches_fp64_central_differences(seed):
+    """The oracle's backward in exact mode equals FP64 central differences
+    (h=1e-4) of the decision-frozen forward, for a linear loss on both
+    channels.  Tolerance: 1e-5 relative to the largest gradient entry plus
+    1e-4 relative per entry."""
+    sc = _small_scene(P=40, seed=seed)
+    H, W = sc["H"], sc["W"]
+    rng = np.random.default_rng(seed)
+    wr = rng.normal(size=(2, H, W))
+    frozen = fd.freeze(sc["means"].astype(np.float64), sc["scales"].astype(np.float64),
+                       sc["rots"].astype(np.float64), sc["opac"].astype(np.float64),
+                       sc["mlp"].astype(np.float64), sc["view"], sc["tx"], sc["rx"], H, W)
+    fwd = frozen[3]
+    grads = raster.render_backward(fwd, sc["means"].astype(np.float64), sc["scales"].astype(np.float64),
+                                   sc["rots"].astype(np.float64), sc["opac"].astype(np.float64),
+                                   sc["mlp"].astype(np.float64), sc["view"], sc["tx"], sc["rx"], wr, H, W,
+                                   dtype=np.float64, ref_compat=False)
+    params = dict(means=sc["means"].astype(np.float64), scales=sc["scales"].astype(np.float64),
+                  rots=sc["rots"].astype(np.float64), opac=sc["opac"].astype(np.float64),
+                  mlp=sc["mlp"].astype(np.float64))
+    gmap = dict(means="dL_dmeans3D", scales="dL_dscales", rots="dL_drotations", opac="dL_dopacity",
+                mlp="dL_dmlp")
+    vis = np.nonzero(fwd["pre"]["radii"] > 0)[0]
+    assert vis.size > 5
+
+    def loss(p):
+        out = fd.frozen_render(frozen, p["means"], p["scales"], p["rots"], p["opac"], p["mlp"], sc["view"],
+                               sc["tx"], sc["rx"], H, W)
+        return float((out * wr).sum())
+
+    h = 1e-4
+    checked = 0
+    for name in ("means", "scales", "rots", "opac", "mlp"):
+        for _ in range(4):
+            g = int(rng.choice(vis))
+            if name == "mlp":
+                P = params["means"].shape[0]
+                idx = (int(rng.integers(0, 96)) + g * 96,)   # a first-layer weight of Gaussian g
+            else:
+                idx = (g, int(rng.integers(0, params[name].shape[1])))
+            plus = {k: v.copy() for k, v in params.items()}
+            minus = {k: v.copy() for k, v in params.items()}
+            plus[name][idx] += h
+            minus[name][idx] -= h
+            num = (loss(plus) - loss(minus)) / (2 * h)
+            ana = grads[gmap[name]].reshape(params[name].shape)[idx]
+            scale = np.abs(grads[gmap[name]]).max() + 1e-12
+            assert abs(num - ana) <= 1e-5 * scale + 1e-4 * abs(num), (name, idx, num, ana)
+            checked += 1
+    assert checked == 20
+
+
+def test_oracle_reference_mode_halves_azimuth_jacobian():
+    """The reference backward's 0.5 on the azimuth Jacobian row
+    (backward.cu:172-173) makes its mean gradient differ from the exact one;
+    the oracle reproduces that difference."""
+    sc = _small_scene(P=40, seed=7)
+    H, W = sc["H"], sc["W"]
+    fwd = raster.render(sc["means"], sc["scales"], sc["rots"], sc["opac"], sc["mlp"], sc["view"], sc["tx"],
+                        sc["rx"], H, W, dtype=np.float64)
+    wr = np.random.default_rng(0).normal(size=(2, H, W))
+    a = raster.render_backward(fwd, sc["means"], sc["scales"], sc["rots"], sc["opac"], sc["mlp"], sc["view"],
+                               sc["tx"], sc["rx"], wr, H, W, dtype=np.float64, ref_compat=True)
+    b = raster.render_backward(fwd, sc["means"], sc["scales"], sc["rots"], sc["opac"], sc["mlp"], sc["view"],
+                               sc["tx"], sc["rx"], wr, H, W, dtype=np.float64, ref_compat=False)
+    assert not np.allclose(a["dL_dmeans3D"], b["dL_dmeans3D"])
+    np.testing.assert_allclose(a["dL_dmlp"], b["dL_dmlp"], rtol=1e-12, atol=0)   # MLP path unaffected
+
+
+def test_mark_visible_oracle():
+    sc = _small_scene(P=200)
+    vis = raster.mark_visible(sc["means"], sc["view"])
+    d = np.linalg.norm(sc["means"] - sc["rx"][None], axis=1)
+    np.testing.assert_array_equal(vis[np.abs(d - 0.2) > 1e-4], (d > 0.2)[np.abs(d - 0.2) > 1e-4])
