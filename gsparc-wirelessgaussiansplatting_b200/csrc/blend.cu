@@ -24,7 +24,7 @@ namespace gsparc {
 __global__ void __launch_bounds__(kBlendThreads)
 blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict__ ranges,
                      const uint32_t* __restrict__ point_list, GeomView geo,
-                     const ImageHeader* __restrict__ hdr, float* __restrict__ final_T,
+                     ImageHeader* __restrict__ hdr, float* __restrict__ final_T,
                      uint32_t* __restrict__ n_contrib, float* __restrict__ out_real,
                      float* __restrict__ out_imag) {
   if (hdr->error) return;
@@ -52,7 +52,7 @@ blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict
   float2 pf_xy = make_float2(0.f, 0.f), pf_sg = make_float2(0.f, 0.f);
   float4 pf_co = make_float4(0.f, 0.f, 0.f, 0.f);
   if (tid < n) {
-    const uint32_t id = point_list[range.x + tid];
+    const uint32_t id = checked_id(point_list[range.x + tid], P, hdr);
     pf_xy = geo.means2D[roff + id];
     pf_co = geo.conic_opacity[roff + id];
     pf_sg = geo.signal[roff + id];
@@ -66,7 +66,7 @@ blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict
     if (__syncthreads_count(done) == kBlendThreads) break;
     const int nxt = (i + 1) * kBlendThreads + tid;
     if (nxt < n) {
-      const uint32_t id = point_list[range.x + nxt];
+      const uint32_t id = checked_id(point_list[range.x + nxt], P, hdr);
       pf_xy = geo.means2D[roff + id];
       pf_co = geo.conic_opacity[roff + id];
       pf_sg = geo.signal[roff + id];
@@ -133,7 +133,7 @@ __device__ __forceinline__ float warp_reduce8(const float v[8], int lane) {
 __global__ void __launch_bounds__(kBlendThreads)
 blend_backward_kernel(int P, int H, int W, TileGrid grid, unsigned grad_mode,
                       const uint2* __restrict__ ranges, const uint32_t* __restrict__ point_list,
-                      GeomView geo, const ImageHeader* __restrict__ hdr,
+                      GeomView geo, ImageHeader* __restrict__ hdr,
                       const float* __restrict__ final_Ts, const uint32_t* __restrict__ n_contrib,
                       const float* __restrict__ dL_dout_real, const float* __restrict__ dL_dout_imag,
                       float* __restrict__ dmean2D, float* __restrict__ dconic,
@@ -183,7 +183,7 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, unsigned grad_mode,
   float2 pf_xy = make_float2(0.f, 0.f), pf_sg = make_float2(0.f, 0.f);
   float4 pf_co = make_float4(0.f, 0.f, 0.f, 0.f);
   if (tid < nproc) {
-    pf_id = point_list[range.x + nproc - 1 - tid];
+    pf_id = checked_id(point_list[range.x + nproc - 1 - tid], P, hdr);
     pf_xy = geo.means2D[roff + pf_id];
     pf_co = geo.conic_opacity[roff + pf_id];
     pf_sg = geo.signal[roff + pf_id];
@@ -198,7 +198,7 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, unsigned grad_mode,
     __syncthreads();
     const int nxt = (i + 1) * kBlendThreads + tid;
     if (nxt < nproc) {
-      pf_id = point_list[range.x + nproc - 1 - nxt];
+      pf_id = checked_id(point_list[range.x + nproc - 1 - nxt], P, hdr);
       pf_xy = geo.means2D[roff + pf_id];
       pf_co = geo.conic_opacity[roff + pf_id];
       pf_sg = geo.signal[roff + pf_id];

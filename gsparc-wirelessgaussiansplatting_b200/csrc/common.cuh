@@ -32,6 +32,7 @@ constexpr int kMlpFloats = kMlpIn * kMlpHidden + kMlpHidden + kMlpOut * kMlpHidd
 // error word bits (image state header)
 constexpr uint32_t kErrCapacity = 1u << 0;   // K exceeded the binning capacity
 constexpr uint32_t kErrSegment = 1u << 1;    // a tile segment exceeded the sort limit
+constexpr uint32_t kErrBadIndex = 1u << 2;   // a point list held an id >= P (arena mismatch)
 
 struct ImageHeader {
   unsigned long long num_rendered;   // K, written by the scan kernel
@@ -264,6 +265,16 @@ __device__ __forceinline__ Mat3 jac_mat(float J00, float J02, float J10, float J
 
 __device__ __forceinline__ void atomic_or_error(ImageHeader* hdr, uint32_t bits) {
   atomicOr(&hdr->error, bits);
+}
+
+// Gaussian id read from a point list, clamped into [0, P) so a mismatched or
+// corrupt arena can never index out of bounds; the error word records it.
+__device__ __forceinline__ uint32_t checked_id(uint32_t id, int P, ImageHeader* hdr) {
+  if (id >= (uint32_t)P) {
+    atomic_or_error(hdr, kErrBadIndex);
+    return 0u;
+  }
+  return id;
 }
 
 }  // namespace gsparc

@@ -71,6 +71,20 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
     for (int i = 0; i < 16; ++i) mv[i] = __ldg(m + i);
     const float3 p = make_float3(__ldg(means3D + 3 * g), __ldg(means3D + 3 * g + 1), __ldg(means3D + 3 * g + 2));
     int radius_i = 0;
+    // computeCov3D (forward.cu:124-149).  Receiver independent: written by the
+    // receiver-0 thread for every Gaussian, including ones receiver 0 culls,
+    // because other receivers of the batch (and the backward) read it.
+    const float3 s = make_float3(mod * __ldg(scales + 3 * g), mod * __ldg(scales + 3 * g + 1),
+                                 mod * __ldg(scales + 3 * g + 2));
+    const float4 q = make_float4(__ldg(rotations + 4 * g), __ldg(rotations + 4 * g + 1),
+                                 __ldg(rotations + 4 * g + 2), __ldg(rotations + 4 * g + 3));
+    const Mat3 M = scale_rot(s, quat_to_rot(q));
+    const Mat3 Sigma = mat_mul(mat_T(M), M);
+    float cov3[6] = {Sigma.c[0][0], Sigma.c[0][1], Sigma.c[0][2], Sigma.c[1][1], Sigma.c[1][2], Sigma.c[2][2]};
+    if (r == 0) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) geo.cov3D[(size_t)g * 6 + i] = cov3[i];
+    }
     // range cull (too_close, auxiliary.h:133-155)
     const float3 t = view_point(p, mv);
     const float rr = t.x * t.x + t.y * t.y + t.z * t.z;
@@ -82,18 +96,6 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
       const float lat = asinf(t.y * inv_r);
       const float ndc_x = lon * kInvPi;
       const float ndc_y = lat * (kTwoInvPi);
-      // computeCov3D (forward.cu:124-149)
-      const float3 s = make_float3(mod * __ldg(scales + 3 * g), mod * __ldg(scales + 3 * g + 1),
-                                   mod * __ldg(scales + 3 * g + 2));
-      const float4 q = make_float4(__ldg(rotations + 4 * g), __ldg(rotations + 4 * g + 1),
-                                   __ldg(rotations + 4 * g + 2), __ldg(rotations + 4 * g + 3));
-      const Mat3 M = scale_rot(s, quat_to_rot(q));
-      const Mat3 Sigma = mat_mul(mat_T(M), M);
-      float cov3[6] = {Sigma.c[0][0], Sigma.c[0][1], Sigma.c[0][2], Sigma.c[1][1], Sigma.c[1][2], Sigma.c[2][2]};
-      if (r == 0) {
-#pragma unroll
-        for (int i = 0; i < 6; ++i) geo.cov3D[(size_t)g * 6 + i] = cov3[i];
-      }
       // computeCov2D (forward.cu:78-122)
       const ProjJac pj = proj_jacobian(t, W, H);
       const Mat3 J = jac_mat(pj.J00, pj.J02, pj.J10, pj.J11, pj.J12);
@@ -116,7 +118,9 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
         const float py = ndc_to_pixel(ndc_y, H);
         radius_i = (int)my_radius;
         tile_rect(px, py, radius_i, grid, x0, y0, x1, y1);
-        if ((x1 - x0) * (y1 - y0) != 0) {
+        // radius_i > 0 keeps the histogram consistent with the scatter, which
+        // keys on radii > 0, even for non-finite inputs (ceil(NaN) -> 0)
+        if (radius_i > 0 && (x1 - x0) * (y1 - y0) != 0) {
           vis = true;
           const float3 rx = make_float3(__ldg(rx_pos + 3 * r), __ldg(rx_pos + 3 * r + 1), __ldg(rx_pos + 3 * r + 2));
           const float3 tx = make_float3(__ldg(tx_pos), __ldg(tx_pos + 1), __ldg(tx_pos + 2));

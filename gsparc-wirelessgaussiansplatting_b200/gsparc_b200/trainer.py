@@ -124,12 +124,5 @@ class SplatTrainer:
     def _allreduce_grads(self):
         """Sum every gradient over the process group in one flat bucket (the
         one exchange step of a receiver-sharded step)."""
-        import torch.distributed as dist
-        ps = [p for p in self.parameters() if p.grad is not None]
-        flat = torch.cat([p.grad.reshape(-1) for p in ps])
-        dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=self.group)
-        off = 0
-        for p in ps:
-            n = p.grad.numel()
-            p.grad.copy_(flat[off:off + n].view_as(p.grad))
-            off += n
+        from .shard import allreduce_grads
+        allreduce_grads(self.parameters(), self.group)

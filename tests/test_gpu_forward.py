@@ -41,8 +41,8 @@ def test_preprocess_matches_oracle(P, seed):
     np.testing.assert_allclose(g["conic_opacity"][0][vis], o["conic_opacity"][vis], rtol=2e-3,
                                atol=1e-6 * np.abs(o["conic_opacity"][vis]).max())
     np.testing.assert_allclose(g["signal"][0][vis], o["signal"][vis], atol=2e-6)
-    near = ~np.isclose(np.linalg.norm(np_in["means"] - np_in["rxs"][0], axis=1), 0.2, atol=1e-4)
-    np.testing.assert_allclose(g["cov3D"][near], o["cov3D"][near], rtol=1e-5, atol=1e-9)
+    # cov3D is written for every Gaussian, culled ones included (batched receivers read it)
+    np.testing.assert_allclose(g["cov3D"], o["cov3D"], rtol=1e-5, atol=1e-9)
 
 
 @pytest.mark.parametrize("tile", [(16, 16), (8, 32), (32, 8)])
