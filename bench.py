@@ -53,6 +53,20 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def _traffic_per_launch():
+    """DRAM bytes per launch recorded from ncu captures (profiles/traffic_per_launch.txt)."""
+    out = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic_per_launch.txt")) as f:
+            for line in f:
+                parts = line.split()
+                if parts and not line.startswith("#") and len(parts) >= 2:
+                    out[parts[0]] = int(parts[1])
+    except OSError:
+        pass
+    return out
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during a timed region."""
 
@@ -231,6 +245,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         sec = timed(dev_step, args.steps)
+        while len(clk.samples) < 3:          # keep the GPU busy until the sampler has a few readings
+            timed(dev_step, max(1, args.steps // 4))
     value = args.steps * world / sec
     # end to end through the public API with host buffers
     for i in range(min(args.warmup, 3)):
@@ -268,12 +284,7 @@ def run_ours(args):
     }
     peak, peak_kind = _peaks()
     achieved = alg.get(dom, 0) / (dom_ms / 1000.0) / 1e9
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic_per_launch.json")) as f:
-            traffic = json.load(f).get(dom)
-    except Exception:
-        pass
+    traffic = _traffic_per_launch().get(dom)
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import raster as oraster
@@ -311,8 +322,8 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -245,8 +245,17 @@ cudaError_t launch_scatter(int P, int R, const TileGrid& grid, const GeomView& g
 
 cudaError_t launch_segment_sort(int R, const TileGrid& grid, ImageView img, BinningView bin, cudaStream_t stream) {
   const size_t sort_smem = (size_t)kSortCap * sizeof(unsigned long long);
-  cudaError_t e = cudaFuncSetAttribute(segment_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem);
+  // set the shared-memory opt-in once per device, so later calls (including
+  // ones made while a CUDA graph is being captured) only enqueue the launch
+  static bool attr_done[64] = {false};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64 || !attr_done[dev]) {
+    e = cudaFuncSetAttribute(segment_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64) attr_done[dev] = true;
+  }
   const int nseg = R * grid.T;
   if (nseg > 0)
     segment_sort_kernel<<<nseg, kSortThreads, sort_smem, stream>>>(img.ranges, img.hdr, bin.keys, bin.keys_alt,

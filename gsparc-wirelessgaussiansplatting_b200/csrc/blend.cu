@@ -45,7 +45,7 @@ blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict
   const size_t roff = (size_t)r * P;
 
   float T = 1.0f;
-  uint32_t contributor = 0, last_contributor = 0;
+  uint32_t last_contributor = 0;
   float acc_r = 0.0f, acc_i = 0.0f;
   bool done = !inside;
 
@@ -72,25 +72,36 @@ blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict
       pf_sg = geo.signal[roff + id];
     }
     const int cnt = min(kBlendThreads, n - i * kBlendThreads);
-    for (int j = 0; !done && j < cnt; ++j) {
-      contributor++;
-      const float2 xy = s_xy[buf][j];
-      const float2 d = make_float2(xy.x - pixf.x, xy.y - pixf.y);
-      const float4 con_o = s_co[buf][j];
-      const float power = -0.5f * (con_o.x * d.x * d.x + con_o.z * d.y * d.y) - con_o.y * d.x * d.y;
-      if (power > 0.0f) continue;
-      const float alpha = fminf(0.99f, con_o.w * expf(power));
-      if (alpha < 1.0f / 255.0f) continue;
-      const float test_T = T * (1 - alpha);
-      if (test_T < 0.0001f) {
-        done = true;
-        continue;
+    const uint32_t list_base = (uint32_t)(i * kBlendThreads);
+    // Predicated, 4-way unrolled walk: the per-entry math of consecutive
+    // entries is independent (only T and the sums carry over), so unrolling
+    // lets the scheduler overlap it.  Decisions are written as the negations
+    // the reference tests (`power > 0`, `alpha < 1/255`) so NaNs take the same
+    // path; the contributor count is the entry's position + 1.
+    for (int j0 = 0; j0 < cnt; j0 += 4) {
+      if (__all_sync(0xffffffffu, done)) break;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int j = j0 + u;
+        if (j < cnt) {
+          const float2 xy = s_xy[buf][j];
+          const float4 con_o = s_co[buf][j];
+          const float2 sg = s_sg[buf][j];
+          const float2 d = make_float2(xy.x - pixf.x, xy.y - pixf.y);
+          const float power = -0.5f * (con_o.x * d.x * d.x + con_o.z * d.y * d.y) - con_o.y * d.x * d.y;
+          const float alpha = fminf(0.99f, con_o.w * expf(power));
+          const float test_T = T * (1 - alpha);
+          const bool take = !done && !(power > 0.0f) && !(alpha < 1.0f / 255.0f);
+          const bool stop = take && (test_T < 0.0001f);
+          done = done || stop;
+          if (take && !stop) {
+            acc_r += sg.x * alpha * T;
+            acc_i += sg.y * alpha * T;
+            T = test_T;
+            last_contributor = list_base + (uint32_t)j + 1u;
+          }
+        }
       }
-      const float2 sg = s_sg[buf][j];
-      acc_r += sg.x * alpha * T;
-      acc_i += sg.y * alpha * T;
-      T = test_T;
-      last_contributor = contributor;
     }
   }
   if (inside) {

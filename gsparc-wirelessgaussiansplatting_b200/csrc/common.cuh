@@ -137,6 +137,16 @@ __device__ __forceinline__ float3 view_point(const float3& p, const float* m) {
   return t;
 }
 
+// squared range |t|^2 with the reference's rounding pinned: the reference
+// expression x*x + y*y + z*z (auxiliary.h:141) compiles to
+// fma(z, z, fma(x, x, y*y)), established against the depth bits recorded from
+// the reference extension (tests/golden/raster_ref_golden.npz); written with
+// explicit intrinsics so the depth key bits do not depend on contraction
+// choices made around this expression
+__device__ __forceinline__ float range_sq(const float3& t) {
+  return __fmaf_rn(t.z, t.z, __fmaf_rn(t.x, t.x, __fmul_rn(t.y, t.y)));
+}
+
 // transpose of the rotation part applied to a vector (auxiliary.h:117-125)
 __device__ __forceinline__ float3 view_vec_T(const float3& v, const float* m) {
   float3 t = {

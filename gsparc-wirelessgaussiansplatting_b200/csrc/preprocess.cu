@@ -87,7 +87,7 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
     }
     // range cull (too_close, auxiliary.h:133-155)
     const float3 t = view_point(p, mv);
-    const float rr = t.x * t.x + t.y * t.y + t.z * t.z;
+    const float rr = range_sq(t);
     if (rr > 0.04f) {
       const float rdist = sqrtf(rr);
       // transformProj (auxiliary.h:101-113)
@@ -163,7 +163,7 @@ __global__ void mark_visible_kernel(int P, const float* __restrict__ means3D,
   for (int i = 0; i < 16; ++i) mv[i] = __ldg(view + i);
   const float3 p = make_float3(means3D[3 * g], means3D[3 * g + 1], means3D[3 * g + 2]);
   const float3 t = view_point(p, mv);
-  const float rr = t.x * t.x + t.y * t.y + t.z * t.z;
+  const float rr = range_sq(t);
   present[g] = rr <= 0.04f ? 0 : 1;
 }
 

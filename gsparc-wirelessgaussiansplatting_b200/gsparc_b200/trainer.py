@@ -51,8 +51,10 @@ class SplatTrainer:
     lambda1 = 0.2            # optimizer.py:8
     confidence_alpha = 0.3   # optimizer.py:33
 
-    def __init__(self, scene: scenes.Scene, H=scenes.H, W=scenes.W, device="cuda", group=None, seed=0):
+    def __init__(self, scene: scenes.Scene, H=scenes.H, W=scenes.W, device="cuda", group=None, seed=0,
+                 capturable=False):
         self.H, self.W, self.device, self.group = H, W, torch.device(device), group
+        self.graph = None
         P = scene.P
         t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=self.device)
         self.centre = nn.Parameter(t(scene.means))
@@ -74,7 +76,7 @@ class SplatTrainer:
             {"params": [self.fc1_w, self.fc1_b, self.fc2_w, self.fc2_b], "lr": 0.002},
             {"params": list(self.confidence.parameters()), "lr": 0.001},
         ]
-        self.optimizer = torch.optim.Adam(groups, lr=0.0, eps=1e-15, fused=True)
+        self.optimizer = torch.optim.Adam(groups, lr=0.0, eps=1e-15, fused=True, capturable=capturable)
         self.scene_lo = torch.tensor(scenes.ROOM_LO, dtype=torch.float32, device=self.device)
         self.scene_hi = torch.tensor(scenes.ROOM_HI, dtype=torch.float32, device=self.device)
         self.eye = torch.eye(4, device=self.device)
@@ -120,6 +122,98 @@ class SplatTrainer:
         with torch.no_grad():
             self.centre.data.clamp_(min=self.scene_lo, max=self.scene_hi)
         return loss.detach()
+
+    # ---- batched, CUDA-graph-capturable step -----------------------------------
+
+    def loss_batched(self, views, rxs, tx, targets, plan):
+        """Mean over R receivers of the per-receiver confidence-weighted loss,
+        rendered in one launch through a static ``RasterPlan``."""
+        from fused_ssim import FusedSSIMMap
+        from .autograd import rasterize
+        out_r, _, _ = rasterize(self.centre, self.emission_mlps(), torch.sigmoid(self.opacity_logit).reshape(-1),
+                                torch.exp(self.log_scale), F.normalize(self.rotation), views, rxs, tx, plan)
+        l1 = torch.abs(out_r - targets).mean(dim=(1, 2))
+        smap = FusedSSIMMap.apply(0.01 ** 2, 0.03 ** 2, out_r.unsqueeze(1), targets.unsqueeze(1), "same", True)
+        s = smap.mean(dim=(1, 2, 3))
+        recon = (1.0 - self.lambda1) * l1 + self.lambda1 * (1.0 - s)
+        conf = self.confidence(rxs).reshape(-1)
+        return (conf * recon - self.confidence_alpha * torch.log(conf)).mean()
+
+    def _batched_body(self):
+        loss = self.loss_batched(self._s_views, self._s_rxs, self._s_tx, self._s_targets, self.plan)
+        loss.backward()
+        with torch.no_grad():
+            g = self.centre.grad
+            torch.where(torch.isnan(g), torch.zeros_like(g), g, out=g)
+            if self.group is not None:
+                self._allreduce_grads()
+        self.optimizer.step()
+        with torch.no_grad():
+            self.centre.data.clamp_(min=self.scene_lo, max=self.scene_hi)
+        return loss.detach()
+
+    def probe_capacity(self, views, rxs, tx, margin=1.25, slack=4096):
+        """Largest instance count over the given receivers, with a margin."""
+        from . import raster
+        kmax = 0
+        with torch.no_grad():
+            for r in range(views.shape[0]):
+                _, _, _, st = raster.forward(self.centre, self.emission_mlps(),
+                                             torch.sigmoid(self.opacity_logit).reshape(-1), torch.exp(self.log_scale),
+                                             F.normalize(self.rotation), self.H, self.W, 1.0, views[r], tx, rxs[r])
+                kmax = max(kmax, st.num_rendered)
+        return int(kmax * margin) + slack
+
+    def capture(self, R, capacity, tx, views=None, rxs=None, targets=None, warmup=3):
+        """Build static buffers for R receivers per step and capture the whole
+        step (render, loss, adjoint, NaN-zeroing, all-reduce, Adam, clamp) in a
+        CUDA graph.  Requires ``capturable=True`` at construction.  The warm-up
+        steps that precede capture (on a side stream, as graph capture needs)
+        run on the given batch; parameters and optimizer state are restored in
+        place afterwards, so the trainer starts from its constructed state."""
+        from .autograd import RasterPlan
+        dev = self.device
+        self.plan = RasterPlan(self.centre.shape[0], R, self.H, self.W, capacity, dev)
+        self._s_views = torch.eye(4, device=dev).repeat(R, 1, 1).contiguous()
+        self._s_rxs = torch.zeros((R, 3), device=dev)
+        self._s_tx = tx.detach().clone().reshape(3)
+        self._s_targets = torch.zeros((R, self.H, self.W), device=dev)
+        if views is not None:
+            self._s_views.copy_(views.reshape(self._s_views.shape))
+            self._s_rxs.copy_(rxs.reshape(self._s_rxs.shape))
+            self._s_targets.copy_(targets.reshape(self._s_targets.shape))
+        backup = [p.detach().clone() for p in self.parameters()]
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            for _ in range(warmup):
+                self.optimizer.zero_grad(set_to_none=True)
+                self._batched_body()
+        torch.cuda.current_stream(dev).wait_stream(side)
+        self.optimizer.zero_grad(set_to_none=True)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._s_loss = self._batched_body()
+        torch.cuda.synchronize(dev)
+        with torch.no_grad():   # in place: the graph holds these addresses
+            for p, b in zip(self.parameters(), backup):
+                p.copy_(b)
+            for st in self.optimizer.state.values():
+                for v in st.values():
+                    if torch.is_tensor(v):
+                        v.zero_()
+        torch.cuda.synchronize(dev)
+
+    def step_graphed(self, views, rxs, targets):
+        """Copy one batch of receivers into the static buffers and replay the
+        captured step.  Returns the loss as a device scalar; the rasterizer's
+        status (K, error word) is in ``self.plan.status_host`` once the stream
+        has been synchronised (``self.plan.check()``)."""
+        self._s_views.copy_(views.reshape(self._s_views.shape), non_blocking=True)
+        self._s_rxs.copy_(rxs.reshape(self._s_rxs.shape), non_blocking=True)
+        self._s_targets.copy_(targets.reshape(self._s_targets.shape), non_blocking=True)
+        self.graph.replay()
+        return self._s_loss
 
     def _allreduce_grads(self):
         """Sum every gradient over the process group in one flat bucket (the

@@ -42,7 +42,9 @@ def test_preprocess_matches_oracle(P, seed):
                                atol=1e-6 * np.abs(o["conic_opacity"][vis]).max())
     np.testing.assert_allclose(g["signal"][0][vis], o["signal"][vis], atol=2e-6)
     # cov3D is written for every Gaussian, culled ones included (batched receivers read it)
-    np.testing.assert_allclose(g["cov3D"], o["cov3D"], rtol=1e-5, atol=1e-9)
+    # off-diagonal entries cancel; FP32 rounding of the products bounds the
+    # absolute error by ~1e-6 of the largest entry
+    np.testing.assert_allclose(g["cov3D"], o["cov3D"], rtol=1e-5, atol=1e-6 * np.abs(o["cov3D"]).max())
 
 
 @pytest.mark.parametrize("tile", [(16, 16), (8, 32), (32, 8)])
