@@ -94,6 +94,12 @@ struct Timed {
 
 }  // namespace
 
+namespace gsparc {
+// error reporting shared with entry points defined in other files
+int report_invalid(const char* what) { return invalid(what); }
+int report_cuda(cudaError_t e, const char* where) { return cuda_fail(e, where); }
+}  // namespace gsparc
+
 extern "C" {
 
 int gsparc_abi_version(void) { return 1; }

@@ -5,6 +5,10 @@
 
 namespace gsparc {
 
+// Record the detail text of a failed call and return its status (capi.cu).
+int report_invalid(const char* what);
+int report_cuda(cudaError_t e, const char* where);
+
 cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, float mod, const float* means3D,
                               const float* mlp, const float* opacities, const float* scales,
                               const float* rotations, const float* views, const float* tx_pos,

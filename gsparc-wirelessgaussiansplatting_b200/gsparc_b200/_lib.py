@@ -53,6 +53,8 @@ _SIGS = {
                                      _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gsparc_ssim_backward": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_float, _c_float,
                                       _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gsparc_ssim_static_scratch": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_float, _c_float,
+                                            _vp, _vp, _vp, _vp, _vp, _vp]),
     "gsparc_timing_enable": (_c_int, [_c_int]),
     "gsparc_timing_kernel_count": (_c_int, []),
     "gsparc_timing_kernel_name": (ctypes.c_char_p, [_c_int]),

@@ -178,6 +178,25 @@ GSPARC_API int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float
                          const float* dm_dmu1, const float* dm_dsigma1_sq,
                          const float* dm_dsigma12, float* dL_dimg1, void* stream);
 
+/* SSIM map and dL/dimg1 in one call that allocates nothing.  No counterpart
+ * in the reference.  For callers that cannot call cudaMalloc (for example a
+ * real-time receiver loop that cannot absorb cudaMalloc's implicit device
+ * synchronisation, or a host handed fixed device buffers by another runtime):
+ * the three partial-derivative maps the gradient needs live in a file-scope
+ * device array of GSPARC_SSIM_STATIC_MAX_PIXELS * 3 floats (12 MiB, held by
+ * every GPU that loads the library until exit).  Inputs img1, img2, dL_dmap
+ * and outputs ssim_map, dL_dimg1 are [B,CH,H,W]; B*CH*H*W must not exceed
+ * GSPARC_SSIM_STATIC_MAX_PIXELS (else GSPARC_ERR_INVALID).  All calls on a
+ * device share the array and leave the last call's maps in it; nothing in it
+ * needs clearing, but calls that overlap on the GPU race on it.  The first
+ * call on a device looks up the array's device address and should be made
+ * before any stream capture. */
+#define GSPARC_SSIM_STATIC_MAX_PIXELS 1048576
+GSPARC_API int gsparc_ssim_static_scratch(int B, int CH, int H, int W, float C1, float C2,
+                                          const float* img1, const float* img2,
+                                          const float* dL_dmap, float* ssim_map, float* dL_dimg1,
+                                          void* stream);
+
 /* ---- per-kernel timing (tracing; no counterpart in the reference, which
  * only times whole renders with time.time(), train.py:673-677) ------------ */
 
