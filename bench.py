@@ -9,11 +9,16 @@ loss, the full hand-written adjoint, Adam.  Each step uses the next receiver
 of a pool; targets are spectra of a second seeded scene at those receivers.
 Synthetic data (no dataset in the container).
 
-value: steps/s with inputs resident in HBM, per-step CUDA events on the
+value: steps/s of the step captured in one CUDA graph (SplatTrainer.capture /
+step_graphed) with inputs resident in HBM; per-step CUDA events on the
 compute stream, L2 flushed (256 MiB write) between steps outside the events.
-e2e: the same step through SplatTrainer with the receiver's target spectrum,
-view matrix and position copied from pinned host memory every step and the
-loss read back to the host, inside the timed region.
+e2e: the same step through SplatTrainer.step_graphed with the receiver's
+target spectrum, view matrix and position copied from pinned host memory
+every step and the loss and rasterizer status read back to the host, inside
+the timed region.  Also reported: the eager drop-in path (reference call
+surface), a 16-receiver batched step, and per-kernel device times of the
+same kernels (from eager steps; graph replays bypass the library's event
+hooks).
 N > 1: one process per GPU (torchrun), receivers sharded, Gaussians
 replicated, gradients all-reduced over NCCL every step (weak scaling).
 --impl reference: the CPU restatement of the same step (oracle/) on the
@@ -198,27 +203,27 @@ def run_ours(args):
     targets_h = targets_d.cpu().pin_memory()
     views_h = torch.tensor(views).pin_memory()
     rxs_h = torch.tensor(rxs).pin_memory()
-    trainer = SplatTrainer(sc, device=dev, group=group)
+    # the product path: the whole step captured in one CUDA graph, one receiver per step
+    trainer = SplatTrainer(sc, device=dev, group=group, capturable=True)
+    capacity = trainer.probe_capacity(views_d, rxs_d, tx)
+    trainer.capture(1, capacity, tx, views_d[0:1], rxs_d[0:1], targets_d[0:1])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
     def dev_step(i):
         j = i % POOL
-        return trainer.step(views_d[j], rxs_d[j], tx, targets_d[j])
+        return trainer.step_graphed(views_d[j:j + 1], rxs_d[j:j + 1], targets_d[j:j + 1])
 
-    tgt_buf = torch.empty((90, 360), dtype=torch.float32, device=dev)
-    view_buf = torch.empty((4, 4), dtype=torch.float32, device=dev)
-    rx_buf = torch.empty(3, dtype=torch.float32, device=dev)
     loss_h = torch.empty((), dtype=torch.float32).pin_memory()
 
     def host_step(i):
+        # target spectrum, view matrix and receiver position copied from pinned
+        # host memory into the graph's inputs; loss and rasterizer status back
         j = i % POOL
-        tgt_buf.copy_(targets_h[j], non_blocking=True)
-        view_buf.copy_(views_h[j], non_blocking=True)
-        rx_buf.copy_(rxs_h[j], non_blocking=True)
-        loss = trainer.step(view_buf, rx_buf, tx, tgt_buf)
+        loss = trainer.step_graphed(views_h[j:j + 1], rxs_h[j:j + 1], targets_h[j:j + 1])
         loss_h.copy_(loss, non_blocking=True)
         stream.synchronize()
+        trainer.plan.check()
         return float(loss_h)
 
     def timed(fn, steps):
@@ -247,6 +252,7 @@ def run_ours(args):
         sec = timed(dev_step, args.steps)
         while len(clk.samples) < 3:          # keep the GPU busy until the sampler has a few readings
             timed(dev_step, max(1, args.steps // 4))
+    trainer.plan.check()                      # the capacity held for every timed step
     value = args.steps * world / sec
     # end to end through the public API with host buffers
     for i in range(min(args.warmup, 3)):
@@ -254,14 +260,34 @@ def run_ours(args):
     e2e_sec = timed(host_step, args.steps)
     e2e = args.steps * world / e2e_sec
     h2d = (90 * 360 + 16 + 3) * 4
-    # per-kernel device times over a third pass of the same steps
+    # the eager drop-in path (reference call surface, instance-count readback per step)
+    eager = SplatTrainer(sc, device=dev, group=group)
+
+    def eager_step(i):
+        j = i % POOL
+        return eager.step(views_d[j], rxs_d[j], tx, targets_d[j])
+
+    for i in range(3):
+        eager_step(i)
+    n_eager = max(1, min(args.steps, 50))
+    dropin = n_eager * world / timed(eager_step, n_eager)
+    # per-kernel device times from eager steps (graph replays bypass the
+    # library's event hooks; the kernels and their work are the same)
     with _lib.KernelTimer() as kt:
-        for i in range(args.steps):
-            dev_step(i)
+        for i in range(n_eager):
+            eager_step(i)
         torch.cuda.synchronize()
     ktimes = {k: v for k, v in kt.results().items() if v[1] > 0}
-    launches = sum(c for _, c in ktimes.values())
+    launches = sum(c for _, c in ktimes.values()) // n_eager
     dom = max(ktimes, key=lambda k: ktimes[k][0])
+    # batched: every receiver of the pool in one captured step
+    btr = SplatTrainer(sc, device=dev, group=group, capturable=True)
+    btr.capture(POOL, capacity * POOL, tx, views_d, rxs_d, targets_d)
+    n_b = max(1, args.steps // 4)
+    bsec = timed(lambda i: btr.step_graphed(views_d, rxs_d, targets_d), n_b)
+    btr.plan.check()
+    batched = {"receivers_per_step": POOL, "steps_per_s": n_b * world / bsec,
+               "spectra_per_s": n_b * POOL * world / bsec}
     dom_ms = ktimes[dom][0] / ktimes[dom][1]
     # algorithmic bytes per launch of the dominant kernel
     with torch.no_grad():
@@ -305,12 +331,16 @@ def run_ours(args):
                            "l2": "flushed between steps (256 MiB write, outside the timed events)",
                            "parallelism": f"dp{world} (receivers sharded, gradients all-reduced)"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
-                "gpu_launches": launches // args.steps * args.steps,
+                "gpu_launches": launches * args.steps,
                 "clocks": clk.summary(),
                 "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                              "avg_launch_ms": dom_ms, "algorithmic_bytes": alg.get(dom)},
-                "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(ktimes.items())},
+                "kernel_ms_per_step": {k: v[0] / n_eager for k, v in sorted(ktimes.items())},
+                "dropin_eager_steps_per_s": dropin,
+                "batched": batched,
+                "path": "CUDA-graph-captured step (SplatTrainer.capture / step_graphed), binning capacity "
+                        f"{capacity}",
                 "cpu_baseline": cpu_base}
         print(json.dumps(line))
     if group is not None:
