@@ -1,45 +1,76 @@
 // Per-tile alpha blending, forward and adjoint.
 //
-// One CTA per (tile, receiver); 256 threads = one pixel each (16x16, 8x32 or
-// 32x8 tiles).  Gaussian attributes for the next batch of 256 list entries
-// are prefetched into registers while the current batch, staged in shared
-// memory, is being blended (double buffer, one barrier per batch).
+// A tile of 256 pixels (16x16, 8x32 or 32x8) is covered by 256/kThreads CTAs
+// of kThreads threads, one pixel each: kThreads = 256 when there are enough
+// tiles to fill the GPU (batched receivers), kThreads = 64 for a single
+// receiver, where the kernel's time is the longest tile list walked by one
+// warp -- four CTAs per tile put that tile's warps on four SMs.
+//
+// Every CTA stages its tile's sorted list in batches of 256 entries (position,
+// conic, signal, footprint box) in shared memory, prefetching the next batch
+// into registers while the current one is blended (double buffer, one
+// barrier per batch).  A warp skips an entry when the splat's footprint box
+// (footprint_box, computed in the preprocess) lies entirely outside the
+// warp's pixels: alpha < 1/255 there, so the reference would skip the entry
+// for every one of those pixels and no result changes.
 //
 // Forward: renderCUDA (cuda_wireless_rasterizer/forward.cu:151-249).  The
 // per-pixel arithmetic keeps the reference's operation order so final T,
-// contributor counts and the spectra match it bit for bit.  Early exit is the
-// same block-wide count of finished pixels.
+// contributor counts and the spectra match it bit for bit.  The walk over a
+// batch is predicated and unrolled by four; block-wide early exit as in the
+// reference.
 //
-// Adjoint: renderCUDA backward (backward.cu:442-616).  Two changes of
-// method: (1) only list positions below the largest contributor count of the
-// tile are visited; (2) the eight per-(pixel, Gaussian) gradient terms are
-// reduced across the warp with a transposing shuffle tree (9 shuffles), then
-// accumulated per batch in shared memory and flushed with one global atomic
-// per (tile, Gaussian, term), instead of 8 global atomics per pixel.
+// Adjoint: renderCUDA backward (backward.cu:442-616), walking from the CTA's
+// largest contributor count down.  The eight per-(pixel, Gaussian) gradient
+// terms are reduced across the warp with a transposing shuffle tree (9
+// shuffles), summed per batch in shared memory and flushed with one global
+// atomic per (CTA, Gaussian, term).
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace gsparc {
 
-__global__ void __launch_bounds__(kBlendThreads)
+constexpr int kBatch = 256;   // list entries staged per round
+
+struct WarpRect {
+  float x0, x1, y0, y1;
+};
+
+__device__ __forceinline__ WarpRect warp_rect(int px, int py) {
+  WarpRect w;
+  w.x0 = (float)__reduce_min_sync(0xffffffffu, px);
+  w.x1 = (float)__reduce_max_sync(0xffffffffu, px);
+  w.y0 = (float)__reduce_min_sync(0xffffffffu, py);
+  w.y1 = (float)__reduce_max_sync(0xffffffffu, py);
+  return w;
+}
+
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads)
 blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict__ ranges,
                      const uint32_t* __restrict__ point_list, GeomView geo,
                      ImageHeader* __restrict__ hdr, float* __restrict__ final_T,
                      uint32_t* __restrict__ n_contrib, float* __restrict__ out_real,
                      float* __restrict__ out_imag) {
+  constexpr int kParts = kBlendThreads / kThreads;
+  constexpr int kPer = kBatch / kThreads;
   if (hdr->error) return;
-  __shared__ float2 s_xy[2][kBlendThreads];
-  __shared__ float4 s_co[2][kBlendThreads];
-  __shared__ float2 s_sg[2][kBlendThreads];
+  __shared__ float2 s_xy[2][kBatch];
+  __shared__ float4 s_co[2][kBatch];
+  __shared__ float2 s_sg[2][kBatch];
+  __shared__ float4 s_bb[2][kBatch];
 
   const int r = blockIdx.z;
-  const int tile = blockIdx.y * grid.gx + blockIdx.x;
+  const int tile_x = blockIdx.x / kParts, part = blockIdx.x % kParts;
+  const int tile = blockIdx.y * grid.gx + tile_x;
   const int tid = threadIdx.x;
-  const int px = blockIdx.x * grid.tile_w + tid % grid.tile_w;
-  const int py = blockIdx.y * grid.tile_h + tid / grid.tile_w;
+  const int li = part * kThreads + tid;
+  const int px = tile_x * grid.tile_w + li % grid.tile_w;
+  const int py = blockIdx.y * grid.tile_h + li / grid.tile_w;
   const bool inside = px < W && py < H;
   const size_t pix = (size_t)r * H * W + (size_t)py * W + px;
   const float2 pixf = make_float2((float)px, (float)py);
+  const WarpRect wr = warp_rect(px, py);
   const uint2 range = ranges[(size_t)r * grid.T + tile];
   const int n = (int)(range.y - range.x);
   const size_t roff = (size_t)r * P;
@@ -49,41 +80,61 @@ blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict
   float acc_r = 0.0f, acc_i = 0.0f;
   bool done = !inside;
 
-  float2 pf_xy = make_float2(0.f, 0.f), pf_sg = make_float2(0.f, 0.f);
-  float4 pf_co = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (tid < n) {
-    const uint32_t id = checked_id(point_list[range.x + tid], P, hdr);
-    pf_xy = geo.means2D[roff + id];
-    pf_co = geo.conic_opacity[roff + id];
-    pf_sg = geo.signal[roff + id];
-  }
-  const int rounds = (n + kBlendThreads - 1) / kBlendThreads;
+  float2 pf_xy[kPer], pf_sg[kPer];
+  float4 pf_co[kPer], pf_bb[kPer];
+  auto prefetch = [&](int base) {
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int e = base + k * kThreads + tid;
+      if (e < n) {
+        const uint32_t id = checked_id(point_list[range.x + e], P, hdr);
+        pf_xy[k] = geo.means2D[roff + id];
+        pf_co[k] = geo.conic_opacity[roff + id];
+        pf_sg[k] = geo.signal[roff + id];
+        pf_bb[k] = geo.box[roff + id];
+      }
+    }
+  };
+  prefetch(0);
+  const int rounds = (n + kBatch - 1) / kBatch;
   for (int i = 0; i < rounds; ++i) {
     const int buf = i & 1;
-    s_xy[buf][tid] = pf_xy;
-    s_co[buf][tid] = pf_co;
-    s_sg[buf][tid] = pf_sg;
-    if (__syncthreads_count(done) == kBlendThreads) break;
-    const int nxt = (i + 1) * kBlendThreads + tid;
-    if (nxt < n) {
-      const uint32_t id = checked_id(point_list[range.x + nxt], P, hdr);
-      pf_xy = geo.means2D[roff + id];
-      pf_co = geo.conic_opacity[roff + id];
-      pf_sg = geo.signal[roff + id];
-    }
-    const int cnt = min(kBlendThreads, n - i * kBlendThreads);
-    const uint32_t list_base = (uint32_t)(i * kBlendThreads);
-    // Predicated, 4-way unrolled walk: the per-entry math of consecutive
-    // entries is independent (only T and the sums carry over), so unrolling
-    // lets the scheduler overlap it.  Decisions are written as the negations
-    // the reference tests (`power > 0`, `alpha < 1/255`) so NaNs take the same
-    // path; the contributor count is the entry's position + 1.
-    for (int j0 = 0; j0 < cnt; j0 += 4) {
-      if (__all_sync(0xffffffffu, done)) break;
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int j = j0 + u;
-        if (j < cnt) {
+    for (int k = 0; k < kPer; ++k) {
+      const int s = k * kThreads + tid;
+      s_xy[buf][s] = pf_xy[k];
+      s_co[buf][s] = pf_co[k];
+      s_sg[buf][s] = pf_sg[k];
+      s_bb[buf][s] = pf_bb[k];
+    }
+    if (__syncthreads_count(done) == kThreads) break;
+    if (i + 1 < rounds) prefetch((i + 1) * kBatch);
+    const int cnt = min(kBatch, n - i * kBatch);
+    const uint32_t list_base = (uint32_t)(i * kBatch);
+    // Walk in chunks of 32 entries: each lane tests one entry's footprint box
+    // against the warp's pixels and a ballot keeps the entries that can touch
+    // them; those are then processed in list order, four per pass, with
+    // branch-free predicated math so consecutive entries overlap (only T and
+    // the sums carry over).  Decisions are the negations of the reference's
+    // tests (`power > 0`, `alpha < 1/255`) so NaNs take the same path; the
+    // contributor count is the entry's list position + 1.
+    for (int c0 = 0; c0 < cnt; c0 += 32) {
+      if (__all_sync(0xffffffffu, done)) break;
+      const int jl = c0 + (threadIdx.x & 31);
+      unsigned mask = __ballot_sync(0xffffffffu, jl < cnt && !box_outside(s_bb[buf][min(jl, kBatch - 1)],
+                                                                          wr.x0, wr.x1, wr.y0, wr.y1));
+      while (mask) {
+        int js[4];
+        bool vs[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          vs[u] = mask != 0u;
+          js[u] = c0 + (vs[u] ? __ffs(mask) - 1 : 0);
+          mask &= mask - 1u;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int j = js[u];
           const float2 xy = s_xy[buf][j];
           const float4 con_o = s_co[buf][j];
           const float2 sg = s_sg[buf][j];
@@ -91,7 +142,7 @@ blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict
           const float power = -0.5f * (con_o.x * d.x * d.x + con_o.z * d.y * d.y) - con_o.y * d.x * d.y;
           const float alpha = fminf(0.99f, con_o.w * expf(power));
           const float test_T = T * (1 - alpha);
-          const bool take = !done && !(power > 0.0f) && !(alpha < 1.0f / 255.0f);
+          const bool take = vs[u] && !done && !(power > 0.0f) && !(alpha < 1.0f / 255.0f);
           const bool stop = take && (test_T < 0.0001f);
           done = done || stop;
           if (take && !stop) {
@@ -141,7 +192,8 @@ __device__ __forceinline__ float warp_reduce8(const float v[8], int lane) {
   return z;
 }
 
-__global__ void __launch_bounds__(kBlendThreads)
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads)
 blend_backward_kernel(int P, int H, int W, TileGrid grid, unsigned grad_mode,
                       const uint2* __restrict__ ranges, const uint32_t* __restrict__ point_list,
                       GeomView geo, ImageHeader* __restrict__ hdr,
@@ -149,23 +201,29 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, unsigned grad_mode,
                       const float* __restrict__ dL_dout_real, const float* __restrict__ dL_dout_imag,
                       float* __restrict__ dmean2D, float* __restrict__ dconic,
                       float* __restrict__ dsig, float* __restrict__ dopac) {
+  constexpr int kParts = kBlendThreads / kThreads;
+  constexpr int kPer = kBatch / kThreads;
   if (hdr->error) return;
-  __shared__ uint32_t s_id[2][kBlendThreads];
-  __shared__ float2 s_xy[2][kBlendThreads];
-  __shared__ float4 s_co[2][kBlendThreads];
-  __shared__ float2 s_sg[2][kBlendThreads];
-  __shared__ float s_grad[2][kBlendThreads][8];
+  __shared__ uint32_t s_id[2][kBatch];
+  __shared__ float2 s_xy[2][kBatch];
+  __shared__ float4 s_co[2][kBatch];
+  __shared__ float2 s_sg[2][kBatch];
+  __shared__ float4 s_bb[2][kBatch];
+  __shared__ float s_grad[2][kBatch][8];
   __shared__ int s_maxlast;
 
   const bool ref = grad_mode == GSPARC_GRAD_REFERENCE;
   const int r = blockIdx.z;
-  const int tile = blockIdx.y * grid.gx + blockIdx.x;
+  const int tile_x = blockIdx.x / kParts, part = blockIdx.x % kParts;
+  const int tile = blockIdx.y * grid.gx + tile_x;
   const int tid = threadIdx.x, lane = tid & 31;
-  const int px = blockIdx.x * grid.tile_w + tid % grid.tile_w;
-  const int py = blockIdx.y * grid.tile_h + tid / grid.tile_w;
+  const int li = part * kThreads + tid;
+  const int px = tile_x * grid.tile_w + li % grid.tile_w;
+  const int py = blockIdx.y * grid.tile_h + li / grid.tile_w;
   const bool inside = px < W && py < H;
   const size_t pix = (size_t)r * H * W + (size_t)py * W + px;
   const float2 pixf = make_float2((float)px, (float)py);
+  const WarpRect wr = warp_rect(px, py);
   const uint2 range = ranges[(size_t)r * grid.T + tile];
   const size_t roff = (size_t)r * P;
 
@@ -175,8 +233,7 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, unsigned grad_mode,
   const float dLi = inside ? dL_dout_imag[pix] : 0.0f;
 
   if (tid == 0) s_maxlast = 0;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) { s_grad[0][tid][k] = 0.0f; s_grad[1][tid][k] = 0.0f; }
+  for (int e = tid; e < 2 * kBatch * 8; e += kThreads) (&s_grad[0][0][0])[e] = 0.0f;
   __syncthreads();
   const int wmax = __reduce_max_sync(0xffffffffu, last_contributor);
   if (lane == 0) atomicMax(&s_maxlast, wmax);
@@ -188,91 +245,131 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, unsigned grad_mode,
   float acc_r = 0.0f, acc_i = 0.0f, last_alpha = 0.0f, last_sr = 0.0f, last_si = 0.0f;
   const float ddelx_dx = 0.5f * W;
   const float ddely_dy = 0.5f * H;
-  int contributor = nproc;
 
-  uint32_t pf_id = 0;
-  float2 pf_xy = make_float2(0.f, 0.f), pf_sg = make_float2(0.f, 0.f);
-  float4 pf_co = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (tid < nproc) {
-    pf_id = checked_id(point_list[range.x + nproc - 1 - tid], P, hdr);
-    pf_xy = geo.means2D[roff + pf_id];
-    pf_co = geo.conic_opacity[roff + pf_id];
-    pf_sg = geo.signal[roff + pf_id];
-  }
-  const int rounds = (nproc + kBlendThreads - 1) / kBlendThreads;
+  uint32_t pf_id[kPer];
+  float2 pf_xy[kPer], pf_sg[kPer];
+  float4 pf_co[kPer], pf_bb[kPer];
+  // batch i holds list positions nproc-1-i*kBatch down to nproc-(i+1)*kBatch
+  auto prefetch = [&](int base) {
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int e = base + k * kThreads + tid;
+      if (e < nproc) {
+        const uint32_t id = checked_id(point_list[range.x + nproc - 1 - e], P, hdr);
+        pf_id[k] = id;
+        pf_xy[k] = geo.means2D[roff + id];
+        pf_co[k] = geo.conic_opacity[roff + id];
+        pf_sg[k] = geo.signal[roff + id];
+        pf_bb[k] = geo.box[roff + id];
+      }
+    }
+  };
+  prefetch(0);
+
+  const int rounds = (nproc + kBatch - 1) / kBatch;
   for (int i = 0; i < rounds; ++i) {
     const int buf = i & 1;
-    s_id[buf][tid] = pf_id;
-    s_xy[buf][tid] = pf_xy;
-    s_co[buf][tid] = pf_co;
-    s_sg[buf][tid] = pf_sg;
-    __syncthreads();
-    const int nxt = (i + 1) * kBlendThreads + tid;
-    if (nxt < nproc) {
-      pf_id = checked_id(point_list[range.x + nproc - 1 - nxt], P, hdr);
-      pf_xy = geo.means2D[roff + pf_id];
-      pf_co = geo.conic_opacity[roff + pf_id];
-      pf_sg = geo.signal[roff + pf_id];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int s = k * kThreads + tid;
+      s_id[buf][s] = pf_id[k];
+      s_xy[buf][s] = pf_xy[k];
+      s_co[buf][s] = pf_co[k];
+      s_sg[buf][s] = pf_sg[k];
+      s_bb[buf][s] = pf_bb[k];
     }
-    const int cnt = min(kBlendThreads, nproc - i * kBlendThreads);
-    for (int j = 0; j < cnt; ++j) {
-      contributor--;
-      float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      bool contrib = false;
-      if (contributor < last_contributor) {
-        const float2 xy = s_xy[buf][j];
-        const float2 d = make_float2(xy.x - pixf.x, xy.y - pixf.y);
-        const float4 con_o = s_co[buf][j];
-        const float power = -0.5f * (con_o.x * d.x * d.x + con_o.z * d.y * d.y) - con_o.y * d.x * d.y;
-        const float G = expf(power);
-        const float a_raw = con_o.w * G;
-        const float alpha = fminf(0.99f, a_raw);
-        if (power <= 0.0f && alpha >= 1.0f / 255.0f) {
-          contrib = true;
-          T = T / (1.f - alpha);
-          const float dchannel_dsignal = alpha * T;
+    __syncthreads();
+    if (i + 1 < rounds) prefetch((i + 1) * kBatch);
+    const int cnt = min(kBatch, nproc - i * kBatch);
+    const int pos_base = nproc - 1 - i * kBatch;   // list position of batch entry 0
+    // Chunks of 32 entries: a ballot keeps the entries whose footprint box
+    // touches the warp's pixels and whose position is below the warp's
+    // largest contributor count; they are processed four per pass with
+    // predicated math.  T is recovered with a reciprocal taken off the
+    // dependency chain (the reference divides, backward.cu:565; the results
+    // differ by at most one rounding).
+    for (int c0 = 0; c0 < cnt; c0 += 32) {
+      const int jl = c0 + lane;
+      unsigned mask = __ballot_sync(0xffffffffu, jl < cnt && pos_base - jl < wmax &&
+                                                     !box_outside(s_bb[buf][min(jl, kBatch - 1)], wr.x0, wr.x1,
+                                                                  wr.y0, wr.y1));
+      while (mask) {
+        int js[4];
+        bool vs[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          vs[u] = mask != 0u;
+          js[u] = c0 + (vs[u] ? __ffs(mask) - 1 : 0);
+          mask &= mask - 1u;
+        }
+        float v[4][8];
+        bool contrib[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int j = js[u];
+          const float2 xy = s_xy[buf][j];
+          const float2 d = make_float2(xy.x - pixf.x, xy.y - pixf.y);
+          const float4 con_o = s_co[buf][j];
           const float2 sg = s_sg[buf][j];
+          const float power = -0.5f * (con_o.x * d.x * d.x + con_o.z * d.y * d.y) - con_o.y * d.x * d.y;
+          const float G = expf(power);
+          const float a_raw = con_o.w * G;
+          const float alpha = fminf(0.99f, a_raw);
+          const bool c = vs[u] && (pos_base - j < last_contributor) && !(power > 0.0f) &&
+                         !(alpha < 1.0f / 255.0f);
+          contrib[u] = c;
+          const float inv_one_minus = __frcp_rn(1.f - alpha);
+          const float Tn = c ? T * inv_one_minus : T;
+          const float dchannel_dsignal = alpha * Tn;
           const float sig_r = sg.x;
           const float sig_i = ref ? sg.x : sg.y;
-          acc_r = last_alpha * last_sr + (1.f - last_alpha) * acc_r;
-          acc_i = last_alpha * last_si + (1.f - last_alpha) * acc_i;
-          last_sr = sig_r;
-          last_si = sig_i;
-          float dL_dalpha = (sig_r - acc_r) * dLr;
-          if (!ref) dL_dalpha += (sig_i - acc_i) * dLi;
-          dL_dalpha *= T;
+          const float acc_rn = last_alpha * last_sr + (1.f - last_alpha) * acc_r;
+          const float acc_in = last_alpha * last_si + (1.f - last_alpha) * acc_i;
+          float dL_dalpha = (sig_r - acc_rn) * dLr;
+          if (!ref) dL_dalpha += (sig_i - acc_in) * dLi;
+          dL_dalpha *= Tn;
           if (!ref && a_raw > 0.99f) dL_dalpha = 0.0f;   // clamp blocks the gradient
-          last_alpha = alpha;
           const float dL_dG = con_o.w * dL_dalpha;
           const float gdx = G * d.x;
           const float gdy = G * d.y;
           const float dG_ddelx = -gdx * con_o.x - gdy * con_o.y;
           const float dG_ddely = -gdy * con_o.z - gdx * con_o.y;
-          v[0] = dL_dG * dG_ddelx * ddelx_dx;
-          v[1] = dL_dG * dG_ddely * ddely_dy;
-          v[2] = -0.5f * gdx * d.x * dL_dG;
-          v[3] = -0.5f * gdx * d.y * dL_dG;
-          v[4] = -0.5f * gdy * d.y * dL_dG;
-          v[5] = G * dL_dalpha;
-          v[6] = dchannel_dsignal * dLr;
-          v[7] = dchannel_dsignal * dLi;
+          v[u][0] = c ? dL_dG * dG_ddelx * ddelx_dx : 0.0f;
+          v[u][1] = c ? dL_dG * dG_ddely * ddely_dy : 0.0f;
+          v[u][2] = c ? -0.5f * gdx * d.x * dL_dG : 0.0f;
+          v[u][3] = c ? -0.5f * gdx * d.y * dL_dG : 0.0f;
+          v[u][4] = c ? -0.5f * gdy * d.y * dL_dG : 0.0f;
+          v[u][5] = c ? G * dL_dalpha : 0.0f;
+          v[u][6] = c ? dchannel_dsignal * dLr : 0.0f;
+          v[u][7] = c ? dchannel_dsignal * dLi : 0.0f;
+          if (c) {
+            T = Tn;
+            acc_r = acc_rn;
+            acc_i = acc_in;
+            last_sr = sig_r;
+            last_si = sig_i;
+            last_alpha = alpha;
+          }
         }
-      }
-      if (__any_sync(0xffffffffu, contrib)) {
-        const float z = warp_reduce8(v, lane);
-        if ((lane & 3) == 0) {
-          const int vidx = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-          atomicAdd(&s_grad[buf][j][vidx], z);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (__any_sync(0xffffffffu, contrib[u])) {
+            const float z = warp_reduce8(v[u], lane);
+            if ((lane & 3) == 0) {
+              const int vidx = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+              atomicAdd(&s_grad[buf][js[u]][vidx], z);
+            }
+          }
         }
       }
     }
     __syncthreads();
-    if (i * kBlendThreads + tid < nproc) {
-      const uint32_t g = s_id[buf][tid];
+    for (int s = tid; s < cnt; s += kThreads) {
+      const uint32_t g = s_id[buf][s];
       const size_t rg = roff + g;
       float gv[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) { gv[k] = s_grad[buf][tid][k]; s_grad[buf][tid][k] = 0.0f; }
+      for (int k = 0; k < 8; ++k) { gv[k] = s_grad[buf][s][k]; s_grad[buf][s][k] = 0.0f; }
       if (gv[0] != 0.0f) atomicAdd(dmean2D + rg * 3 + 0, gv[0]);
       if (gv[1] != 0.0f) atomicAdd(dmean2D + rg * 3 + 1, gv[1]);
       if (gv[2] != 0.0f) atomicAdd(dconic + rg * 4 + 0, gv[2]);
@@ -285,13 +382,23 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, unsigned grad_mode,
   }
 }
 
+// 64-thread CTAs (four per tile) while the launch has fewer tiles than two
+// per SM; full-tile CTAs otherwise.
+static bool use_split_tiles(int R, const TileGrid& grid) { return (long long)R * grid.T < 2 * 148; }
+
 cudaError_t launch_blend_forward(int P, int R, int H, int W, const TileGrid& grid, const GeomView& geo,
                                  const ImageView& img, const BinningView& bin, float* out_real,
                                  float* out_imag, cudaStream_t stream) {
   if (R == 0 || grid.T == 0) return cudaSuccess;
-  dim3 g(grid.gx, grid.gy, R);
-  blend_forward_kernel<<<g, kBlendThreads, 0, stream>>>(P, H, W, grid, img.ranges, bin.point_list, geo, img.hdr,
-                                                        img.final_T, img.n_contrib, out_real, out_imag);
+  if (use_split_tiles(R, grid)) {
+    dim3 g(grid.gx * (kBlendThreads / 64), grid.gy, R);
+    blend_forward_kernel<64><<<g, 64, 0, stream>>>(P, H, W, grid, img.ranges, bin.point_list, geo, img.hdr,
+                                                   img.final_T, img.n_contrib, out_real, out_imag);
+  } else {
+    dim3 g(grid.gx, grid.gy, R);
+    blend_forward_kernel<kBlendThreads><<<g, kBlendThreads, 0, stream>>>(
+        P, H, W, grid, img.ranges, bin.point_list, geo, img.hdr, img.final_T, img.n_contrib, out_real, out_imag);
+  }
   return cudaGetLastError();
 }
 
@@ -300,10 +407,17 @@ cudaError_t launch_blend_backward(int P, int R, int H, int W, const TileGrid& gr
                                   const float* dL_dout_real, const float* dL_dout_imag, float* dmean2D,
                                   float* dconic, float* dsig, float* dopac, cudaStream_t stream) {
   if (R == 0 || grid.T == 0) return cudaSuccess;
-  dim3 g(grid.gx, grid.gy, R);
-  blend_backward_kernel<<<g, kBlendThreads, 0, stream>>>(P, H, W, grid, grad_mode, img.ranges, bin.point_list, geo,
-                                                         img.hdr, img.final_T, img.n_contrib, dL_dout_real,
-                                                         dL_dout_imag, dmean2D, dconic, dsig, dopac);
+  if (use_split_tiles(R, grid)) {
+    dim3 g(grid.gx * (kBlendThreads / 64), grid.gy, R);
+    blend_backward_kernel<64><<<g, 64, 0, stream>>>(P, H, W, grid, grad_mode, img.ranges, bin.point_list, geo,
+                                                    img.hdr, img.final_T, img.n_contrib, dL_dout_real,
+                                                    dL_dout_imag, dmean2D, dconic, dsig, dopac);
+  } else {
+    dim3 g(grid.gx, grid.gy, R);
+    blend_backward_kernel<kBlendThreads><<<g, kBlendThreads, 0, stream>>>(
+        P, H, W, grid, grad_mode, img.ranges, bin.point_list, geo, img.hdr, img.final_T, img.n_contrib,
+        dL_dout_real, dL_dout_imag, dmean2D, dconic, dsig, dopac);
+  }
   return cudaGetLastError();
 }
 

@@ -4,6 +4,7 @@
 //   geometry state  [R][P]  means2D float2 | depth f32 | radii i32 |
 //                           conic_opacity float4 | signal float2 (real, imag)
 //                   [P]     cov3D 6 x f32 (receiver independent)
+//                   [R][P]  footprint box float4 (blend skipping, see below)
 //   image state     header (K, error word) | ranges uint2[R*T] |
 //                   counts u32[R*T] | cursor u32[R*T] |
 //                   final_T f32[R*H*W] | n_contrib u32[R*H*W]
@@ -58,6 +59,7 @@ struct GeomView {
   float4* conic_opacity;
   float2* signal;
   float* cov3D;
+  float4* box;   // [R][P] pixel box (x_lo, x_hi, y_lo, y_hi) outside which alpha < 1/255
 };
 
 struct ImageView {
@@ -87,9 +89,10 @@ __host__ __device__ inline size_t carve_geom(char* base, size_t P, size_t R, Geo
   char* d = take(n * sizeof(float4));
   char* e = take(n * sizeof(float2));
   char* f = take(P * 6 * sizeof(float));
+  char* g = take(n * sizeof(float4));
   if (v) {
     v->means2D = (float2*)a; v->depth = (float*)b; v->radii = (int*)c;
-    v->conic_opacity = (float4*)d; v->signal = (float2*)e; v->cov3D = (float*)f;
+    v->conic_opacity = (float4*)d; v->signal = (float2*)e; v->cov3D = (float*)f; v->box = (float4*)g;
   }
   return off;
 }
@@ -271,6 +274,37 @@ __device__ __forceinline__ Mat3 jac_mat(float J00, float J02, float J10, float J
   J.c[1][0] = J10; J.c[1][1] = J11; J.c[1][2] = J12;
   J.c[2][0] = 0.0f; J.c[2][1] = 0.0f; J.c[2][2] = 0.0f;
   return J;
+}
+
+// Conservative pixel box (x_lo, x_hi, y_lo, y_hi) of a splat: outside it
+// the blend's alpha = min(0.99, o * exp(power)) stays below 1/255, so a warp
+// whose pixels all lie outside may skip the entry without changing any result.
+//  * alpha <= o, so o < 0.99/255 never reaches 1/255: empty box;
+//  * otherwise contributing pixels satisfy Q = a dx^2 + 2 b dx dy + c dy^2 <=
+//    2 ln(255 o); the box bounds that ellipse with a 2 % + 2e-3 margin on the
+//    level and 1 % + 0.01 px on the half-widths, which covers the FP32
+//    rounding of `power` whenever the conic is not near-degenerate;
+//  * near-degenerate conics (b^2 > 0.99 ac), a non-positive determinant and
+//    non-finite values give an unbounded box (never skipped); NaN positions
+//    give NaN bounds, which every comparison treats as "do not skip".
+__device__ __forceinline__ float4 footprint_box(const float2 xy, const float4 co) {
+  const float inf = __int_as_float(0x7f800000);
+  const float l = logf(255.0f * co.w);
+  if (l < -0.01f) return make_float4(inf, -inf, inf, -inf);
+  const float q0 = fmaxf(l, 0.0f) * 2.04f + 2e-3f;
+  const float ac = co.x * co.z;
+  const float det = ac - co.y * co.y;
+  const float ex = sqrtf(q0 * co.z / det) * 1.01f + 0.01f;
+  const float ey = sqrtf(q0 * co.x / det) * 1.01f + 0.01f;
+  if (!(det > 0.0f) || !(co.y * co.y <= 0.99f * ac) || !(ex < 1e30f) || !(ey < 1e30f))
+    return make_float4(-inf, inf, -inf, inf);
+  return make_float4(xy.x - ex, xy.x + ex, xy.y - ey, xy.y + ey);
+}
+
+// True when the box lies entirely outside the pixel rectangle [x0,x1]x[y0,y1]
+// (false for NaN boxes).
+__device__ __forceinline__ bool box_outside(const float4 b, float x0, float x1, float y0, float y1) {
+  return b.y < x0 || b.x > x1 || b.w < y0 || b.z > y1;
 }
 
 __device__ __forceinline__ void atomic_or_error(ImageHeader* hdr, uint32_t bits) {

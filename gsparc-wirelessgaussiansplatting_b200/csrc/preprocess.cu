@@ -127,7 +127,9 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
           geo.signal[rg] = emission_mlp_ref(g, P, mlp, p, rx, tx);
           geo.depth[rg] = rdist;
           geo.means2D[rg] = make_float2(px, py);
-          geo.conic_opacity[rg] = make_float4(conic.x, conic.y, conic.z, __ldg(opacities + g));
+          const float4 co = make_float4(conic.x, conic.y, conic.z, __ldg(opacities + g));
+          geo.conic_opacity[rg] = co;
+          geo.box[rg] = footprint_box(make_float2(px, py), co);
         }
       }
     }
