@@ -9,10 +9,10 @@ loss, the full hand-written adjoint, Adam.  Each step uses the next receiver
 of a pool; targets are spectra of a second seeded scene at those receivers.
 Synthetic data (no dataset in the container).
 
-value: steps/s of the step captured in one CUDA graph (SplatTrainer.capture /
-step_graphed) with inputs resident in HBM; per-step CUDA events on the
+value: steps/s of the step captured in one CUDA graph (FusedTrainer: flat
+per-Gaussian state, fused activation-adjoint Adam) with inputs resident in HBM; per-step CUDA events on the
 compute stream, L2 flushed (256 MiB write) between steps outside the events.
-e2e: the same step through SplatTrainer.step_graphed with the receiver's
+e2e: the same step through FusedTrainer.step with the receiver's
 target spectrum, view matrix and position copied from pinned host memory
 every step and the loss and rasterizer status read back to the host, inside
 the timed region.  Also reported: the eager drop-in path (reference call
@@ -184,6 +184,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
     from gsparc_b200 import _lib, raster, scenes
+    from gsparc_b200.fused import FusedTrainer
     from gsparc_b200.trainer import SplatTrainer
 
     world, rank, local, group = _dist_setup()
@@ -204,7 +205,7 @@ def run_ours(args):
     views_h = torch.tensor(views).pin_memory()
     rxs_h = torch.tensor(rxs).pin_memory()
     # the product path: the whole step captured in one CUDA graph, one receiver per step
-    trainer = SplatTrainer(sc, device=dev, group=group, capturable=True)
+    trainer = FusedTrainer(sc, device=dev, group=group)
     capacity = trainer.probe_capacity(views_d, rxs_d, tx)
     trainer.capture(1, capacity, tx, views_d[0:1], rxs_d[0:1], targets_d[0:1])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -212,7 +213,7 @@ def run_ours(args):
 
     def dev_step(i):
         j = i % POOL
-        return trainer.step_graphed(views_d[j:j + 1], rxs_d[j:j + 1], targets_d[j:j + 1])
+        return trainer.step(views_d[j:j + 1], rxs_d[j:j + 1], targets_d[j:j + 1])
 
     loss_h = torch.empty((), dtype=torch.float32).pin_memory()
 
@@ -220,7 +221,7 @@ def run_ours(args):
         # target spectrum, view matrix and receiver position copied from pinned
         # host memory into the graph's inputs; loss and rasterizer status back
         j = i % POOL
-        loss = trainer.step_graphed(views_h[j:j + 1], rxs_h[j:j + 1], targets_h[j:j + 1])
+        loss = trainer.step(views_h[j:j + 1], rxs_h[j:j + 1], targets_h[j:j + 1])
         loss_h.copy_(loss, non_blocking=True)
         stream.synchronize()
         trainer.plan.check()
@@ -281,17 +282,17 @@ def run_ours(args):
     launches = sum(c for _, c in ktimes.values()) // n_eager
     dom = max(ktimes, key=lambda k: ktimes[k][0])
     # batched: every receiver of the pool in one captured step
-    btr = SplatTrainer(sc, device=dev, group=group, capturable=True)
+    btr = FusedTrainer(sc, device=dev, group=group)
     btr.capture(POOL, capacity * POOL, tx, views_d, rxs_d, targets_d)
     n_b = max(1, args.steps // 4)
-    bsec = timed(lambda i: btr.step_graphed(views_d, rxs_d, targets_d), n_b)
+    bsec = timed(lambda i: btr.step(views_d, rxs_d, targets_d), n_b)
     btr.plan.check()
     batched = {"receivers_per_step": POOL, "steps_per_s": n_b * world / bsec,
                "spectra_per_s": n_b * POOL * world / bsec}
     dom_ms = ktimes[dom][0] / ktimes[dom][1]
     # algorithmic bytes per launch of the dominant kernel
     with torch.no_grad():
-        _, _, _, st = raster.forward(trainer.centre, trainer.emission_mlps(), torch.sigmoid(trainer.opacity_logit),
+        _, _, _, st = raster.forward(trainer.centre, trainer.mlp, torch.sigmoid(trainer.opacity_logit),
                                      torch.exp(trainer.log_scale), torch.nn.functional.normalize(trainer.rotation),
                                      90, 360, 1.0, views_d[0], tx, rxs_d[0])
     K = st.num_rendered
@@ -339,8 +340,8 @@ def run_ours(args):
                 "kernel_ms_per_step": {k: v[0] / n_eager for k, v in sorted(ktimes.items())},
                 "dropin_eager_steps_per_s": dropin,
                 "batched": batched,
-                "path": "CUDA-graph-captured step (SplatTrainer.capture / step_graphed), binning capacity "
-                        f"{capacity}",
+                "path": "CUDA-graph-captured step with flat per-Gaussian state and the fused activation-adjoint "
+                        f"Adam (gsparc_b200.fused.FusedTrainer), binning capacity {capacity}",
                 "cpu_baseline": cpu_base}
         print(json.dumps(line))
     if group is not None:

@@ -43,12 +43,13 @@ bool valid_tile(int th, int tw) {
 // ---- optional per-kernel timing (CUDA events around each launch) ----------
 enum KernelId {
   KID_PREPROCESS, KID_SCAN, KID_CHECK, KID_SCATTER, KID_SEGSORT, KID_BLEND_FWD, KID_BLEND_BWD,
-  KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_COUNT
+  KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_ADAM, KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
     "preprocess_kernel", "scan_segments_kernel", "check_capacity_kernel", "scatter_kernel",
     "segment_sort_kernel", "blend_forward_kernel", "blend_backward_kernel", "geometry_backward_kernel",
-    "emission_backward_kernel", "ssim_forward_kernel", "ssim_backward_kernel", "mark_visible_kernel"};
+    "emission_backward_kernel", "ssim_forward_kernel", "ssim_backward_kernel", "mark_visible_kernel",
+    "gaussian_adam_kernels"};
 
 struct PendingTiming {
   int id;
@@ -340,6 +341,37 @@ int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float C2, const 
   GS_CHECK(launch_ssim_backward(B * CH, H, W, img1, img2, dL_dmap, dm_dmu1, dm_dsigma1_sq, dm_dsigma12, dL_dimg1,
                                 (cudaStream_t)stream),
            "ssim backward");
+  return GSPARC_OK;
+}
+
+// ---- fused optimizer ---------------------------------------------------------
+
+size_t gsparc_gaussian_state_floats(int P) {
+  if (P < 0) return 0;
+  return gaussian_layout((size_t)P).total;
+}
+
+int gsparc_gaussian_state_layout(int P, size_t* offsets5) {
+  if (P < 0 || !offsets5) return invalid("gaussian state layout");
+  const GaussianLayout L = gaussian_layout((size_t)P);
+  offsets5[0] = L.centre; offsets5[1] = L.scale; offsets5[2] = L.quat; offsets5[3] = L.opacity; offsets5[4] = L.mlp;
+  return GSPARC_OK;
+}
+
+int gsparc_gaussian_adam_step(int P, float* params, const float* grads, float* exp_avg, float* exp_avg_sq,
+                              float* step_count, const float* lr5, float beta1, float beta2, float eps,
+                              const float* centre_lo3, const float* centre_hi3, void* stream) {
+  if (P < 0) return invalid("P");
+  if (!step_count || !lr5 || !centre_lo3 || !centre_hi3) return invalid("null step, learning-rate or clamp pointer");
+  if (P > 0 && (!params || !grads || !exp_avg || !exp_avg_sq)) return invalid("null state pointer");
+  if ((((uintptr_t)params) | ((uintptr_t)grads) | ((uintptr_t)exp_avg) | ((uintptr_t)exp_avg_sq)) & 15u)
+    return invalid("state buffers must be 16-byte aligned");
+  if (!(beta1 >= 0.f && beta1 < 1.f && beta2 >= 0.f && beta2 < 1.f && eps >= 0.f)) return invalid("Adam betas/eps");
+  cudaStream_t s = (cudaStream_t)stream;
+  Timed t(KID_ADAM, s);
+  GS_CHECK(launch_gaussian_adam(P, params, grads, exp_avg, exp_avg_sq, step_count, lr5, beta1, beta2, eps, centre_lo3,
+                                centre_hi3, s),
+           "gaussian adam");
   return GSPARC_OK;
 }
 

@@ -123,6 +123,24 @@ __host__ __device__ inline size_t carve_binning(char* base, size_t K, BinningVie
   return off;
 }
 
+// Flat per-Gaussian training state (parameters, gradients, Adam moments):
+// segments in float units, each starting on a 256-byte boundary.
+struct GaussianLayout {
+  size_t centre, scale, quat, opacity, mlp, total;
+};
+
+__host__ __device__ inline GaussianLayout gaussian_layout(size_t P) {
+  auto a = [](size_t x) { return (x + 63) / 64 * 64; };
+  GaussianLayout L;
+  L.centre = 0;
+  L.scale = a(3 * P);
+  L.quat = L.scale + a(3 * P);
+  L.opacity = L.quat + a(4 * P);
+  L.mlp = L.opacity + a(P);
+  L.total = L.mlp + a((size_t)kMlpFloats * P);
+  return L;
+}
+
 // ---------------------------------------------------------------------------
 // Projection math.  The float expression order of every helper below is kept
 // identical to the reference kernels (cited per function) so the integer

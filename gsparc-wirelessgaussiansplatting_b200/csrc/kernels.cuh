@@ -47,6 +47,10 @@ cudaError_t launch_emission_backward(int P, int R, const float* means3D, const f
                                      const float* rx_pos, const int* radii, const float* dsig, float* dL_dmlp,
                                      float* dL_dmeans3D, cudaStream_t stream);
 
+cudaError_t launch_gaussian_adam(int P, float* params, const float* grads, float* m, float* v, float* step,
+                                 const float* lr5, float beta1, float beta2, float eps, const float* lo3,
+                                 const float* hi3, cudaStream_t stream);
+
 cudaError_t launch_ssim_forward(int planes, int H, int W, float C1, float C2, const float* img1, const float* img2,
                                 float* map, float* dmu1, float* ds11, float* ds12, cudaStream_t stream);
 

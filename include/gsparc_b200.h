@@ -178,6 +178,33 @@ GSPARC_API int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float
                          const float* dm_dmu1, const float* dm_dsigma1_sq,
                          const float* dm_dsigma12, float* dL_dimg1, void* stream);
 
+/* ---- fused optimizer over the per-Gaussian parameters ------------------- */
+
+/* Floats in a flat per-Gaussian training-state buffer for P Gaussians, and
+ * the float offsets of its five segments (centre [P,3], log-scale [P,3],
+ * quaternion [P,4], opacity logit [P], emission MLP [194*P] in the layout of
+ * EmissionMLPs.get_all_params); each segment starts on a 256-byte boundary. */
+GSPARC_API size_t gsparc_gaussian_state_floats(int P);
+GSPARC_API int gsparc_gaussian_state_layout(int P, size_t* offsets5);
+
+/* One Adam step (torch's update rule) over all per-Gaussian parameters,
+ * fused with the adjoints of their activations.  Replaces the
+ * torch.optim.Adam step over GaussianModel's parameter groups
+ * (gaussian.py:176-197) together with the autograd of the activations
+ * exp / normalize / sigmoid (gaussian.py:33-38), the NaN-zeroing of the
+ * centre gradient (train.py:443-445) and the centre clamp (train.py:556-562).
+ * params, exp_avg, exp_avg_sq: flat state buffers (raw parameters), updated in
+ * place; grads: same layout, gradients with respect to the ACTIVATED values
+ * (as gsparc_rasterize_backward returns them); step_count: device float,
+ * incremented by this call; lr5: device floats (centre, scale, rotation,
+ * opacity, MLP); centre_lo3 / centre_hi3: device clamp box.  All buffers
+ * 16-byte aligned. */
+GSPARC_API int gsparc_gaussian_adam_step(int P, float* params, const float* grads, float* exp_avg,
+                                         float* exp_avg_sq, float* step_count, const float* lr5,
+                                         float beta1, float beta2, float eps,
+                                         const float* centre_lo3, const float* centre_hi3,
+                                         void* stream);
+
 /* SSIM map and dL/dimg1 in one call that allocates nothing.  No counterpart
  * in the reference.  For callers that cannot call cudaMalloc (for example a
  * real-time receiver loop that cannot absorb cudaMalloc's implicit device
