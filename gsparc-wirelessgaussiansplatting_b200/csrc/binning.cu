@@ -128,8 +128,24 @@ scatter_kernel(int P, TileGrid grid, GeomView geo, uint32_t* __restrict__ cursor
 }
 
 // ---- per-segment sort -------------------------------------------------------
+// Two launches over all segments; each CTA returns at once unless its segment
+// belongs to its size class:
+//  * small (n <= kSmallCap): bitonic network in shared memory, 256 threads,
+//    many CTAs per SM;
+//  * large: each of 512 threads sorts 16 keys in registers, then merge-path
+//    merges in shared memory (9 levels for 8192 keys -- far less shared-memory
+//    traffic than a bitonic network's 91 passes); segments above kSortCap are
+//    sorted in kSortCap chunks and merged through global memory.
+constexpr int kSmallThreads = 256;
+constexpr int kSmallCap = 2048;
 constexpr int kSortThreads = 512;
-constexpr int kSortCap = 8192;   // keys per shared-memory sort (64 KB)
+constexpr int kPerThread = 16;
+constexpr int kSortCap = kSortThreads * kPerThread;   // 8192 keys
+// Shared-memory index with one pad slot per 16 keys: thread t's run
+// [16t, 16t+16) then starts at 17t, so a warp's strided accesses spread over
+// the banks (2-way) instead of all landing on one (32-way).
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
+constexpr int kPadded = kSortCap + kSortCap / 16;    // 8704 keys per buffer, 2 x 68 KB
 
 __device__ __forceinline__ void bitonic_sort_shared(unsigned long long* s, int npad) {
   for (int k = 2; k <= npad; k <<= 1) {
@@ -150,6 +166,71 @@ __device__ __forceinline__ int next_pow2(int n) {
   int p = 1;
   while (p < n) p <<= 1;
   return p;
+}
+
+// Sorting network over a register array (all indices compile-time).
+template <int N>
+__device__ __forceinline__ void register_bitonic(unsigned long long (&a)[N]) {
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        const int l = i ^ j;
+        if (l > i) {
+          const bool up = (i & k) == 0;
+          const unsigned long long x = a[i], y = a[l];
+          const bool sw = (x > y) == up;
+          a[i] = sw ? y : x;
+          a[l] = sw ? x : y;
+        }
+      }
+}
+
+// Sort kSortCap keys held in `a` (shared memory, pidx layout, padded with ~0)
+// using `b` as the second buffer; returns the buffer holding the result.
+__device__ unsigned long long* merge_sort_shared(unsigned long long* a, unsigned long long* b) {
+  const int t = threadIdx.x;
+  {
+    unsigned long long r[kPerThread];
+#pragma unroll
+    for (int k = 0; k < kPerThread; ++k) r[k] = a[pidx(t * kPerThread + k)];
+    register_bitonic<kPerThread>(r);
+#pragma unroll
+    for (int k = 0; k < kPerThread; ++k) a[pidx(t * kPerThread + k)] = r[k];
+  }
+  __syncthreads();
+  unsigned long long* src = a;
+  unsigned long long* dst = b;
+  for (int width = kPerThread; width < kSortCap; width <<= 1) {
+    const int out0 = t * kPerThread;
+    const int base = (out0 / (2 * width)) * (2 * width);
+    const int a0 = base, b0 = base + width;   // run starts (logical indices)
+    const int d = out0 - base;
+    // merge path: number of A elements among the first d outputs (A wins ties)
+    int lo = max(0, d - width), hi = min(d, width);
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (src[pidx(a0 + mid)] <= src[pidx(b0 + d - 1 - mid)]) lo = mid + 1;
+      else hi = mid;
+    }
+    int i = lo, j = d - lo;
+#pragma unroll
+    for (int k = 0; k < kPerThread; ++k) {
+      const unsigned long long x = i < width ? src[pidx(a0 + i)] : ~0ull;
+      const unsigned long long y = j < width ? src[pidx(b0 + j)] : ~0ull;
+      const bool take_a = (j >= width) || (i < width && x <= y);
+      dst[pidx(out0 + k)] = take_a ? x : y;
+      i += take_a ? 1 : 0;
+      j += take_a ? 0 : 1;
+    }
+    __syncthreads();
+    unsigned long long* tmp = src;
+    src = dst;
+    dst = tmp;
+  }
+  return src;
 }
 
 // Merge two sorted runs a[0:na), b[0:nb) into out[0:na+nb) with one CTA
@@ -174,36 +255,53 @@ __device__ void merge_runs_cta(const unsigned long long* __restrict__ a, int na,
   }
 }
 
-__global__ void __launch_bounds__(kSortThreads)
-segment_sort_kernel(const uint2* __restrict__ ranges, const ImageHeader* __restrict__ hdr,
-                    unsigned long long* __restrict__ keys, unsigned long long* __restrict__ keys_alt,
-                    uint32_t* __restrict__ point_list) {
+__global__ void __launch_bounds__(kSmallThreads)
+segment_sort_small_kernel(const uint2* __restrict__ ranges, const ImageHeader* __restrict__ hdr,
+                          const unsigned long long* __restrict__ keys, uint32_t* __restrict__ point_list) {
   if (hdr->error) return;
-  extern __shared__ unsigned long long skeys[];
+  __shared__ unsigned long long skeys[kSmallCap];
   const uint2 rg = ranges[blockIdx.x];
   const int n = (int)(rg.y - rg.x);
-  if (n <= 0) return;
-  unsigned long long* seg = keys + rg.x;
+  if (n <= 0 || n > kSmallCap) return;
+  const unsigned long long* seg = keys + rg.x;
   if (n == 1) {
     if (threadIdx.x == 0) point_list[rg.x] = (uint32_t)seg[0];
     return;
   }
+  const int npad = next_pow2(n);
+  for (int i = threadIdx.x; i < npad; i += blockDim.x) skeys[i] = i < n ? seg[i] : ~0ull;
+  __syncthreads();
+  bitonic_sort_shared(skeys, npad);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) point_list[rg.x + i] = (uint32_t)skeys[i];
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+segment_sort_large_kernel(const uint2* __restrict__ ranges, const ImageHeader* __restrict__ hdr,
+                          unsigned long long* __restrict__ keys, unsigned long long* __restrict__ keys_alt,
+                          uint32_t* __restrict__ point_list) {
+  if (hdr->error) return;
+  extern __shared__ unsigned long long smem[];
+  unsigned long long* sa = smem;
+  unsigned long long* sb = smem + kPadded;
+  const uint2 rg = ranges[blockIdx.x];
+  const int n = (int)(rg.y - rg.x);
+  if (n <= kSmallCap) return;
+  unsigned long long* seg = keys + rg.x;
   if (n <= kSortCap) {
-    const int npad = next_pow2(n);
-    for (int i = threadIdx.x; i < npad; i += blockDim.x) skeys[i] = i < n ? seg[i] : ~0ull;
+    for (int i = threadIdx.x; i < kSortCap; i += blockDim.x) sa[pidx(i)] = i < n ? seg[i] : ~0ull;
     __syncthreads();
-    bitonic_sort_shared(skeys, npad);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) point_list[rg.x + i] = (uint32_t)skeys[i];
+    const unsigned long long* res = merge_sort_shared(sa, sb);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) point_list[rg.x + i] = (uint32_t)res[pidx(i)];
     return;
   }
-  // large segment: sort kSortCap-sized chunks in shared memory, then merge
-  // pairs of runs through global memory, ping-ponging keys <-> keys_alt
+  // above kSortCap: sort chunks in shared memory, then merge runs through
+  // global memory, ping-ponging keys <-> keys_alt
   for (int c0 = 0; c0 < n; c0 += kSortCap) {
     const int cn = min(kSortCap, n - c0);
-    for (int i = threadIdx.x; i < kSortCap; i += blockDim.x) skeys[i] = i < cn ? seg[c0 + i] : ~0ull;
+    for (int i = threadIdx.x; i < kSortCap; i += blockDim.x) sa[pidx(i)] = i < cn ? seg[c0 + i] : ~0ull;
     __syncthreads();
-    bitonic_sort_shared(skeys, kSortCap);
-    for (int i = threadIdx.x; i < cn; i += blockDim.x) seg[c0 + i] = skeys[i];
+    const unsigned long long* res = merge_sort_shared(sa, sb);
+    for (int i = threadIdx.x; i < cn; i += blockDim.x) seg[c0 + i] = res[pidx(i)];
     __syncthreads();
   }
   unsigned long long* src = seg;
@@ -215,7 +313,9 @@ segment_sort_kernel(const uint2* __restrict__ ranges, const ImageHeader* __restr
       merge_runs_cta(src + lo, na, src + lo + na, nb, dst + lo);
     }
     __syncthreads();
-    unsigned long long* t = src; src = dst; dst = t;
+    unsigned long long* t = src;
+    src = dst;
+    dst = t;
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) point_list[rg.x + i] = (uint32_t)src[i];
 }
@@ -244,22 +344,26 @@ cudaError_t launch_scatter(int P, int R, const TileGrid& grid, const GeomView& g
 }
 
 cudaError_t launch_segment_sort(int R, const TileGrid& grid, ImageView img, BinningView bin, cudaStream_t stream) {
-  const size_t sort_smem = (size_t)kSortCap * sizeof(unsigned long long);
+  const size_t sort_smem = 2 * (size_t)kPadded * sizeof(unsigned long long);
   // set the shared-memory opt-in once per device, so later calls (including
-  // ones made while a CUDA graph is being captured) only enqueue the launch
+  // ones made while a CUDA graph is being captured) only enqueue the launches
   static bool attr_done[64] = {false};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64 || !attr_done[dev]) {
-    e = cudaFuncSetAttribute(segment_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem);
+    e = cudaFuncSetAttribute(segment_sort_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sort_smem);
     if (e != cudaSuccess) return e;
     if (dev >= 0 && dev < 64) attr_done[dev] = true;
   }
   const int nseg = R * grid.T;
-  if (nseg > 0)
-    segment_sort_kernel<<<nseg, kSortThreads, sort_smem, stream>>>(img.ranges, img.hdr, bin.keys, bin.keys_alt,
-                                                                  bin.point_list);
+  if (nseg == 0) return cudaSuccess;
+  segment_sort_small_kernel<<<nseg, kSmallThreads, 0, stream>>>(img.ranges, img.hdr, bin.keys, bin.point_list);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  segment_sort_large_kernel<<<nseg, kSortThreads, sort_smem, stream>>>(img.ranges, img.hdr, bin.keys, bin.keys_alt,
+                                                                      bin.point_list);
   return cudaGetLastError();
 }
 
