@@ -6,6 +6,7 @@
 // and of one backward:
 //   memset(accumulated grads) -> blend adjoint -> geometry adjoint
 //   -> emission-MLP adjoint.
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -43,13 +44,14 @@ bool valid_tile(int th, int tw) {
 // ---- optional per-kernel timing (CUDA events around each launch) ----------
 enum KernelId {
   KID_PREPROCESS, KID_SCAN, KID_CHECK, KID_SCATTER, KID_SEGSORT, KID_BLEND_FWD, KID_BLEND_BWD,
-  KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_ADAM, KID_COUNT
+  KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_ADAM, KID_LOSS, KID_ACTIVATE,
+  KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
     "preprocess_kernel", "scan_segments_kernel", "check_capacity_kernel", "scatter_kernel",
     "segment_sort_kernel", "blend_forward_kernel", "blend_backward_kernel", "geometry_backward_kernel",
     "emission_backward_kernel", "ssim_forward_kernel", "ssim_backward_kernel", "mark_visible_kernel",
-    "gaussian_adam_kernels"};
+    "gaussian_adam_kernels", "splat_loss_kernels", "gaussian_activate_kernel"};
 
 struct PendingTiming {
   int id;
@@ -103,7 +105,7 @@ int report_cuda(cudaError_t e, const char* where) { return cuda_fail(e, where); 
 
 extern "C" {
 
-int gsparc_abi_version(void) { return 1; }
+int gsparc_abi_version(void) { return 2; }
 
 const char* gsparc_status_string(int status) {
   switch (status) {
@@ -344,33 +346,75 @@ int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float C2, const 
   return GSPARC_OK;
 }
 
-// ---- fused optimizer ---------------------------------------------------------
+// ---- training loss -------------------------------------------------------------
 
-size_t gsparc_gaussian_state_floats(int P) {
-  if (P < 0) return 0;
-  return gaussian_layout((size_t)P).total;
+size_t gsparc_splat_loss_scratch_floats(int R, int H, int W, int hidden) {
+  if (R < 0 || H < 0 || W < 0 || hidden < 0) return 0;
+  return loss_layout((size_t)R, (size_t)H, (size_t)W, (size_t)hidden).total;
 }
 
-int gsparc_gaussian_state_layout(int P, size_t* offsets5) {
-  if (P < 0 || !offsets5) return invalid("gaussian state layout");
-  const GaussianLayout L = gaussian_layout((size_t)P);
-  offsets5[0] = L.centre; offsets5[1] = L.scale; offsets5[2] = L.quat; offsets5[3] = L.opacity; offsets5[4] = L.mlp;
+int gsparc_splat_loss(int R, int H, int W, int hidden, float lambda1, float alpha, float C1, float C2,
+                      const float* pred, const float* target, const float* rx_pos, const float* conf_params,
+                      float* scratch, float* loss_out, float* terms, float* dL_dpred, float* dL_dconf_params,
+                      void* stream) {
+  if (R < 1 || H < 1 || W < 1) return invalid("R, H and W must be positive");
+  if (R > 65535 || (H + 7) / 8 > 65535) return invalid("R or H too large for the tile grid");
+  if ((size_t)H * W > (size_t)INT32_MAX) return invalid("H*W too large");
+  if (hidden < 1 || hidden > 4096) return invalid("hidden must be in [1, 4096]");
+  if (!pred || !target || !rx_pos || !conf_params || !scratch || !loss_out || !dL_dpred || !dL_dconf_params)
+    return invalid("null pointer");
+  if (((uintptr_t)scratch) & 15u) return invalid("scratch must be 16-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  Timed t(KID_LOSS, s);
+  GS_CHECK(launch_splat_loss(R, H, W, hidden, lambda1, alpha, C1, C2, pred, target, rx_pos, conf_params, scratch,
+                             loss_out, terms, dL_dpred, dL_dconf_params, s),
+           "splat loss");
   return GSPARC_OK;
 }
 
-int gsparc_gaussian_adam_step(int P, float* params, const float* grads, float* exp_avg, float* exp_avg_sq,
-                              float* step_count, const float* lr5, float beta1, float beta2, float eps,
-                              const float* centre_lo3, const float* centre_hi3, void* stream) {
+// ---- fused optimizer ---------------------------------------------------------
+
+size_t gsparc_gaussian_state_floats(int P, int conf_floats) {
+  if (P < 0 || conf_floats < 0) return 0;
+  return gaussian_layout((size_t)P, (size_t)conf_floats).total;
+}
+
+int gsparc_gaussian_state_layout(int P, int conf_floats, size_t* offsets6) {
+  if (P < 0 || conf_floats < 0 || !offsets6) return invalid("gaussian state layout");
+  const GaussianLayout L = gaussian_layout((size_t)P, (size_t)conf_floats);
+  offsets6[0] = L.centre; offsets6[1] = L.scale; offsets6[2] = L.quat; offsets6[3] = L.opacity;
+  offsets6[4] = L.mlp; offsets6[5] = L.conf;
+  return GSPARC_OK;
+}
+
+int gsparc_gaussian_activate(int P, const float* params, float* scales, float* rotations, float* opacities,
+                             void* stream) {
   if (P < 0) return invalid("P");
-  if (!step_count || !lr5 || !centre_lo3 || !centre_hi3) return invalid("null step, learning-rate or clamp pointer");
-  if (P > 0 && (!params || !grads || !exp_avg || !exp_avg_sq)) return invalid("null state pointer");
+  if (P == 0) return GSPARC_OK;
+  if (!params || !scales || !rotations || !opacities) return invalid("null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  Timed t(KID_ACTIVATE, s);
+  GS_CHECK(launch_gaussian_activate(P, params, scales, rotations, opacities, s), "gaussian activate");
+  return GSPARC_OK;
+}
+
+int gsparc_gaussian_adam_step(int P, int conf_floats, float* params, const float* grads, float* exp_avg,
+                              float* exp_avg_sq, float* step_count, const float* lr6, float beta1, float beta2,
+                              float eps, const float* centre_lo3, const float* centre_hi3, float* scales,
+                              float* rotations, float* opacities, void* stream) {
+  if (P < 0 || conf_floats < 0) return invalid("P or conf_floats");
+  if (!step_count || !lr6 || !centre_lo3 || !centre_hi3) return invalid("null step, learning-rate or clamp pointer");
+  if ((P > 0 || conf_floats > 0) && (!params || !grads || !exp_avg || !exp_avg_sq))
+    return invalid("null state pointer");
   if ((((uintptr_t)params) | ((uintptr_t)grads) | ((uintptr_t)exp_avg) | ((uintptr_t)exp_avg_sq)) & 15u)
     return invalid("state buffers must be 16-byte aligned");
+  const int n_act = (scales != nullptr) + (rotations != nullptr) + (opacities != nullptr);
+  if (n_act != 0 && n_act != 3) return invalid("activation outputs: give all three or none");
   if (!(beta1 >= 0.f && beta1 < 1.f && beta2 >= 0.f && beta2 < 1.f && eps >= 0.f)) return invalid("Adam betas/eps");
   cudaStream_t s = (cudaStream_t)stream;
   Timed t(KID_ADAM, s);
-  GS_CHECK(launch_gaussian_adam(P, params, grads, exp_avg, exp_avg_sq, step_count, lr5, beta1, beta2, eps, centre_lo3,
-                                centre_hi3, s),
+  GS_CHECK(launch_gaussian_adam(P, conf_floats, params, grads, exp_avg, exp_avg_sq, step_count, lr6, beta1, beta2,
+                                eps, centre_lo3, centre_hi3, scales, rotations, opacities, s),
            "gaussian adam");
   return GSPARC_OK;
 }

@@ -126,10 +126,12 @@ __host__ __device__ inline size_t carve_binning(char* base, size_t K, BinningVie
 // Flat per-Gaussian training state (parameters, gradients, Adam moments):
 // segments in float units, each starting on a 256-byte boundary.
 struct GaussianLayout {
-  size_t centre, scale, quat, opacity, mlp, total;
+  size_t centre, scale, quat, opacity, mlp, conf, total;
 };
 
-__host__ __device__ inline GaussianLayout gaussian_layout(size_t P) {
+// conf_floats: size of the trailing segment for a global (not per-Gaussian)
+// parameter block such as the confidence MLP; 0 for none.
+__host__ __device__ inline GaussianLayout gaussian_layout(size_t P, size_t conf_floats = 0) {
   auto a = [](size_t x) { return (x + 63) / 64 * 64; };
   GaussianLayout L;
   L.centre = 0;
@@ -137,9 +139,15 @@ __host__ __device__ inline GaussianLayout gaussian_layout(size_t P) {
   L.quat = L.scale + a(3 * P);
   L.opacity = L.quat + a(4 * P);
   L.mlp = L.opacity + a(P);
-  L.total = L.mlp + a((size_t)kMlpFloats * P);
+  L.conf = L.mlp + a((size_t)kMlpFloats * P);
+  L.total = L.conf + a(conf_floats);
   return L;
 }
+
+// Scratch of the fused training loss (ssim.cu), in floats.
+struct LossLayout {
+  size_t nblk, dmu1, ds11, ds12, partial, pre, coef, total;
+};
 
 // ---------------------------------------------------------------------------
 // Projection math.  The float expression order of every helper below is kept

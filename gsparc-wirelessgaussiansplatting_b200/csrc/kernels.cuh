@@ -47,9 +47,20 @@ cudaError_t launch_emission_backward(int P, int R, const float* means3D, const f
                                      const float* rx_pos, const int* radii, const float* dsig, float* dL_dmlp,
                                      float* dL_dmeans3D, cudaStream_t stream);
 
-cudaError_t launch_gaussian_adam(int P, float* params, const float* grads, float* m, float* v, float* step,
-                                 const float* lr5, float beta1, float beta2, float eps, const float* lo3,
-                                 const float* hi3, cudaStream_t stream);
+cudaError_t launch_gaussian_adam(int P, int conf_floats, float* params, const float* grads, float* m, float* v,
+                                 float* step, const float* lr6, float beta1, float beta2, float eps,
+                                 const float* lo3, const float* hi3, float* act_scales, float* act_rots,
+                                 float* act_opac, cudaStream_t stream);
+
+cudaError_t launch_gaussian_activate(int P, const float* params, float* act_scales, float* act_rots,
+                                     float* act_opac, cudaStream_t stream);
+
+LossLayout loss_layout(size_t R, size_t H, size_t W, size_t hidden);
+
+cudaError_t launch_splat_loss(int R, int H, int W, int hidden, float lambda1, float alpha, float C1, float C2,
+                              const float* pred, const float* target, const float* rx, const float* conf_params,
+                              float* scratch, float* loss_out, float* terms, float* dL_dpred, float* dconf,
+                              cudaStream_t stream);
 
 cudaError_t launch_ssim_forward(int planes, int H, int W, float C1, float C2, const float* img1, const float* img2,
                                 float* map, float* dmu1, float* ds11, float* ds12, cudaStream_t stream);

@@ -178,31 +178,71 @@ GSPARC_API int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float
                          const float* dm_dmu1, const float* dm_dsigma1_sq,
                          const float* dm_dsigma12, float* dL_dimg1, void* stream);
 
+/* ---- training loss ------------------------------------------------------ */
+
+/* Scratch floats gsparc_splat_loss needs for R spectra of H x W and a
+ * confidence MLP with `hidden` units. */
+GSPARC_API size_t gsparc_splat_loss_scratch_floats(int R, int H, int W, int hidden);
+
+/* The training loss of train.py:420-436 and its adjoint in one call, for R
+ * spectra at once (the loss of a batch is the mean over its receivers):
+ *   l1_r   = mean |pred_r - target_r|                 (utils.py:40-41)
+ *   ssim_r = mean fused-SSIM map, "same" padding      (train.py:423)
+ *   recon_r = (1 - lambda1) l1_r + lambda1 (1 - ssim_r)
+ *   conf_r = 1 + exp(fc2(relu(fc1(rx_pos_r))))        (ConfidenceMLP,
+ *                                                      gaussian.py:575-609)
+ *   loss   = mean_r (conf_r recon_r - alpha log conf_r)
+ * Replaces l1_loss + fused_ssim + the confidence head and their autograd.
+ * pred, target, dL_dpred: [R,H,W]; rx_pos: [R,3]; conf_params: the MLP's
+ * parameters flat in nn.Module order (fc1.weight [hidden,3], fc1.bias
+ * [hidden], fc2.weight [1,hidden], fc2.bias [1]: 5*hidden+1 floats);
+ * dL_dconf_params: same layout, overwritten; loss_out: 1 float; terms:
+ * optional [R,4] (l1, ssim, conf, loss_r); scratch: 16-byte aligned,
+ * gsparc_splat_loss_scratch_floats floats.  All device memory. */
+GSPARC_API int gsparc_splat_loss(int R, int H, int W, int hidden, float lambda1, float alpha,
+                                 float C1, float C2, const float* pred, const float* target,
+                                 const float* rx_pos, const float* conf_params, float* scratch,
+                                 float* loss_out, float* terms, float* dL_dpred,
+                                 float* dL_dconf_params, void* stream);
+
 /* ---- fused optimizer over the per-Gaussian parameters ------------------- */
 
-/* Floats in a flat per-Gaussian training-state buffer for P Gaussians, and
- * the float offsets of its five segments (centre [P,3], log-scale [P,3],
- * quaternion [P,4], opacity logit [P], emission MLP [194*P] in the layout of
- * EmissionMLPs.get_all_params); each segment starts on a 256-byte boundary. */
-GSPARC_API size_t gsparc_gaussian_state_floats(int P);
-GSPARC_API int gsparc_gaussian_state_layout(int P, size_t* offsets5);
+/* Floats in a flat training-state buffer for P Gaussians plus a global block
+ * of conf_floats floats (the confidence MLP; 0 for none), and the float
+ * offsets of its six segments: centre [P,3], log-scale [P,3], quaternion
+ * [P,4], opacity logit [P], emission MLP [194*P] in the layout of
+ * EmissionMLPs.get_all_params, global block [conf_floats].  Each segment
+ * starts on a 256-byte boundary; the padding between segments must stay
+ * zero in the gradient buffer. */
+GSPARC_API size_t gsparc_gaussian_state_floats(int P, int conf_floats);
+GSPARC_API int gsparc_gaussian_state_layout(int P, int conf_floats, size_t* offsets6);
 
-/* One Adam step (torch's update rule) over all per-Gaussian parameters,
- * fused with the adjoints of their activations.  Replaces the
- * torch.optim.Adam step over GaussianModel's parameter groups
+/* Activated per-Gaussian values of a flat state buffer (gaussian.py:33-38):
+ * scales [P,3] = exp(log-scale), rotations [P,4] = normalize(quaternion),
+ * opacities [P] = sigmoid(logit). */
+GSPARC_API int gsparc_gaussian_activate(int P, const float* params, float* scales, float* rotations,
+                                        float* opacities, void* stream);
+
+/* One Adam step (torch's update rule) over the whole flat state, fused with
+ * the adjoints of the activations.  Replaces the torch.optim.Adam step over
+ * GaussianModel's parameter groups and the confidence MLP's
  * (gaussian.py:176-197) together with the autograd of the activations
  * exp / normalize / sigmoid (gaussian.py:33-38), the NaN-zeroing of the
  * centre gradient (train.py:443-445) and the centre clamp (train.py:556-562).
  * params, exp_avg, exp_avg_sq: flat state buffers (raw parameters), updated in
  * place; grads: same layout, gradients with respect to the ACTIVATED values
- * (as gsparc_rasterize_backward returns them); step_count: device float,
- * incremented by this call; lr5: device floats (centre, scale, rotation,
- * opacity, MLP); centre_lo3 / centre_hi3: device clamp box.  All buffers
+ * (as gsparc_rasterize_backward returns them) and, in the global block, with
+ * respect to its parameters; step_count: device float, incremented by this
+ * call; lr6: device floats (centre, scale, rotation, opacity, emission MLP,
+ * global block); centre_lo3 / centre_hi3: device clamp box.  scales,
+ * rotations, opacities: optional (all or none) outputs of the activated
+ * updated parameters, as gsparc_gaussian_activate writes them.  State buffers
  * 16-byte aligned. */
-GSPARC_API int gsparc_gaussian_adam_step(int P, float* params, const float* grads, float* exp_avg,
-                                         float* exp_avg_sq, float* step_count, const float* lr5,
-                                         float beta1, float beta2, float eps,
+GSPARC_API int gsparc_gaussian_adam_step(int P, int conf_floats, float* params, const float* grads,
+                                         float* exp_avg, float* exp_avg_sq, float* step_count,
+                                         const float* lr6, float beta1, float beta2, float eps,
                                          const float* centre_lo3, const float* centre_hi3,
+                                         float* scales, float* rotations, float* opacities,
                                          void* stream);
 
 /* SSIM map and dL/dimg1 in one call that allocates nothing.  No counterpart

@@ -86,6 +86,10 @@ def test_fused_trainer_matches_autograd_trainer():
         torch.cuda.synchronize()
         fz.plan.check()
         assert abs(le - lf) <= 1e-4 * abs(le)
+    # the activated rasterizer inputs the optimizer wrote for the next step
+    torch.testing.assert_close(fz.act_scales, torch.exp(fz.log_scale), rtol=2e-7, atol=0)
+    torch.testing.assert_close(fz.act_rots, torch.nn.functional.normalize(fz.rotation), rtol=4e-7, atol=1e-7)
+    torch.testing.assert_close(fz.act_opac, torch.sigmoid(fz.opacity_logit), rtol=2e-7, atol=0)
     raw = fz.raw_parameters()
     pairs = [(ref.centre, raw["centre"]), (ref.log_scale, raw["log_scale"]), (ref.rotation, raw["rotation"]),
              (ref.opacity_logit, raw["opacity_logit"]), (ref.fc1_w, raw["fc1_w"]), (ref.fc1_b, raw["fc1_b"]),
