@@ -20,46 +20,61 @@
 
 namespace gsparc {
 
-// ---- scan of per-segment counts -> ranges, cursors, K ----------------------
+// ---- scan of per-segment counts -> ranges, cursors, K, chunk bases ---------
 // One block; n = R*T segments (a few thousand at most for a spectrum batch).
+
+// Exclusive scan of one value per thread over the 1024-thread block; every
+// thread also receives the block total.
+__device__ __forceinline__ unsigned long long block_exclusive_scan(unsigned long long local,
+                                                                   unsigned long long* warp_tot,
+                                                                   unsigned long long& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned long long incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_tot[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    unsigned long long w = warp_tot[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long v = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += v;
+    }
+    warp_tot[lane] = w;   // inclusive over warps
+  }
+  __syncthreads();
+  const unsigned long long excl = (wid ? warp_tot[wid - 1] : 0ull) + (incl - local);
+  total = warp_tot[31];
+  __syncthreads();
+  return excl;
+}
+
 __global__ void __launch_bounds__(1024)
 scan_segments_kernel(int n, const uint32_t* __restrict__ counts, uint2* __restrict__ ranges,
-                     uint32_t* __restrict__ cursor, ImageHeader* __restrict__ hdr) {
+                     uint32_t* __restrict__ cursor, uint32_t* __restrict__ chunk_base,
+                     ImageHeader* __restrict__ hdr) {
   __shared__ unsigned long long warp_tot[32];
-  __shared__ unsigned long long carry;
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  if (tid == 0) carry = 0;
-  __syncthreads();
+  const int tid = threadIdx.x;
+  unsigned long long carry = 0, carry_b = 0;
   for (int base = 0; base < n; base += 1024 * 4) {
     // each thread owns 4 consecutive segments of this chunk
-    uint32_t c[4];
-    unsigned long long local = 0;
+    uint32_t c[4], nb[4];
+    unsigned long long local = 0, local_b = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int i = base + tid * 4 + k;
       c[k] = i < n ? counts[i] : 0u;
+      nb[k] = c[k] ? (c[k] - 1u) / kBwdChunk : 0u;   // interior chunk boundaries of the segment
       local += c[k];
+      local_b += nb[k];
     }
-    // inclusive warp scan of `local`
-    unsigned long long incl = local;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += v;
-    }
-    if (lane == 31) warp_tot[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-      unsigned long long w = warp_tot[lane];
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long v = __shfl_up_sync(0xffffffffu, w, o);
-        if (lane >= o) w += v;
-      }
-      warp_tot[lane] = w;   // inclusive over warps
-    }
-    __syncthreads();
-    unsigned long long start = carry + (wid ? warp_tot[wid - 1] : 0ull) + (incl - local);
+    unsigned long long tot, tot_b;
+    unsigned long long start = carry + block_exclusive_scan(local, warp_tot, tot);
+    unsigned long long start_b = carry_b + block_exclusive_scan(local_b, warp_tot, tot_b);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int i = base + tid * 4 + k;
@@ -67,14 +82,18 @@ scan_segments_kernel(int n, const uint32_t* __restrict__ counts, uint2* __restri
         // empty tiles keep the reference's zeroed range (rasterizer_impl.cu:303)
         ranges[i] = c[k] ? make_uint2((uint32_t)start, (uint32_t)(start + c[k])) : make_uint2(0u, 0u);
         cursor[i] = (uint32_t)start;
+        chunk_base[i] = (uint32_t)start_b;
         start += c[k];
+        start_b += nb[k];
       }
     }
-    __syncthreads();
-    if (tid == 0) carry += warp_tot[31];
-    __syncthreads();
+    carry += tot;
+    carry_b += tot_b;
   }
-  if (tid == 0) hdr->num_rendered = carry;
+  if (tid == 0) {
+    hdr->num_rendered = carry;
+    chunk_base[n] = (uint32_t)carry_b;
+  }
 }
 
 // Flags a capacity overflow before any kernel writes into the binning arena.
@@ -321,8 +340,8 @@ segment_sort_large_kernel(const uint2* __restrict__ ranges, const ImageHeader* _
 }
 
 cudaError_t launch_scan_segments(int n, const uint32_t* counts, uint2* ranges, uint32_t* cursor,
-                                 ImageHeader* hdr, cudaStream_t stream) {
-  scan_segments_kernel<<<1, 1024, 0, stream>>>(n, counts, ranges, cursor, hdr);
+                                 uint32_t* chunk_base, ImageHeader* hdr, cudaStream_t stream) {
+  scan_segments_kernel<<<1, 1024, 0, stream>>>(n, counts, ranges, cursor, chunk_base, hdr);
   return cudaGetLastError();
 }
 

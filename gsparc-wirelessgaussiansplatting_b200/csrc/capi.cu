@@ -192,7 +192,8 @@ int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w,
   }
   {
     Timed t(KID_SCAN, s);
-    GS_CHECK(launch_scan_segments(R * grid.T, img.counts, img.ranges, img.cursor, img.hdr, s), "scan");
+    GS_CHECK(launch_scan_segments(R * grid.T, img.counts, img.ranges, img.cursor, img.chunk_base, img.hdr, s),
+             "scan");
   }
   if (num_rendered) {
     unsigned long long k = 0;
@@ -286,8 +287,8 @@ int gsparc_rasterize_backward(int P, int R, int H, int W, int tile_h, int tile_w
   GS_CHECK(cudaMemsetAsync(dL_dopacity, 0, (size_t)P * sizeof(float), s), "memset dopacity");
   {
     Timed t(KID_BLEND_BWD, s);
-    GS_CHECK(launch_blend_backward(P, R, H, W, grid, grad_mode, geo, img, bin, dL_dout_real, dL_dout_imag,
-                                   dL_dmeans2D, dL_dconic, dL_dsignal, dL_dopacity, s),
+    GS_CHECK(launch_blend_backward(P, R, H, W, grid, grad_mode, binning_capacity, geo, img, bin, dL_dout_real,
+                                   dL_dout_imag, dL_dmeans2D, dL_dconic, dL_dsignal, dL_dopacity, s),
              "blend backward");
   }
   {

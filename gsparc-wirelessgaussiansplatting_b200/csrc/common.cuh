@@ -69,12 +69,21 @@ struct ImageView {
   uint32_t* cursor;
   float* final_T;
   uint32_t* n_contrib;
+  uint32_t* chunk_base;   // [R*T + 1]: exclusive scan of interior chunk boundaries per tile
+  float2* accum;          // [R, H, W]: accumulated (real, imag) of the forward
 };
+
+// The adjoint walks each tile's list in chunks of kBwdChunk entries, one CTA
+// per (tile, chunk); the forward checkpoints every pixel's (T, accumulated
+// real, imag) at each interior chunk boundary so a chunk can start without
+// the entries behind it.
+constexpr int kBwdChunk = 64;
 
 struct BinningView {
   unsigned long long* keys;
   unsigned long long* keys_alt;
   uint32_t* point_list;
+  float4* ckpt;           // [K / kBwdChunk][256 pixels]
 };
 
 // Host/device carving of the three caller-provided arenas.  The sizes are the
@@ -106,9 +115,12 @@ __host__ __device__ inline size_t carve_image(char* base, size_t R, size_t T, si
   char* c = take(R * T * sizeof(uint32_t));
   char* d = take(R * npix * sizeof(float));
   char* e = take(R * npix * sizeof(uint32_t));
+  char* f = take((R * T + 1) * sizeof(uint32_t));
+  char* g = take(R * npix * sizeof(float2));
   if (v) {
     v->hdr = (ImageHeader*)h; v->ranges = (uint2*)a; v->counts = (uint32_t*)b;
     v->cursor = (uint32_t*)c; v->final_T = (float*)d; v->n_contrib = (uint32_t*)e;
+    v->chunk_base = (uint32_t*)f; v->accum = (float2*)g;
   }
   return off;
 }
@@ -119,7 +131,11 @@ __host__ __device__ inline size_t carve_binning(char* base, size_t K, BinningVie
   char* a = take(K * sizeof(unsigned long long));
   char* b = take(K * sizeof(unsigned long long));
   char* c = take(K * sizeof(uint32_t));
-  if (v) { v->keys = (unsigned long long*)a; v->keys_alt = (unsigned long long*)b; v->point_list = (uint32_t*)c; }
+  char* d = take((K / kBwdChunk) * kBlendThreads * sizeof(float4));
+  if (v) {
+    v->keys = (unsigned long long*)a; v->keys_alt = (unsigned long long*)b; v->point_list = (uint32_t*)c;
+    v->ckpt = (float4*)d;
+  }
   return off;
 }
 

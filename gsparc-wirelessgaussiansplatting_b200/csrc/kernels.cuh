@@ -18,8 +18,8 @@ cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, 
 cudaError_t launch_mark_visible(int P, const float* means3D, const float* view, uint8_t* present,
                                 cudaStream_t stream);
 
-cudaError_t launch_scan_segments(int n, const uint32_t* counts, uint2* ranges, uint32_t* cursor, ImageHeader* hdr,
-                                 cudaStream_t stream);
+cudaError_t launch_scan_segments(int n, const uint32_t* counts, uint2* ranges, uint32_t* cursor,
+                                 uint32_t* chunk_base, ImageHeader* hdr, cudaStream_t stream);
 
 cudaError_t launch_check_capacity(ImageView img, unsigned long long capacity, cudaStream_t stream);
 
@@ -33,7 +33,8 @@ cudaError_t launch_blend_forward(int P, int R, int H, int W, const TileGrid& gri
                                  cudaStream_t stream);
 
 cudaError_t launch_blend_backward(int P, int R, int H, int W, const TileGrid& grid, unsigned grad_mode,
-                                  const GeomView& geo, const ImageView& img, const BinningView& bin,
+                                  long long capacity, const GeomView& geo, const ImageView& img,
+                                  const BinningView& bin,
                                   const float* dL_dout_real, const float* dL_dout_imag, float* dmean2D,
                                   float* dconic, float* dsig, float* dopac, cudaStream_t stream);
 
