@@ -1,4 +1,4 @@
-// Forward preprocess: one thread per (Gaussian, receiver).
+// Forward preprocess: one thread per (Gaussian, receiver), 64-thread CTAs.
 //
 // Follows preprocessCUDA (cuda_wireless_rasterizer/forward.cu:252-327) and the
 // per-Gaussian emission MLP computeSignalFromMLP (forward.cu:17-75).  The
@@ -13,14 +13,67 @@
 
 namespace gsparc {
 
+// ---- per-Gaussian emission MLP ---------------------------------------------
 // computeSignalFromMLP (forward.cu:17-75): h = leaky(b1 + W1 rx),
 // o = sigmoid(b2 + W2 h - log(|tx - mean| + 1e-6)).
-__device__ __forceinline__ float2 emission_mlp_ref(int g, int P, const float* __restrict__ mlp,
-                                                   const float3 mean, const float3 rx, const float3 tx) {
-  const float* w1 = mlp + (size_t)g * (kMlpIn * kMlpHidden);
-  const float* b1 = mlp + (size_t)P * (kMlpIn * kMlpHidden) + (size_t)g * kMlpHidden;
-  const float* w2 = mlp + (size_t)P * (kMlpIn * kMlpHidden + kMlpHidden) + (size_t)g * (kMlpOut * kMlpHidden);
-  const float* b2 = mlp + (size_t)P * (kMlpIn * kMlpHidden + kMlpHidden + kMlpOut * kMlpHidden) + (size_t)g * kMlpOut;
+//
+// The parameters of a warp's 32 consecutive Gaussians are contiguous in each
+// of the four blocks of the flat buffer (W1 [P,32,3], b1 [P,32], W2 [P,2,32],
+// b2 [P,2]), so the warp stages them into shared memory with coalesced
+// loads, one padded row per Gaussian (row strides 97, 33, 65 are odd, so the
+// 32 threads reading their own rows hit 32 different banks).  Each thread
+// then evaluates its Gaussian's MLP in the reference's operation order.
+constexpr int kPreThreads = 64;
+constexpr int kW1S = 97, kB1S = 33, kW2S = 65, kB2S = 2;
+constexpr int kMlpSmemPerWarp = 32 * (kW1S + kB1S + kW2S + kB2S);   // floats
+
+template <bool kVec>
+__device__ __forceinline__ void stage_mlp(float* __restrict__ sm, const float* __restrict__ mlp, int P, int g0,
+                                          int lane) {
+  const int nv = min(32, P - g0);
+  float* w1 = sm;
+  float* b1 = w1 + 32 * kW1S;
+  float* w2 = b1 + 32 * kB1S;
+  float* b2 = w2 + 32 * kW2S;
+  const float* gw1 = mlp + (size_t)g0 * (kMlpIn * kMlpHidden);
+  const float* gb1 = mlp + (size_t)P * (kMlpIn * kMlpHidden) + (size_t)g0 * kMlpHidden;
+  const float* gw2 = mlp + (size_t)P * (kMlpIn * kMlpHidden + kMlpHidden) + (size_t)g0 * (kMlpOut * kMlpHidden);
+  const float* gb2 = mlp + (size_t)P * (kMlpIn * kMlpHidden + kMlpHidden + kMlpOut * kMlpHidden) + (size_t)g0 * kMlpOut;
+  if (kVec) {   // 16-byte aligned buffer: rows of 96, 32 and 64 floats split into whole float4s
+    for (int e = lane; e < nv * 24; e += 32) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(gw1) + e);
+      float* d = w1 + (e / 24) * kW1S + (e % 24) * 4;
+      d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+    }
+    for (int e = lane; e < nv * 8; e += 32) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(gb1) + e);
+      float* d = b1 + (e / 8) * kB1S + (e % 8) * 4;
+      d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+    }
+    for (int e = lane; e < nv * 16; e += 32) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(gw2) + e);
+      float* d = w2 + (e / 16) * kW2S + (e % 16) * 4;
+      d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+    }
+    if (lane < nv) {
+      const float2 v = __ldg(reinterpret_cast<const float2*>(gb2) + lane);
+      b2[lane * kB2S] = v.x;
+      b2[lane * kB2S + 1] = v.y;
+    }
+  } else {
+    for (int e = lane; e < nv * 96; e += 32) w1[(e / 96) * kW1S + e % 96] = __ldg(gw1 + e);
+    for (int e = lane; e < nv * 32; e += 32) b1[(e / 32) * kB1S + e % 32] = __ldg(gb1 + e);
+    for (int e = lane; e < nv * 64; e += 32) w2[(e / 64) * kW2S + e % 64] = __ldg(gw2 + e);
+    for (int e = lane; e < nv * 2; e += 32) b2[(e / 2) * kB2S + e % 2] = __ldg(gb2 + e);
+  }
+}
+
+__device__ __forceinline__ float2 emission_mlp_row(const float* __restrict__ sm, int lane, const float3 mean,
+                                                   const float3 rx, const float3 tx) {
+  const float* w1 = sm + lane * kW1S;
+  const float* b1 = sm + 32 * kW1S + lane * kB1S;
+  const float* w2 = sm + 32 * (kW1S + kB1S) + lane * kW2S;
+  const float* b2 = sm + 32 * (kW1S + kB1S + kW2S) + lane * kB2S;
   const float in[3] = {rx.x, rx.y, rx.z};
   const float3 diff = make_float3(tx.x - mean.x, tx.y - mean.y, tx.z - mean.z);
   const float d = sqrtf(diff.x * diff.x + diff.y * diff.y + diff.z * diff.z);
@@ -28,32 +81,37 @@ __device__ __forceinline__ float2 emission_mlp_ref(int g, int P, const float* __
   float hidden[kMlpHidden];
 #pragma unroll
   for (int i = 0; i < kMlpHidden; ++i) {
-    float s = __ldg(b1 + i);
+    float s = b1[i];
 #pragma unroll
-    for (int j = 0; j < kMlpIn; ++j) s += __ldg(w1 + i * kMlpIn + j) * in[j];
+    for (int j = 0; j < kMlpIn; ++j) s += w1[i * kMlpIn + j] * in[j];
     hidden[i] = (s > 0.0f) ? s : (0.01f * s);
   }
   float o[kMlpOut];
 #pragma unroll
   for (int k = 0; k < kMlpOut; ++k) {
-    float s = __ldg(b2 + k);
+    float s = b2[k];
 #pragma unroll
-    for (int j = 0; j < kMlpHidden; ++j) s += __ldg(w2 + k * kMlpHidden + j) * hidden[j];
+    for (int j = 0; j < kMlpHidden; ++j) s += w2[k * kMlpHidden + j] * hidden[j];
     const float att = s - log_d;
     o[k] = 1.0f / (1.0f + expf(-att));
   }
   return make_float2(o[0], o[1]);
 }
 
-template <bool kSharedHist>
-__global__ void __launch_bounds__(256)
+// Dynamic shared memory: the warps' MLP staging areas, then (kSharedHist)
+// one counter per tile.
+template <bool kSharedHist, bool kVec>
+__global__ void __launch_bounds__(kPreThreads)
 preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
                   const float* __restrict__ means3D, const float* __restrict__ mlp,
                   const float* __restrict__ opacities, const float* __restrict__ scales,
                   const float* __restrict__ rotations, const float* __restrict__ views,
                   const float* __restrict__ tx_pos, const float* __restrict__ rx_pos,
                   GeomView geo, int* __restrict__ radii_out, uint32_t* __restrict__ counts) {
-  extern __shared__ uint32_t hist[];
+  extern __shared__ float smem[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  float* sm_mlp = smem + wid * kMlpSmemPerWarp;
+  uint32_t* hist = reinterpret_cast<uint32_t*>(smem + (kPreThreads / 32) * kMlpSmemPerWarp);
   const int r = blockIdx.y;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (kSharedHist) {
@@ -63,13 +121,14 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
 
   bool vis = false;
   int x0 = 0, y0 = 0, x1 = 0, y1 = 0;
+  const size_t rg = (size_t)r * P + g;
+  float3 p = make_float3(0.f, 0.f, 0.f);
   if (g < P) {
-    const size_t rg = (size_t)r * P + g;
     const float* m = views + 16 * r;
     float mv[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) mv[i] = __ldg(m + i);
-    const float3 p = make_float3(__ldg(means3D + 3 * g), __ldg(means3D + 3 * g + 1), __ldg(means3D + 3 * g + 2));
+    p = make_float3(__ldg(means3D + 3 * g), __ldg(means3D + 3 * g + 1), __ldg(means3D + 3 * g + 2));
     int radius_i = 0;
     // computeCov3D (forward.cu:124-149).  Receiver independent: written by the
     // receiver-0 thread for every Gaussian, including ones receiver 0 culls,
@@ -122,9 +181,6 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
         // keys on radii > 0, even for non-finite inputs (ceil(NaN) -> 0)
         if (radius_i > 0 && (x1 - x0) * (y1 - y0) != 0) {
           vis = true;
-          const float3 rx = make_float3(__ldg(rx_pos + 3 * r), __ldg(rx_pos + 3 * r + 1), __ldg(rx_pos + 3 * r + 2));
-          const float3 tx = make_float3(__ldg(tx_pos), __ldg(tx_pos + 1), __ldg(tx_pos + 2));
-          geo.signal[rg] = emission_mlp_ref(g, P, mlp, p, rx, tx);
           geo.depth[rg] = rdist;
           geo.means2D[rg] = make_float2(px, py);
           const float4 co = make_float4(conic.x, conic.y, conic.z, __ldg(opacities + g));
@@ -136,6 +192,16 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
     if (!vis) radius_i = 0;
     geo.radii[rg] = radius_i;
     if (radii_out) radii_out[rg] = radius_i;
+  }
+  // emission MLP of the visible Gaussians, from the warp's staged parameters
+  if (__any_sync(0xffffffffu, vis)) {
+    stage_mlp<kVec>(sm_mlp, mlp, P, blockIdx.x * blockDim.x + wid * 32, lane);
+    __syncwarp();
+    if (vis) {
+      const float3 rx = make_float3(__ldg(rx_pos + 3 * r), __ldg(rx_pos + 3 * r + 1), __ldg(rx_pos + 3 * r + 2));
+      const float3 tx = make_float3(__ldg(tx_pos), __ldg(tx_pos + 1), __ldg(tx_pos + 2));
+      geo.signal[rg] = emission_mlp_row(sm_mlp, lane, p, rx, tx);
+    }
   }
 
   if (vis) {
@@ -169,7 +235,14 @@ __global__ void mark_visible_kernel(int P, const float* __restrict__ means3D,
   present[g] = rr <= 0.04f ? 0 : 1;
 }
 
-constexpr int kMaxSharedHistTiles = 40960;   // 160 KB of shared counters
+constexpr size_t kMlpSmemBytes = (kPreThreads / 32) * kMlpSmemPerWarp * sizeof(float);   // 50,432 B
+constexpr int kMaxSharedHistTiles = (int)((227 * 1024 - kMlpSmemBytes) / sizeof(uint32_t));
+
+template <bool kSharedHist, bool kVec>
+static cudaError_t set_preprocess_smem(int dev) {
+  return cudaFuncSetAttribute(preprocess_kernel<kSharedHist, kVec>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              227 * 1024);
+}
 
 cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, float mod,
                               const float* means3D, const float* mlp, const float* opacities,
@@ -177,18 +250,40 @@ cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, 
                               const float* tx_pos, const float* rx_pos, const GeomView& geo,
                               int* radii_out, uint32_t* counts, cudaStream_t stream) {
   if (P == 0 || R == 0) return cudaSuccess;
-  dim3 block(256), gridd((P + 255) / 256, R);
+  // the shared-memory opt-in is set once per device, so later calls (including
+  // ones made while a CUDA graph is being captured) only enqueue the launch
+  static bool attr_done[64] = {false};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64 || !attr_done[dev]) {
+    if ((e = set_preprocess_smem<true, true>(dev)) != cudaSuccess) return e;
+    if ((e = set_preprocess_smem<true, false>(dev)) != cudaSuccess) return e;
+    if ((e = set_preprocess_smem<false, true>(dev)) != cudaSuccess) return e;
+    if ((e = set_preprocess_smem<false, false>(dev)) != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64) attr_done[dev] = true;
+  }
+  const bool vec = (((uintptr_t)mlp) & 15u) == 0;
+  dim3 block(kPreThreads), gridd((P + kPreThreads - 1) / kPreThreads, R);
   if (grid.T <= kMaxSharedHistTiles) {
-    const size_t smem = (size_t)grid.T * sizeof(uint32_t);
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(preprocess_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-    }
-    preprocess_kernel<true><<<gridd, block, smem, stream>>>(P, H, W, grid, mod, means3D, mlp, opacities, scales,
-                                                            rotations, views, tx_pos, rx_pos, geo, radii_out, counts);
+    const size_t smem = kMlpSmemBytes + (size_t)grid.T * sizeof(uint32_t);
+    if (vec)
+      preprocess_kernel<true, true><<<gridd, block, smem, stream>>>(P, H, W, grid, mod, means3D, mlp, opacities,
+                                                                    scales, rotations, views, tx_pos, rx_pos, geo,
+                                                                    radii_out, counts);
+    else
+      preprocess_kernel<true, false><<<gridd, block, smem, stream>>>(P, H, W, grid, mod, means3D, mlp, opacities,
+                                                                     scales, rotations, views, tx_pos, rx_pos, geo,
+                                                                     radii_out, counts);
   } else {
-    preprocess_kernel<false><<<gridd, block, 0, stream>>>(P, H, W, grid, mod, means3D, mlp, opacities, scales,
-                                                          rotations, views, tx_pos, rx_pos, geo, radii_out, counts);
+    if (vec)
+      preprocess_kernel<false, true><<<gridd, block, kMlpSmemBytes, stream>>>(
+          P, H, W, grid, mod, means3D, mlp, opacities, scales, rotations, views, tx_pos, rx_pos, geo, radii_out,
+          counts);
+    else
+      preprocess_kernel<false, false><<<gridd, block, kMlpSmemBytes, stream>>>(
+          P, H, W, grid, mod, means3D, mlp, opacities, scales, rotations, views, tx_pos, rx_pos, geo, radii_out,
+          counts);
   }
   return cudaGetLastError();
 }
