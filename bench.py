@@ -285,9 +285,10 @@ def run_ours(args):
             trainer.step_eager(views_d[j:j + 1], rxs_d[j:j + 1], tx, targets_d[j:j + 1])
         torch.cuda.synchronize()
     ktimes = {k: v for k, v in kt.results().items() if v[1] > 0}
-    # kernels per timed call: the sort is two launches, the loss three, the
-    # optimizer three (step counter, per-Gaussian groups, MLP groups)
-    per_call = {"segment_sort_kernel": 2, "splat_loss_kernels": 3, "gaussian_adam_kernels": 3}
+    # kernels per timed call: the depth sort is four launches (radix passes),
+    # the loss three, the optimizer three (step counter, per-Gaussian groups,
+    # MLP groups)
+    per_call = {"depth_sort_kernels": 4, "splat_loss_kernels": 3, "gaussian_adam_kernels": 3}
     launches = sum(c * per_call.get(k, 1) for k, (_, c) in ktimes.items()) // n_eager
     dom = max(ktimes, key=lambda k: ktimes[k][0])
     # batched: every receiver of the pool in one captured step
@@ -310,8 +311,9 @@ def run_ours(args):
         "blend_backward_kernel": K * 36 + npix * 16 + vis * 40,
         "blend_forward_kernel": K * 36 + npix * 16,
         "preprocess_kernel": P_GAUSS * 44 + vis * 776 + P_GAUSS * 44,
-        "segment_sort_kernel": K * 8 + K * 4 + 138 * 8,
-        "scatter_kernel": vis * 20 + K * 8,
+        "depth_sort_kernels": P_GAUSS * 16 * 4,
+        "segment_place_kernel": K * 12 + 138 * 8,
+        "scatter_kernel": vis * 24 + K * 4,
         "emission_backward_kernel": vis * (776 + 12 + 8) + P_GAUSS * 776,
         "geometry_backward_kernel": vis * (12 + 40 + 24 + 24 + 24) + P_GAUSS * 64,
         "ssim_forward_kernel": npix * 8 + npix * 16,

@@ -43,13 +43,13 @@ bool valid_tile(int th, int tw) {
 
 // ---- optional per-kernel timing (CUDA events around each launch) ----------
 enum KernelId {
-  KID_PREPROCESS, KID_SCAN, KID_CHECK, KID_SCATTER, KID_SEGSORT, KID_BLEND_FWD, KID_BLEND_BWD,
+  KID_PREPROCESS, KID_SCAN, KID_CHECK, KID_SCATTER, KID_DEPTH_SORT, KID_PLACE, KID_BLEND_FWD, KID_BLEND_BWD,
   KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_ADAM, KID_LOSS, KID_ACTIVATE,
   KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
     "preprocess_kernel", "scan_segments_kernel", "check_capacity_kernel", "scatter_kernel",
-    "segment_sort_kernel", "blend_forward_kernel", "blend_backward_kernel", "geometry_backward_kernel",
+    "depth_sort_kernels", "segment_place_kernel", "blend_forward_kernel", "blend_backward_kernel", "geometry_backward_kernel",
     "emission_backward_kernel", "ssim_forward_kernel", "ssim_backward_kernel", "mark_visible_kernel",
     "gaussian_adam_kernels", "splat_loss_kernels", "gaussian_activate_kernel"};
 
@@ -162,7 +162,7 @@ int gsparc_binning_state_layout(long long capacity, size_t* o) {
   BinningView v;
   char* base = (char*)(uintptr_t)4096;
   carve_binning(base, (size_t)capacity, &v);
-  o[0] = (char*)v.keys - base; o[1] = (char*)v.keys_alt - base; o[2] = (char*)v.point_list - base;
+  o[0] = (char*)v.seg_rank - base; o[1] = (char*)v.point_list - base; o[2] = (char*)v.ckpt - base;
   return GSPARC_OK;
 }
 
@@ -172,6 +172,8 @@ int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w,
                              const float* tx_pos, const float* rx_pos, int* radii_out, void* geom_state,
                              void* image_state, long long* num_rendered, void* stream) {
   if (P < 0 || R < 1 || H <= 0 || W <= 0) return invalid("sizes (need P >= 0, R >= 1, H, W > 0)");
+  if (P > kMaxBinningP) return invalid("P above 1048576 Gaussians per call (the binning's rank bitmap limit)");
+  if (R > 65535) return invalid("R above 65535 receivers per call");
   if (!valid_tile(tile_h, tile_w)) return invalid("tile shape must be 16x16, 8x32 or 32x8");
   if (!image_state || !viewmatrices || !tx_pos || !rx_pos) return invalid("null state or receiver pointer");
   if (P > 0 && (!geom_state || !means3D || !emission_mlps || !opacities || !scales || !rotations))
@@ -184,6 +186,9 @@ int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w,
   carve_image((char*)image_state, (size_t)R, (size_t)grid.T, (size_t)H * W, &img);
   GS_CHECK(cudaMemsetAsync(img.hdr, 0, sizeof(ImageHeader), s), "memset header");
   GS_CHECK(cudaMemsetAsync(img.counts, 0, (size_t)R * grid.T * sizeof(uint32_t), s), "memset counts");
+  if (P > 0)
+    GS_CHECK(cudaMemsetAsync(geo.sort_state, 0, sort_state_words((size_t)P, (size_t)R) * sizeof(uint32_t), s),
+             "memset sort state");
   {
     Timed t(KID_PREPROCESS, s);
     GS_CHECK(launch_preprocess(P, R, H, W, grid, scale_modifier, means3D, emission_mlps, opacities, scales,
@@ -225,12 +230,16 @@ int gsparc_rasterize_render(int P, int R, int H, int W, int tile_h, int tile_w, 
     GS_CHECK(launch_check_capacity(img, (unsigned long long)capacity, s), "capacity check");
   }
   {
+    Timed t(KID_DEPTH_SORT, s);
+    GS_CHECK(launch_depth_sort(P, R, geo, img, s), "depth sort");
+  }
+  {
     Timed t(KID_SCATTER, s);
     GS_CHECK(launch_scatter(P, R, grid, geo, img, bin, s), "scatter");
   }
   {
-    Timed t(KID_SEGSORT, s);
-    GS_CHECK(launch_segment_sort(R, grid, img, bin, s), "segment sort");
+    Timed t(KID_PLACE, s);
+    GS_CHECK(launch_segment_place(P, R, grid, geo, img, bin, s), "segment place");
   }
   {
     Timed t(KID_BLEND_FWD, s);

@@ -34,6 +34,7 @@ constexpr int kMlpFloats = kMlpIn * kMlpHidden + kMlpHidden + kMlpOut * kMlpHidd
 constexpr uint32_t kErrCapacity = 1u << 0;   // K exceeded the binning capacity
 constexpr uint32_t kErrSegment = 1u << 1;    // a tile segment exceeded the sort limit
 constexpr uint32_t kErrBadIndex = 1u << 2;   // a point list held an id >= P (arena mismatch)
+constexpr uint32_t kErrSortWait = 1u << 3;   // a depth-sort look-back wait gave up (bounded spin)
 
 struct ImageHeader {
   unsigned long long num_rendered;   // K, written by the scan kernel
@@ -52,6 +53,17 @@ struct TileGrid {
       : tile_h(th), tile_w(tw), gx((W + tw - 1) / tw), gy((H + th - 1) / th), T(gx * gy) {}
 };
 
+// Per-receiver depth order (binning.cu): an LSD radix sort of one 32-bit key
+// per (receiver, Gaussian) -- the depth bits of visible Gaussians, ~0 for the
+// rest -- in tiles of kSortTileKeys keys with decoupled look-back.
+constexpr int kSortTileKeys = 2048;   // 256 threads x 8 keys
+__host__ __device__ inline size_t sort_tiles(size_t P) { return (P + kSortTileKeys - 1) / kSortTileKeys; }
+// words of the sort state: digit histograms [R][4][256], tile tickets [R][4],
+// look-back words [R][4][tiles][256]; zeroed before every preprocess
+__host__ __device__ inline size_t sort_state_words(size_t P, size_t R) {
+  return R * 1024 + R * 4 + R * 4 * sort_tiles(P) * 256;
+}
+
 struct GeomView {
   float2* means2D;
   float* depth;
@@ -59,7 +71,11 @@ struct GeomView {
   float4* conic_opacity;
   float2* signal;
   float* cov3D;
-  float4* box;   // [R][P] pixel box (x_lo, x_hi, y_lo, y_hi) outside which alpha < 1/255
+  float4* box;            // [R][P] pixel box (x_lo, x_hi, y_lo, y_hi) outside which alpha < 1/255
+  uint32_t* sort_key[2];  // [R][P] radix ping-pong; sort_key[0] starts as the depth keys
+  uint32_t* sort_val[2];  // [R][P]; sort_val[0] ends as the Gaussian ids in depth order
+  uint32_t* rank;         // [R][P] position of each Gaussian in its receiver's depth order
+  uint32_t* sort_state;   // sort_state_words(P, R) words
 };
 
 struct ImageView {
@@ -80,9 +96,8 @@ struct ImageView {
 constexpr int kBwdChunk = 64;
 
 struct BinningView {
-  unsigned long long* keys;
-  unsigned long long* keys_alt;
-  uint32_t* point_list;
+  uint32_t* seg_rank;     // [K] depth rank of each instance, grouped by segment (unordered within)
+  uint32_t* point_list;   // [K] Gaussian ids, segments in depth order
   float4* ckpt;           // [K / kBwdChunk][256 pixels]
 };
 
@@ -99,9 +114,18 @@ __host__ __device__ inline size_t carve_geom(char* base, size_t P, size_t R, Geo
   char* e = take(n * sizeof(float2));
   char* f = take(P * 6 * sizeof(float));
   char* g = take(n * sizeof(float4));
+  char* k0 = take(n * sizeof(uint32_t));
+  char* k1 = take(n * sizeof(uint32_t));
+  char* v0 = take(n * sizeof(uint32_t));
+  char* v1 = take(n * sizeof(uint32_t));
+  char* rk = take(n * sizeof(uint32_t));
+  char* ss = take(sort_state_words(P, R) * sizeof(uint32_t));
   if (v) {
     v->means2D = (float2*)a; v->depth = (float*)b; v->radii = (int*)c;
     v->conic_opacity = (float4*)d; v->signal = (float2*)e; v->cov3D = (float*)f; v->box = (float4*)g;
+    v->sort_key[0] = (uint32_t*)k0; v->sort_key[1] = (uint32_t*)k1;
+    v->sort_val[0] = (uint32_t*)v0; v->sort_val[1] = (uint32_t*)v1;
+    v->rank = (uint32_t*)rk; v->sort_state = (uint32_t*)ss;
   }
   return off;
 }
@@ -128,13 +152,11 @@ __host__ __device__ inline size_t carve_image(char* base, size_t R, size_t T, si
 __host__ __device__ inline size_t carve_binning(char* base, size_t K, BinningView* v) {
   size_t off = 0;
   auto take = [&](size_t bytes) { char* p = base ? base + off : nullptr; off = align_up(off + bytes, 256); return p; };
-  char* a = take(K * sizeof(unsigned long long));
-  char* b = take(K * sizeof(unsigned long long));
+  char* a = take(K * sizeof(uint32_t));
   char* c = take(K * sizeof(uint32_t));
   char* d = take((K / kBwdChunk) * kBlendThreads * sizeof(float4));
   if (v) {
-    v->keys = (unsigned long long*)a; v->keys_alt = (unsigned long long*)b; v->point_list = (uint32_t*)c;
-    v->ckpt = (float4*)d;
+    v->seg_rank = (uint32_t*)a; v->point_list = (uint32_t*)c; v->ckpt = (float4*)d;
   }
   return off;
 }

@@ -26,7 +26,13 @@ cudaError_t launch_check_capacity(ImageView img, unsigned long long capacity, cu
 cudaError_t launch_scatter(int P, int R, const TileGrid& grid, const GeomView& geo, ImageView img, BinningView bin,
                            cudaStream_t stream);
 
-cudaError_t launch_segment_sort(int R, const TileGrid& grid, ImageView img, BinningView bin, cudaStream_t stream);
+// Largest P the binning supports (the placement's rank bitmap lives in shared memory).
+constexpr int kMaxBinningP = 1 << 20;
+
+cudaError_t launch_depth_sort(int P, int R, const GeomView& geo, ImageView img, cudaStream_t stream);
+
+cudaError_t launch_segment_place(int P, int R, const TileGrid& grid, const GeomView& geo, ImageView img,
+                                 BinningView bin, cudaStream_t stream);
 
 cudaError_t launch_blend_forward(int P, int R, int H, int W, const TileGrid& grid, const GeomView& geo,
                                  const ImageView& img, const BinningView& bin, float* out_real, float* out_imag,

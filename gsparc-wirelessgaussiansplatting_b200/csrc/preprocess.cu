@@ -98,8 +98,9 @@ __device__ __forceinline__ float2 emission_mlp_row(const float* __restrict__ sm,
   return make_float2(o[0], o[1]);
 }
 
-// Dynamic shared memory: the warps' MLP staging areas, then (kSharedHist)
-// one counter per tile.
+// Dynamic shared memory: the warps' MLP staging areas, the 4 x 256 digit
+// counters of the depth keys (the radix sort's histograms), then
+// (kSharedHist) one counter per tile.
 template <bool kSharedHist, bool kVec>
 __global__ void __launch_bounds__(kPreThreads)
 preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
@@ -111,13 +112,14 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   float* sm_mlp = smem + wid * kMlpSmemPerWarp;
-  uint32_t* hist = reinterpret_cast<uint32_t*>(smem + (kPreThreads / 32) * kMlpSmemPerWarp);
+  uint32_t* dhist = reinterpret_cast<uint32_t*>(smem + (kPreThreads / 32) * kMlpSmemPerWarp);
+  uint32_t* hist = dhist + 1024;
   const int r = blockIdx.y;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (kSharedHist) {
+  for (int t = threadIdx.x; t < 1024; t += blockDim.x) dhist[t] = 0;
+  if (kSharedHist)
     for (int t = threadIdx.x; t < grid.T; t += blockDim.x) hist[t] = 0;
-    __syncthreads();
-  }
+  __syncthreads();
 
   bool vis = false;
   int x0 = 0, y0 = 0, x1 = 0, y1 = 0;
@@ -130,6 +132,7 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
     for (int i = 0; i < 16; ++i) mv[i] = __ldg(m + i);
     p = make_float3(__ldg(means3D + 3 * g), __ldg(means3D + 3 * g + 1), __ldg(means3D + 3 * g + 2));
     int radius_i = 0;
+    uint32_t dkey = 0xffffffffu;   // depth key of the per-receiver depth order: culled Gaussians sort last
     // computeCov3D (forward.cu:124-149).  Receiver independent: written by the
     // receiver-0 thread for every Gaussian, including ones receiver 0 culls,
     // because other receivers of the batch (and the backward) read it.
@@ -181,6 +184,7 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
         // keys on radii > 0, even for non-finite inputs (ceil(NaN) -> 0)
         if (radius_i > 0 && (x1 - x0) * (y1 - y0) != 0) {
           vis = true;
+          dkey = __float_as_uint(rdist);
           geo.depth[rg] = rdist;
           geo.means2D[rg] = make_float2(px, py);
           const float4 co = make_float4(conic.x, conic.y, conic.z, __ldg(opacities + g));
@@ -192,6 +196,9 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
     if (!vis) radius_i = 0;
     geo.radii[rg] = radius_i;
     if (radii_out) radii_out[rg] = radius_i;
+    geo.sort_key[0][rg] = dkey;
+#pragma unroll
+    for (int pass = 0; pass < 4; ++pass) atomicAdd(&dhist[pass * 256 + ((dkey >> (8 * pass)) & 255u)], 1u);
   }
   // emission MLP of the visible Gaussians, from the warp's staged parameters
   if (__any_sync(0xffffffffu, vis)) {
@@ -212,12 +219,16 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
         else atomicAdd(&counts[(size_t)r * grid.T + tile], 1u);
       }
   }
+  __syncthreads();
   if (kSharedHist) {
-    __syncthreads();
     for (int t = threadIdx.x; t < grid.T; t += blockDim.x) {
       const uint32_t c = hist[t];
       if (c) atomicAdd(&counts[(size_t)r * grid.T + t], c);
     }
+  }
+  for (int t = threadIdx.x; t < 1024; t += blockDim.x) {
+    const uint32_t c = dhist[t];
+    if (c) atomicAdd(&geo.sort_state[(size_t)r * 1024 + t], c);
   }
 }
 
@@ -235,7 +246,8 @@ __global__ void mark_visible_kernel(int P, const float* __restrict__ means3D,
   present[g] = rr <= 0.04f ? 0 : 1;
 }
 
-constexpr size_t kMlpSmemBytes = (kPreThreads / 32) * kMlpSmemPerWarp * sizeof(float);   // 50,432 B
+// MLP staging (50,432 B) + digit counters (4 KB)
+constexpr size_t kMlpSmemBytes = (kPreThreads / 32) * kMlpSmemPerWarp * sizeof(float) + 1024 * sizeof(uint32_t);
 constexpr int kMaxSharedHistTiles = (int)((227 * 1024 - kMlpSmemBytes) / sizeof(uint32_t));
 
 template <bool kSharedHist, bool kVec>

@@ -236,7 +236,7 @@ def state_views(st: ForwardState):
     out["final_T"] = view(st.image, io[4], R * H * W, torch.float32, (R, H, W))
     out["n_contrib"] = view(st.image, io[5], R * H * W, torch.int32, (R, H, W))
     if st.capacity > 0:
-        out["point_list"] = view(st.binning, bo[2], st.capacity, torch.int32, (st.capacity,))
+        out["point_list"] = view(st.binning, bo[1], st.capacity, torch.int32, (st.capacity,))
     return out
 
 

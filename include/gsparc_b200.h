@@ -74,7 +74,8 @@ GSPARC_API size_t gsparc_binning_state_bytes(long long capacity);
 /* Byte offsets of the sub-arrays inside each arena (for inspection / tests).
  * geom:    means2D, depth, radii, conic_opacity, signal, cov3D   (6 entries)
  * image:   header, ranges, counts, cursor, final_T, n_contrib    (6 entries)
- * binning: keys, keys_alt, point_list                            (3 entries) */
+ * binning: seg_rank (per-instance depth rank, grouped by segment),
+ *          point_list, adjoint checkpoints                       (3 entries) */
 GSPARC_API int gsparc_geom_state_layout(int P, int R, size_t* offsets6);
 GSPARC_API int gsparc_image_state_layout(int R, int H, int W, int tile_h, int tile_w, size_t* offsets6);
 GSPARC_API int gsparc_binning_state_layout(long long capacity, size_t* offsets3);
@@ -92,7 +93,9 @@ GSPARC_API int gsparc_binning_state_layout(long long capacity, size_t* offsets3)
  * gaussian.py:565-572), opacities [P] (activated), scales [P,3] (activated),
  * rotations [P,4] (normalised, (w,x,y,z)), viewmatrices [R,16] (transposed
  * world->receiver, as built by preprocess_data.py:177-202), tx_pos [3],
- * rx_pos [R,3].  radii_out [R,P] may be NULL.
+ * rx_pos [R,3].  radii_out [R,P] may be NULL.  Limits: P <= 1048576 (the
+ * binning places each tile's instances with a bitmap over the P depth
+ * ranks, held in shared memory), R <= 65535.
  *
  * When num_rendered is non-NULL, K is copied to the host and the stream is
  * synchronised (the reference's blocking readback, rasterizer_impl.cu:274);
@@ -105,10 +108,11 @@ GSPARC_API int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, 
                              const float* rx_pos, int* radii_out, void* geom_state,
                              void* image_state, long long* num_rendered, void* stream);
 
-/* Stage 2 of the forward: duplicate instances into per-(receiver, tile)
- * segments, sort every segment by (depth bits, Gaussian id) -- the order the
- * reference's stable radix sort on (tile | depth) produces -- and blend each
- * tile front to back.  Replaces duplicateWithKeys, cub::DeviceRadixSort,
+/* Stage 2 of the forward: put each receiver's Gaussians in (depth bits,
+ * Gaussian id) order, duplicate instances into per-(receiver, tile) segments
+ * and place every segment in that order -- the order the reference's stable
+ * radix sort on (tile | depth) produces -- then blend each tile front to
+ * back.  Replaces duplicateWithKeys, cub::DeviceRadixSort,
  * identifyTileRanges and FORWARD::render (rasterizer_impl.cu:276-331,
  * forward.cu:151-249).  out_real / out_imag are [R,H,W] (one channel).
  * If K exceeds `capacity` the device error word gets the capacity bit and the

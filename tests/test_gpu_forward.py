@@ -157,7 +157,10 @@ def test_edge_cases_empty_and_culled():
     # every Gaussian within the 0.2 m cull radius
     np_in, th = make_inputs(50, seed=9)
     rxp = torch.tensor([0.0, 1.0, 0.0], device=dev)
-    th["means"] = rxp[None] + 0.05 * torch.randn(50, 3, device=dev)
+    gen = torch.Generator().manual_seed(9)
+    off = torch.randn(50, 3, generator=gen)
+    off = off / off.norm(dim=1, keepdim=True) * (0.15 * torch.rand(50, 1, generator=gen))   # inside 0.15 m
+    th["means"] = rxp[None] + off.to(dev)
     th["rxs"] = rxp[None]
     th["views"] = torch.from_numpy(scenes.view_matrix(rxp.cpu().numpy())[None]).to(dev)
     out_r, out_i, radii, st = gpu_forward(th)
