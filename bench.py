@@ -285,10 +285,9 @@ def run_ours(args):
             trainer.step_eager(views_d[j:j + 1], rxs_d[j:j + 1], tx, targets_d[j:j + 1])
         torch.cuda.synchronize()
     ktimes = {k: v for k, v in kt.results().items() if v[1] > 0}
-    # kernels per timed call: the depth sort is four launches (radix passes),
-    # the loss three, the optimizer three (step counter, per-Gaussian groups,
-    # MLP groups)
-    per_call = {"depth_sort_kernels": 4, "splat_loss_kernels": 3, "gaussian_adam_kernels": 3}
+    # kernels per timed call: the loss is two launches (the depth sort is one
+    # cooperative launch at this size, the optimizer one)
+    per_call = {"splat_loss_kernels": 2}
     launches = sum(c * per_call.get(k, 1) for k, (_, c) in ktimes.items()) // n_eager
     dom = max(ktimes, key=lambda k: ktimes[k][0])
     # batched: every receiver of the pool in one captured step

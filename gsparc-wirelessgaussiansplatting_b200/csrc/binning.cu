@@ -23,82 +23,6 @@
 
 namespace gsparc {
 
-// ---- scan of per-segment counts -> ranges, cursors, K, chunk bases ---------
-// One block; n = R*T segments (a few thousand at most for a spectrum batch).
-
-// Exclusive scan of one value per thread over the 1024-thread block; every
-// thread also receives the block total.
-__device__ __forceinline__ unsigned long long block_exclusive_scan(unsigned long long local,
-                                                                   unsigned long long* warp_tot,
-                                                                   unsigned long long& total) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  unsigned long long incl = local;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  if (lane == 31) warp_tot[wid] = incl;
-  __syncthreads();
-  if (wid == 0) {
-    unsigned long long w = warp_tot[lane];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned long long v = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += v;
-    }
-    warp_tot[lane] = w;   // inclusive over warps
-  }
-  __syncthreads();
-  const unsigned long long excl = (wid ? warp_tot[wid - 1] : 0ull) + (incl - local);
-  total = warp_tot[31];
-  __syncthreads();
-  return excl;
-}
-
-__global__ void __launch_bounds__(1024)
-scan_segments_kernel(int n, const uint32_t* __restrict__ counts, uint2* __restrict__ ranges,
-                     uint32_t* __restrict__ cursor, uint32_t* __restrict__ chunk_base,
-                     ImageHeader* __restrict__ hdr) {
-  __shared__ unsigned long long warp_tot[32];
-  const int tid = threadIdx.x;
-  unsigned long long carry = 0, carry_b = 0;
-  for (int base = 0; base < n; base += 1024 * 4) {
-    // each thread owns 4 consecutive segments of this chunk
-    uint32_t c[4], nb[4];
-    unsigned long long local = 0, local_b = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int i = base + tid * 4 + k;
-      c[k] = i < n ? counts[i] : 0u;
-      nb[k] = c[k] ? (c[k] - 1u) / kBwdChunk : 0u;   // interior chunk boundaries of the segment
-      local += c[k];
-      local_b += nb[k];
-    }
-    unsigned long long tot, tot_b;
-    unsigned long long start = carry + block_exclusive_scan(local, warp_tot, tot);
-    unsigned long long start_b = carry_b + block_exclusive_scan(local_b, warp_tot, tot_b);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int i = base + tid * 4 + k;
-      if (i < n) {
-        // empty tiles keep the reference's zeroed range (rasterizer_impl.cu:303)
-        ranges[i] = c[k] ? make_uint2((uint32_t)start, (uint32_t)(start + c[k])) : make_uint2(0u, 0u);
-        cursor[i] = (uint32_t)start;
-        chunk_base[i] = (uint32_t)start_b;
-        start += c[k];
-        start_b += nb[k];
-      }
-    }
-    carry += tot;
-    carry_b += tot_b;
-  }
-  if (tid == 0) {
-    hdr->num_rendered = carry;
-    chunk_base[n] = (uint32_t)carry_b;
-  }
-}
-
 // Flags a capacity overflow before any kernel writes into the binning arena.
 __global__ void check_capacity_kernel(ImageHeader* hdr, unsigned long long capacity) {
   hdr->capacity = capacity;
@@ -298,9 +222,19 @@ __device__ __forceinline__ void radix_pass_body(RadixShared& sh, int P, int pass
   __syncthreads();   // shared memory is reused by the next pass
 }
 
+// The binning capacity is recorded and K checked against it by the first CTA
+// of the first pass, before any kernel that writes the binning arena runs.
+__device__ __forceinline__ void capacity_check(ImageHeader* hdr, unsigned long long capacity) {
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    hdr->capacity = capacity;
+    if (hdr->num_rendered > capacity) atomic_or_error(hdr, kErrCapacity);
+  }
+}
+
 __global__ void __launch_bounds__(kRadixThreads)
-radix_pass_kernel(int P, int pass, GeomView geo, ImageHeader* __restrict__ hdr) {
+radix_pass_kernel(int P, int pass, GeomView geo, ImageHeader* __restrict__ hdr, unsigned long long capacity) {
   __shared__ RadixShared sh;
+  if (pass == 0) capacity_check(hdr, capacity);
   radix_pass_body(sh, P, pass, true, geo, hdr);
 }
 
@@ -325,8 +259,9 @@ __device__ __forceinline__ void receiver_barrier(uint32_t* counter, uint32_t exp
 }
 
 __global__ void __launch_bounds__(kRadixThreads)
-radix_sort_coop_kernel(int P, GeomView geo, ImageHeader* __restrict__ hdr) {
+radix_sort_coop_kernel(int P, GeomView geo, ImageHeader* __restrict__ hdr, unsigned long long capacity) {
   __shared__ RadixShared sh;
+  capacity_check(hdr, capacity);
   // barrier counters share the (unused) ticket words of passes 1..3
   uint32_t* bars = geo.sort_state + (size_t)gridDim.y * 1024 + (size_t)blockIdx.y * 4;
   for (int pass = 0; pass < 4; ++pass) {
@@ -397,34 +332,6 @@ __device__ __forceinline__ int next_pow2(int n) {
   return p;
 }
 
-// Exclusive scan of one value per thread over the CTA (any multiple of 32
-// threads up to 1024); every thread also receives the total.
-__device__ __forceinline__ uint32_t cta_exclusive_scan(uint32_t local, uint32_t* warp_tot, uint32_t& total) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  uint32_t incl = local;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  if (lane == 31) warp_tot[wid] = incl;
-  __syncthreads();
-  if (wid == 0) {
-    uint32_t w = lane < nw ? warp_tot[lane] : 0u;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t v = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += v;
-    }
-    if (lane < nw) warp_tot[lane] = w;
-  }
-  __syncthreads();
-  const uint32_t excl = (wid ? warp_tot[wid - 1] : 0u) + (incl - local);
-  total = warp_tot[nw - 1];
-  __syncthreads();
-  return excl;
-}
-
 __global__ void __launch_bounds__(kPlaceThreads)
 segment_place_kernel(int P, int T, const uint2* __restrict__ ranges, const ImageHeader* __restrict__ hdr,
                      const uint32_t* __restrict__ seg_rank, GeomView geo, uint32_t* __restrict__ point_list) {
@@ -486,7 +393,7 @@ segment_place_kernel(int P, int T, const uint2* __restrict__ ranges, const Image
     tsum += c;
   }
   uint32_t total;
-  uint32_t off = cta_exclusive_scan(tsum, warp_tot, total);
+  uint32_t off = cta_exclusive_scan<uint32_t>(tsum, warp_tot, total);
   for (int gi = g0; gi < g1; ++gi) {
     const uint32_t c = pre[gi];
     pre[gi] = off;
@@ -517,12 +424,6 @@ segment_place_kernel(int P, int T, const uint2* __restrict__ ranges, const Image
   }
 }
 
-cudaError_t launch_scan_segments(int n, const uint32_t* counts, uint2* ranges, uint32_t* cursor,
-                                 uint32_t* chunk_base, ImageHeader* hdr, cudaStream_t stream) {
-  scan_segments_kernel<<<1, 1024, 0, stream>>>(n, counts, ranges, cursor, chunk_base, hdr);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_check_capacity(ImageView img, unsigned long long capacity, cudaStream_t stream) {
   check_capacity_kernel<<<1, 1, 0, stream>>>(img.hdr, capacity);
   return cudaGetLastError();
@@ -542,7 +443,8 @@ cudaError_t launch_scatter(int P, int R, const TileGrid& grid, const GeomView& g
 
 // One cooperative launch when every CTA of the sort fits on the GPU at once
 // (the launch itself guarantees co-residency), else one launch per pass.
-cudaError_t launch_depth_sort(int P, int R, const GeomView& geo, ImageView img, cudaStream_t stream) {
+cudaError_t launch_depth_sort(int P, int R, const GeomView& geo, ImageView img, unsigned long long capacity,
+                              cudaStream_t stream) {
   if (P == 0 || R == 0) return cudaSuccess;
   static long long coop_capacity[64] = {0};
   int dev = 0;
@@ -571,10 +473,10 @@ cudaError_t launch_depth_sort(int P, int R, const GeomView& geo, ImageView img, 
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     ImageHeader* hdr = img.hdr;
-    return cudaLaunchKernelEx(&cfg, radix_sort_coop_kernel, P, geo, hdr);
+    return cudaLaunchKernelEx(&cfg, radix_sort_coop_kernel, P, geo, hdr, capacity);
   }
   for (int pass = 0; pass < 4; ++pass) {
-    radix_pass_kernel<<<grid, kRadixThreads, 0, stream>>>(P, pass, geo, img.hdr);
+    radix_pass_kernel<<<grid, kRadixThreads, 0, stream>>>(P, pass, geo, img.hdr, capacity);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

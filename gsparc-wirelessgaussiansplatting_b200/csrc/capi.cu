@@ -1,8 +1,10 @@
 // extern "C" entry points: argument checks, arena carving and launch order.
 //
 // Launch sequence of one forward (all on the caller's stream):
-//   memset(header, counts) -> preprocess(+tile histogram) -> scan   [prepare]
-//   capacity check -> scatter -> segment sort -> blend              [render]
+//   memset(header, counts, sort state) -> preprocess (+ tile and digit
+//   histograms; its last CTA scans the tile counts)               [prepare]
+//   depth sort (+ capacity check) -> scatter -> segment placement -> blend
+//                                                                  [render]
 // and of one backward:
 //   memset(accumulated grads) -> blend adjoint -> geometry adjoint
 //   -> emission-MLP adjoint.
@@ -43,12 +45,12 @@ bool valid_tile(int th, int tw) {
 
 // ---- optional per-kernel timing (CUDA events around each launch) ----------
 enum KernelId {
-  KID_PREPROCESS, KID_SCAN, KID_CHECK, KID_SCATTER, KID_DEPTH_SORT, KID_PLACE, KID_BLEND_FWD, KID_BLEND_BWD,
+  KID_PREPROCESS, KID_CHECK, KID_SCATTER, KID_DEPTH_SORT, KID_PLACE, KID_BLEND_FWD, KID_BLEND_BWD,
   KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_ADAM, KID_LOSS, KID_ACTIVATE,
   KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
-    "preprocess_kernel", "scan_segments_kernel", "check_capacity_kernel", "scatter_kernel",
+    "preprocess_kernel", "check_capacity_kernel", "scatter_kernel",
     "depth_sort_kernels", "segment_place_kernel", "blend_forward_kernel", "blend_backward_kernel", "geometry_backward_kernel",
     "emission_backward_kernel", "ssim_forward_kernel", "ssim_backward_kernel", "mark_visible_kernel",
     "gaussian_adam_kernels", "splat_loss_kernels", "gaussian_activate_kernel"};
@@ -192,13 +194,12 @@ int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w,
   {
     Timed t(KID_PREPROCESS, s);
     GS_CHECK(launch_preprocess(P, R, H, W, grid, scale_modifier, means3D, emission_mlps, opacities, scales,
-                               rotations, viewmatrices, tx_pos, rx_pos, geo, radii_out, img.counts, s),
+                               rotations, viewmatrices, tx_pos, rx_pos, geo, radii_out, img, s),
              "preprocess");
   }
-  {
-    Timed t(KID_SCAN, s);
-    GS_CHECK(launch_scan_segments(R * grid.T, img.counts, img.ranges, img.cursor, img.chunk_base, img.hdr, s),
-             "scan");
+  if (P == 0) {   // no preprocess CTA to scan: empty segments
+    GS_CHECK(cudaMemsetAsync(img.ranges, 0, (size_t)R * grid.T * sizeof(uint2), s), "memset ranges");
+    GS_CHECK(cudaMemsetAsync(img.chunk_base, 0, ((size_t)R * grid.T + 1) * sizeof(uint32_t), s), "memset chunks");
   }
   if (num_rendered) {
     unsigned long long k = 0;
@@ -225,13 +226,12 @@ int gsparc_rasterize_render(int P, int R, int H, int W, int tile_h, int tile_w, 
   carve_image((char*)image_state, (size_t)R, (size_t)grid.T, (size_t)H * W, &img);
   BinningView bin{};
   carve_binning((char*)binning_state, (size_t)capacity, &bin);
-  {
+  if (P == 0) {
     Timed t(KID_CHECK, s);
     GS_CHECK(launch_check_capacity(img, (unsigned long long)capacity, s), "capacity check");
-  }
-  {
-    Timed t(KID_DEPTH_SORT, s);
-    GS_CHECK(launch_depth_sort(P, R, geo, img, s), "depth sort");
+  } else {
+    Timed t(KID_DEPTH_SORT, s);   // also records the capacity and flags K > capacity
+    GS_CHECK(launch_depth_sort(P, R, geo, img, (unsigned long long)capacity, s), "depth sort");
   }
   {
     Timed t(KID_SCATTER, s);

@@ -37,9 +37,9 @@ constexpr uint32_t kErrBadIndex = 1u << 2;   // a point list held an id >= P (ar
 constexpr uint32_t kErrSortWait = 1u << 3;   // a depth-sort look-back wait gave up (bounded spin)
 
 struct ImageHeader {
-  unsigned long long num_rendered;   // K, written by the scan kernel
+  unsigned long long num_rendered;   // K, written by the preprocess's last CTA (segment scan)
   unsigned int error;                // error bits, OR-ed by kernels
-  unsigned int pad;
+  unsigned int arrived;              // preprocess CTAs done (the last one scans the tile counts)
   unsigned long long capacity;       // binning capacity the render was given
   unsigned long long reserved[29];   // pad to 256 bytes
 };
@@ -182,9 +182,84 @@ __host__ __device__ inline GaussianLayout gaussian_layout(size_t P, size_t conf_
   return L;
 }
 
+// Exclusive scan of one value per thread over the CTA (any multiple of 32
+// threads up to 1024); every thread also receives the total.  warp_tot: 32
+// words of shared memory.
+template <typename V>
+__device__ __forceinline__ V cta_exclusive_scan(V local, V* warp_tot, V& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  V incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const V v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_tot[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    V w = lane < nw ? warp_tot[lane] : V(0);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const V v = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += v;
+    }
+    if (lane < nw) warp_tot[lane] = w;
+  }
+  __syncthreads();
+  const V excl = (wid ? warp_tot[wid - 1] : V(0)) + (incl - local);
+  total = warp_tot[nw - 1];
+  __syncthreads();
+  return excl;
+}
+
+// ---- scan of per-segment counts -> ranges, cursors, K, chunk bases ---------
+// Run by the preprocess's last CTA (preprocess.cu) (any block size) once every CTA's tile
+// counts have landed: n = R*T segments, each thread owns 8 consecutive
+// segments of every chunk of 8 * blockDim.x.
+__device__ __forceinline__ void scan_segments_cta(int n, const uint32_t* __restrict__ counts, uint2* __restrict__ ranges,
+                                  uint32_t* __restrict__ cursor, uint32_t* __restrict__ chunk_base,
+                                  ImageHeader* __restrict__ hdr) {
+  __shared__ unsigned long long warp_tot[32];
+  const int tid = threadIdx.x;
+  unsigned long long carry = 0, carry_b = 0;
+  for (int base = 0; base < n; base += (int)blockDim.x * 8) {
+    uint32_t c[8], nb[8];
+    unsigned long long local = 0, local_b = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = base + tid * 8 + k;
+      c[k] = i < n ? __ldcg(counts + i) : 0u;
+      nb[k] = c[k] ? (c[k] - 1u) / kBwdChunk : 0u;   // interior chunk boundaries of the segment
+      local += c[k];
+      local_b += nb[k];
+    }
+    unsigned long long tot, tot_b;
+    unsigned long long start = carry + cta_exclusive_scan<unsigned long long>(local, warp_tot, tot);
+    unsigned long long start_b = carry_b + cta_exclusive_scan<unsigned long long>(local_b, warp_tot, tot_b);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = base + tid * 8 + k;
+      if (i < n) {
+        // empty tiles keep the reference's zeroed range (rasterizer_impl.cu:303)
+        ranges[i] = c[k] ? make_uint2((uint32_t)start, (uint32_t)(start + c[k])) : make_uint2(0u, 0u);
+        cursor[i] = (uint32_t)start;
+        chunk_base[i] = (uint32_t)start_b;
+        start += c[k];
+        start_b += nb[k];
+      }
+    }
+    carry += tot;
+    carry_b += tot_b;
+  }
+  if (tid == 0) {
+    hdr->num_rendered = carry;
+    chunk_base[n] = (uint32_t)carry_b;
+  }
+}
+
 // Scratch of the fused training loss (ssim.cu), in floats.
 struct LossLayout {
-  size_t nblk, dmu1, ds11, ds12, partial, pre, coef, total;
+  size_t nblk, dmu1, ds11, ds12, partial, pre, coef, sync, total;
 };
 
 // ---------------------------------------------------------------------------

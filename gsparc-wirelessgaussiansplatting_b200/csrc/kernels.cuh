@@ -9,17 +9,17 @@ namespace gsparc {
 int report_invalid(const char* what);
 int report_cuda(cudaError_t e, const char* where);
 
+// Preprocess, tile counts and (last CTA) the segment scan: ranges, cursors,
+// chunk bases and K in the image header.
 cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, float mod, const float* means3D,
                               const float* mlp, const float* opacities, const float* scales,
                               const float* rotations, const float* views, const float* tx_pos,
-                              const float* rx_pos, const GeomView& geo, int* radii_out, uint32_t* counts,
+                              const float* rx_pos, const GeomView& geo, int* radii_out, const ImageView& img,
                               cudaStream_t stream);
 
 cudaError_t launch_mark_visible(int P, const float* means3D, const float* view, uint8_t* present,
                                 cudaStream_t stream);
 
-cudaError_t launch_scan_segments(int n, const uint32_t* counts, uint2* ranges, uint32_t* cursor,
-                                 uint32_t* chunk_base, ImageHeader* hdr, cudaStream_t stream);
 
 cudaError_t launch_check_capacity(ImageView img, unsigned long long capacity, cudaStream_t stream);
 
@@ -29,7 +29,10 @@ cudaError_t launch_scatter(int P, int R, const TileGrid& grid, const GeomView& g
 // Largest P the binning supports (the placement's rank bitmap lives in shared memory).
 constexpr int kMaxBinningP = 1 << 20;
 
-cudaError_t launch_depth_sort(int P, int R, const GeomView& geo, ImageView img, cudaStream_t stream);
+// Depth order of every receiver's Gaussians; also records the binning
+// capacity in the header and flags K > capacity.
+cudaError_t launch_depth_sort(int P, int R, const GeomView& geo, ImageView img, unsigned long long capacity,
+                              cudaStream_t stream);
 
 cudaError_t launch_segment_place(int P, int R, const TileGrid& grid, const GeomView& geo, ImageView img,
                                  BinningView bin, cudaStream_t stream);

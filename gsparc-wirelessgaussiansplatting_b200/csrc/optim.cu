@@ -17,7 +17,8 @@
 // Adam follows torch's update: m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2,
 // p -= (lr / bc1) * m / (sqrt(v) / sqrt(bc2) + eps), bc_i = 1 - b_i^t, with the
 // step count t and the learning rates read from device memory so the whole
-// update can be captured in a CUDA graph.
+// update can be captured in a CUDA graph.  All groups are updated by one
+// launch (train_adam_kernel).
 //
 // Flat layout of parameters, gradients and both moments (floats), each
 // segment starting on a 256-byte boundary (gaussian_layout):
@@ -35,9 +36,8 @@ struct AdamHyper {
   float lr, step_size, inv_sqrt_bc2, beta1, beta2, eps;
 };
 
-__device__ __forceinline__ AdamHyper adam_hyper(const float* lr6, int group, const float* step, float beta1,
-                                                float beta2, float eps) {
-  const float t = *step;
+__device__ __forceinline__ AdamHyper adam_hyper(const float* lr6, int group, float t, float beta1, float beta2,
+                                                float eps) {
   AdamHyper h;
   h.lr = lr6[group];
   const float bc1 = 1.0f - powf(beta1, t);
@@ -64,16 +64,12 @@ __device__ __forceinline__ void store_normalized(float* dst, const float q[4]) {
   for (int k = 0; k < 4; ++k) dst[k] = q[k] / nrm;
 }
 
-__global__ void adam_count_kernel(float* step) { *step += 1.0f; }
-
-__global__ void __launch_bounds__(256)
-gaussian_adam_kernel(int P, GaussianLayout L, float* __restrict__ params, const float* __restrict__ grads,
-                     float* __restrict__ m, float* __restrict__ v, const float* __restrict__ step,
-                     const float* __restrict__ lr6, float beta1, float beta2, float eps,
-                     const float* __restrict__ lo3, const float* __restrict__ hi3, float* __restrict__ act_s,
-                     float* __restrict__ act_q, float* __restrict__ act_o) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= P) return;
+__device__ __forceinline__ void gaussian_adam_body(int g, GaussianLayout L, float* __restrict__ params,
+                                                   const float* __restrict__ grads, float* __restrict__ m,
+                                                   float* __restrict__ v, float step, const float* __restrict__ lr6,
+                                                   float beta1, float beta2, float eps, const float* __restrict__ lo3,
+                                                   const float* __restrict__ hi3, float* __restrict__ act_s,
+                                                   float* __restrict__ act_q, float* __restrict__ act_o) {
   const size_t oC = L.centre, oS = L.scale, oQ = L.quat, oO = L.opacity;
   // centre: NaN-zeroed gradient, Adam, clamp
   {
@@ -166,15 +162,15 @@ gaussian_activate_kernel(int P, GaussianLayout L, const float* __restrict__ para
 // vectorised.  Indices below n_mlp use learning rate 4, the rest rate 5; both
 // segments start on a 256-byte boundary, so no float4 straddles them, and the
 // padding between them holds zeros that Adam leaves at zero.
-__global__ void __launch_bounds__(256)
-mlp_adam_kernel(size_t n, size_t n_mlp, float* __restrict__ params, const float* __restrict__ grads,
-                float* __restrict__ m, float* __restrict__ v, const float* __restrict__ step,
-                const float* __restrict__ lr6, float beta1, float beta2, float eps) {
+__device__ __forceinline__ void mlp_adam_body(int block, int nblocks, size_t n, size_t n_mlp,
+                                              float* __restrict__ params, const float* __restrict__ grads,
+                                              float* __restrict__ m, float* __restrict__ v, float step,
+                                              const float* __restrict__ lr6, float beta1, float beta2, float eps) {
   const AdamHyper h4 = adam_hyper(lr6, 4, step, beta1, beta2, eps);
   const AdamHyper h5 = (n > n_mlp) ? adam_hyper(lr6, 5, step, beta1, beta2, eps) : h4;
   const size_t n4 = n / 4;
-  const size_t stride = (size_t)gridDim.x * blockDim.x;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
+  const size_t stride = (size_t)nblocks * blockDim.x;
+  for (size_t i = block * (size_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
     const AdamHyper& h = (4 * i < n_mlp) ? h4 : h5;
     float4 p = reinterpret_cast<float4*>(params)[i];
     const float4 g = reinterpret_cast<const float4*>(grads)[i];
@@ -188,7 +184,7 @@ mlp_adam_kernel(size_t n, size_t n_mlp, float* __restrict__ params, const float*
     reinterpret_cast<float4*>(m)[i] = mm;
     reinterpret_cast<float4*>(v)[i] = vv;
   }
-  for (size_t i = n4 * 4 + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+  for (size_t i = n4 * 4 + block * (size_t)blockDim.x + threadIdx.x; i < n; i += stride) {
     const AdamHyper& h = (i < n_mlp) ? h4 : h5;
     float mi = m[i], vi = v[i];
     params[i] = adam_update(params[i], grads[i], mi, vi, h);
@@ -197,29 +193,49 @@ mlp_adam_kernel(size_t n, size_t n_mlp, float* __restrict__ params, const float*
   }
 }
 
+// One launch for the whole state: CTAs [0, nb_g) update the per-Gaussian
+// groups, the rest stream the MLP / global segments, so the short latency-bound
+// per-Gaussian work overlaps the bandwidth-bound MLP update.  Every CTA uses
+// step t = stored count + 1; the last CTA to finish (arrival counter in the
+// word after the count) stores t and clears the counter.
+__global__ void __launch_bounds__(256)
+train_adam_kernel(int P, GaussianLayout L, int nb_g, size_t n, size_t n_mlp, float* __restrict__ params,
+                  const float* __restrict__ grads, float* __restrict__ m, float* __restrict__ v,
+                  float* __restrict__ step, const float* __restrict__ lr6, float beta1, float beta2, float eps,
+                  const float* __restrict__ lo3, const float* __restrict__ hi3, float* __restrict__ act_s,
+                  float* __restrict__ act_q, float* __restrict__ act_o) {
+  const float t = __ldcg(step) + 1.0f;
+  if ((int)blockIdx.x < nb_g) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < P) gaussian_adam_body(g, L, params, grads, m, v, t, lr6, beta1, beta2, eps, lo3, hi3, act_s, act_q, act_o);
+  } else {
+    mlp_adam_body(blockIdx.x - nb_g, gridDim.x - nb_g, n, n_mlp, params + L.mlp, grads + L.mlp, m + L.mlp,
+                  v + L.mlp, t, lr6, beta1, beta2, eps);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned* arrived = reinterpret_cast<unsigned*>(step + 1);
+    __threadfence();
+    if (atomicAdd(arrived, 1u) == gridDim.x - 1) {
+      step[0] = t;
+      *arrived = 0u;
+    }
+  }
+}
+
 cudaError_t launch_gaussian_adam(int P, int conf_floats, float* params, const float* grads, float* m, float* v,
                                  float* step, const float* lr6, float beta1, float beta2, float eps,
                                  const float* lo3, const float* hi3, float* act_scales, float* act_rots,
                                  float* act_opac, cudaStream_t stream) {
-  adam_count_kernel<<<1, 1, 0, stream>>>(step);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
   const GaussianLayout L = gaussian_layout((size_t)P, (size_t)conf_floats);
-  if (P > 0) {
-    gaussian_adam_kernel<<<(P + 255) / 256, 256, 0, stream>>>(P, L, params, grads, m, v, step, lr6, beta1, beta2,
-                                                              eps, lo3, hi3, act_scales, act_rots, act_opac);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-  }
-  const size_t off = L.mlp;
   const size_t n_mlp = (size_t)kMlpFloats * P;
   const size_t n = conf_floats > 0 ? (L.conf - L.mlp) + (size_t)conf_floats : n_mlp;
-  if (n == 0) return cudaSuccess;
-  int blocks = (int)((n / 4 + 255) / 256);
-  if (blocks > 148 * 8) blocks = 148 * 8;
-  if (blocks < 1) blocks = 1;
-  mlp_adam_kernel<<<blocks, 256, 0, stream>>>(n, n_mlp, params + off, grads + off, m + off, v + off, step, lr6,
-                                              beta1, beta2, eps);
+  const int nb_g = (P + 255) / 256;
+  int nb_m = (int)((n / 4 + 255) / 256);
+  if (nb_m > 148 * 8) nb_m = 148 * 8;
+  if (nb_m < 1) nb_m = 1;
+  train_adam_kernel<<<nb_g + nb_m, 256, 0, stream>>>(P, L, nb_g, n, n_mlp, params, grads, m, v, step, lr6, beta1,
+                                                     beta2, eps, lo3, hi3, act_scales, act_rots, act_opac);
   return cudaGetLastError();
 }
 

@@ -7,7 +7,10 @@
 //   * receivers are batched on grid.y, outputs are receiver-major SoA;
 //   * the per-tile instance histogram the binning needs is accumulated here
 //     in shared memory (one global atomic per touched tile per block) instead
-//     of a separate scan over tiles_touched (rasterizer_impl.cu:270).
+//     of a separate scan over tiles_touched (rasterizer_impl.cu:270), and the
+//     last CTA to finish scans it into the tile ranges (no separate launch);
+//   * the depth key of every (receiver, Gaussian) and its digit histograms
+//     for the depth order (binning.cu) are produced here too.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -108,7 +111,8 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
                   const float* __restrict__ opacities, const float* __restrict__ scales,
                   const float* __restrict__ rotations, const float* __restrict__ views,
                   const float* __restrict__ tx_pos, const float* __restrict__ rx_pos,
-                  GeomView geo, int* __restrict__ radii_out, uint32_t* __restrict__ counts) {
+                  GeomView geo, int* __restrict__ radii_out, ImageView img) {
+  uint32_t* __restrict__ counts = img.counts;
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   float* sm_mlp = smem + wid * kMlpSmemPerWarp;
@@ -230,6 +234,18 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
     const uint32_t c = dhist[t];
     if (c) atomicAdd(&geo.sort_state[(size_t)r * 1024 + t], c);
   }
+  // the last CTA to finish scans the tile counts into segment ranges
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&img.hdr->arrived, 1u) == gridDim.x * gridDim.y - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    scan_segments_cta((int)gridDim.y * grid.T, counts, img.ranges, img.cursor, img.chunk_base, img.hdr);
+  }
 }
 
 // Range cull only (checkFrustum, rasterizer_impl.cu:173-185).
@@ -248,19 +264,23 @@ __global__ void mark_visible_kernel(int P, const float* __restrict__ means3D,
 
 // MLP staging (50,432 B) + digit counters (4 KB)
 constexpr size_t kMlpSmemBytes = (kPreThreads / 32) * kMlpSmemPerWarp * sizeof(float) + 1024 * sizeof(uint32_t);
-constexpr int kMaxSharedHistTiles = (int)((227 * 1024 - kMlpSmemBytes) / sizeof(uint32_t));
+// dynamic shared memory ceiling: 227 KB per CTA less 1 KB kept for the
+// kernel's static shared memory (the last CTA's scan)
+constexpr int kPreDynSmemMax = 226 * 1024;
+constexpr int kMaxSharedHistTiles = (int)((kPreDynSmemMax - kMlpSmemBytes) / sizeof(uint32_t));
 
 template <bool kSharedHist, bool kVec>
 static cudaError_t set_preprocess_smem(int dev) {
+  (void)dev;
   return cudaFuncSetAttribute(preprocess_kernel<kSharedHist, kVec>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              227 * 1024);
+                              kPreDynSmemMax);
 }
 
 cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, float mod,
                               const float* means3D, const float* mlp, const float* opacities,
                               const float* scales, const float* rotations, const float* views,
                               const float* tx_pos, const float* rx_pos, const GeomView& geo,
-                              int* radii_out, uint32_t* counts, cudaStream_t stream) {
+                              int* radii_out, const ImageView& img, cudaStream_t stream) {
   if (P == 0 || R == 0) return cudaSuccess;
   // the shared-memory opt-in is set once per device, so later calls (including
   // ones made while a CUDA graph is being captured) only enqueue the launch
@@ -282,20 +302,20 @@ cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, 
     if (vec)
       preprocess_kernel<true, true><<<gridd, block, smem, stream>>>(P, H, W, grid, mod, means3D, mlp, opacities,
                                                                     scales, rotations, views, tx_pos, rx_pos, geo,
-                                                                    radii_out, counts);
+                                                                    radii_out, img);
     else
       preprocess_kernel<true, false><<<gridd, block, smem, stream>>>(P, H, W, grid, mod, means3D, mlp, opacities,
                                                                      scales, rotations, views, tx_pos, rx_pos, geo,
-                                                                     radii_out, counts);
+                                                                     radii_out, img);
   } else {
     if (vec)
       preprocess_kernel<false, true><<<gridd, block, kMlpSmemBytes, stream>>>(
           P, H, W, grid, mod, means3D, mlp, opacities, scales, rotations, views, tx_pos, rx_pos, geo, radii_out,
-          counts);
+          img);
     else
       preprocess_kernel<false, false><<<gridd, block, kMlpSmemBytes, stream>>>(
           P, H, W, grid, mod, means3D, mlp, opacities, scales, rotations, views, tx_pos, rx_pos, geo, radii_out,
-          counts);
+          img);
   }
   return cudaGetLastError();
 }

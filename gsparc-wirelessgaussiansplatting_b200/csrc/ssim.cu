@@ -163,9 +163,10 @@ ssim_backward_kernel(int H, int W, const float* __restrict__ img1, const float* 
 //   conf_r  = 1 + exp(fc2(relu(fc1(rx_r))))              (gaussian.py:575-609)
 //   loss    = mean_r (conf_r recon_r - alpha log conf_r)
 // and its adjoint with respect to pred and the confidence-MLP parameters,
-// in three launches: tile moments + per-tile partial sums, a one-CTA head
-// (reductions, MLP forward/backward, per-receiver gradient scales) and the
-// SSIM/L1 backward with the per-receiver scales applied while staging.
+// in two launches: tile moments + per-tile partial sums, whose last CTA runs
+// the head (reductions, MLP forward/backward, per-receiver gradient scales),
+// then the SSIM/L1 backward with the per-receiver scales applied while
+// staging.
 // Every reduction has a fixed order, so the loss is deterministic.
 // ---------------------------------------------------------------------------
 
@@ -175,11 +176,22 @@ __device__ __forceinline__ float warp_sum_all(float v) {
   return v;
 }
 
+__device__ __forceinline__ void loss_head_body(int R, int nblk, int HW, int hidden, float lambda1, float alpha,
+                                               const float* __restrict__ rx, const float* __restrict__ cp,
+                                               const float2* __restrict__ partial, float* __restrict__ pre,
+                                               float4* __restrict__ coef, float* __restrict__ terms,
+                                               float* __restrict__ loss_out, float* __restrict__ dconf);
+
+// Tile moments, SSIM partial derivatives and per-tile partial sums; the last
+// CTA to finish (arrival counter in the scratch) runs the head.
 __global__ void __launch_bounds__(256)
 loss_forward_kernel(int H, int W, float C1, float C2, const float* __restrict__ pred,
                     const float* __restrict__ target, float* __restrict__ dm_dmu1,
                     float* __restrict__ dm_dsigma1_sq, float* __restrict__ dm_dsigma12,
-                    float2* __restrict__ partial) {
+                    float2* __restrict__ partial, int hidden, float lambda1, float alpha,
+                    const float* __restrict__ rx, const float* __restrict__ cp, float* __restrict__ pre,
+                    float4* __restrict__ coef, float* __restrict__ terms, float* __restrict__ loss_out,
+                    float* __restrict__ dconf, unsigned* __restrict__ arrived) {
   __shared__ float s1[kTH][kTW + 1];
   __shared__ float s2[kTH][kTW + 1];
   __shared__ float hx[5][kTH][kSW];
@@ -244,14 +256,26 @@ loss_forward_kernel(int H, int W, float C1, float C2, const float* __restrict__ 
     for (int w = 0; w < 8; ++w) { a += red[0][w]; b += red[1][w]; }
     partial[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = make_float2(a, b);
   }
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(arrived, 1u) == gridDim.x * gridDim.y * gridDim.z - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    loss_head_body(gridDim.z, gridDim.x * gridDim.y, H * W, hidden, lambda1, alpha, rx, cp, partial, pre, coef,
+                   terms, loss_out, dconf);
+    if (threadIdx.x == 0) *arrived = 0u;
+  }
 }
 
 // One CTA: warp per receiver for the reductions and the confidence MLP
 // forward, then thread per MLP parameter for its gradient (sum over
 // receivers in receiver order).  coef[r] = (dL/dpred scale of the L1 term,
 // dL/dmap of the SSIM term, loss_r, dL/draw_r).
-__global__ void __launch_bounds__(256)
-loss_head_kernel(int R, int nblk, int HW, int hidden, float lambda1, float alpha, const float* __restrict__ rx,
+__device__ __forceinline__ void loss_head_body(int R, int nblk, int HW, int hidden, float lambda1, float alpha,
+                                               const float* __restrict__ rx,
                  const float* __restrict__ cp, const float2* __restrict__ partial, float* __restrict__ pre,
                  float4* __restrict__ coef, float* __restrict__ terms, float* __restrict__ loss_out,
                  float* __restrict__ dconf) {
@@ -264,7 +288,7 @@ loss_head_kernel(int R, int nblk, int HW, int hidden, float lambda1, float alpha
   for (int r = warp; r < R; r += 8) {
     float a = 0.0f, b = 0.0f;
     for (int i = lane; i < nblk; i += 32) {
-      const float2 p = partial[(size_t)r * nblk + i];
+      const float2 p = __ldcg(partial + (size_t)r * nblk + i);   // written by other CTAs
       a += p.x;
       b += p.y;
     }
@@ -391,7 +415,8 @@ LossLayout loss_layout(size_t R, size_t H, size_t W, size_t hidden) {
   L.partial = L.ds12 + a(n);
   L.pre = L.partial + a(2 * R * L.nblk);
   L.coef = L.pre + a(R * hidden);
-  L.total = L.coef + a(4 * R);
+  L.sync = L.coef + a(4 * R);
+  L.total = L.sync + 64;
   return L;
 }
 
@@ -404,12 +429,10 @@ cudaError_t launch_splat_loss(int R, int H, int W, int hidden, float lambda1, fl
   float2* partial = reinterpret_cast<float2*>(scratch + L.partial);
   float4* coef = reinterpret_cast<float4*>(scratch + L.coef);
   loss_forward_kernel<<<grid, 256, 0, stream>>>(H, W, C1, C2, pred, target, scratch + L.dmu1, scratch + L.ds11,
-                                                scratch + L.ds12, partial);
+                                                scratch + L.ds12, partial, hidden, lambda1, alpha, rx, conf_params,
+                                                scratch + L.pre, coef, terms, loss_out, dconf,
+                                                reinterpret_cast<unsigned*>(scratch + L.sync));
   cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  loss_head_kernel<<<1, 256, 0, stream>>>(R, (int)L.nblk, H * W, hidden, lambda1, alpha, rx, conf_params, partial,
-                                          scratch + L.pre, coef, terms, loss_out, dconf);
-  e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   loss_backward_kernel<<<grid, 256, 0, stream>>>(H, W, pred, target, scratch + L.dmu1, scratch + L.ds11,
                                                  scratch + L.ds12, coef, dL_dpred);

@@ -104,7 +104,7 @@ class FusedTrainer:
         self.act_scales = torch.empty((P, 3), dtype=torch.float32, device=dev)
         self.act_rots = torch.empty((P, 4), dtype=torch.float32, device=dev)
         self.act_opac = torch.empty((P,), dtype=torch.float32, device=dev)
-        self.step_count = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.step_count = torch.zeros(2, dtype=torch.float32, device=dev)   # step, arrival counter (0)
         self.lr6 = torch.tensor(lr, dtype=torch.float32, device=dev)
         self.lo3 = torch.tensor(scenes.ROOM_LO, dtype=torch.float32, device=dev)
         self.hi3 = torch.tensor(scenes.ROOM_HI, dtype=torch.float32, device=dev)

@@ -10,7 +10,7 @@ Per receiver (train.py:420-436):
 
 and for a batch of R receivers the mean of the per-receiver losses.
 ``gsparc_splat_loss`` evaluates all of it and its gradients with respect to
-the rendered spectra and the confidence-MLP parameters in three launches,
+the rendered spectra and the confidence-MLP parameters in two launches,
 replacing the ~45 small torch kernels of the autograd formulation.
 """
 from __future__ import annotations
@@ -42,7 +42,7 @@ class SplatLoss:
         self.lambda1, self.alpha = float(lambda1), float(alpha)
         dev = torch.device(device)
         n = int(_lib.lib().gsparc_splat_loss_scratch_floats(self.R, self.H, self.W, self.hidden))
-        self.scratch = torch.empty(max(n, 1), dtype=torch.float32, device=dev)
+        self.scratch = torch.zeros(max(n, 1), dtype=torch.float32, device=dev)   # zero once: arrival counter
         self.loss = torch.zeros((), dtype=torch.float32, device=dev)
         self.terms = torch.zeros((self.R, 4), dtype=torch.float32, device=dev)
         self.dpred = torch.empty((self.R, self.H, self.W), dtype=torch.float32, device=dev)

@@ -202,7 +202,9 @@ GSPARC_API size_t gsparc_splat_loss_scratch_floats(int R, int H, int W, int hidd
  * [hidden], fc2.weight [1,hidden], fc2.bias [1]: 5*hidden+1 floats);
  * dL_dconf_params: same layout, overwritten; loss_out: 1 float; terms:
  * optional [R,4] (l1, ssim, conf, loss_r); scratch: 16-byte aligned,
- * gsparc_splat_loss_scratch_floats floats.  All device memory. */
+ * gsparc_splat_loss_scratch_floats floats, zero-filled before its first use
+ * (it holds an arrival counter that every call leaves at zero).  All device
+ * memory. */
 GSPARC_API int gsparc_splat_loss(int R, int H, int W, int hidden, float lambda1, float alpha,
                                  float C1, float C2, const float* pred, const float* target,
                                  const float* rx_pos, const float* conf_params, float* scratch,
@@ -236,8 +238,9 @@ GSPARC_API int gsparc_gaussian_activate(int P, const float* params, float* scale
  * params, exp_avg, exp_avg_sq: flat state buffers (raw parameters), updated in
  * place; grads: same layout, gradients with respect to the ACTIVATED values
  * (as gsparc_rasterize_backward returns them) and, in the global block, with
- * respect to its parameters; step_count: device float, incremented by this
- * call; lr6: device floats (centre, scale, rotation, opacity, emission MLP,
+ * respect to its parameters; step_count: two device words, the step count
+ * (float, incremented by this call) and a 32-bit arrival counter that must be
+ * 0 before the first call (every call leaves it at 0); lr6: device floats (centre, scale, rotation, opacity, emission MLP,
  * global block); centre_lo3 / centre_hi3: device clamp box.  scales,
  * rotations, opacities: optional (all or none) outputs of the activated
  * updated parameters, as gsparc_gaussian_activate writes them.  State buffers
