@@ -46,14 +46,15 @@ bool valid_tile(int th, int tw) {
 // ---- optional per-kernel timing (CUDA events around each launch) ----------
 enum KernelId {
   KID_PREPROCESS, KID_CHECK, KID_SCATTER, KID_DEPTH_SORT, KID_PLACE, KID_BLEND_FWD, KID_BLEND_BWD,
-  KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_ADAM, KID_LOSS, KID_ACTIVATE,
+  KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_ADAM, KID_LOSS, KID_ACTIVATE, KID_SHARED_MLP, KID_SHARED_MLP_BWD,
   KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
     "preprocess_kernel", "check_capacity_kernel", "scatter_kernel",
     "depth_sort_kernels", "segment_place_kernel", "blend_forward_kernel", "blend_backward_kernel", "geometry_backward_kernel",
     "emission_backward_kernel", "ssim_forward_kernel", "ssim_backward_kernel", "mark_visible_kernel",
-    "gaussian_adam_kernels", "splat_loss_kernels", "gaussian_activate_kernel"};
+    "gaussian_adam_kernels", "splat_loss_kernels", "gaussian_activate_kernel", "shared_mlp_forward_kernels",
+    "shared_mlp_backward_kernels"};
 
 struct PendingTiming {
   int id;
@@ -178,7 +179,7 @@ int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w,
   if (R > 65535) return invalid("R above 65535 receivers per call");
   if (!valid_tile(tile_h, tile_w)) return invalid("tile shape must be 16x16, 8x32 or 32x8");
   if (!image_state || !viewmatrices || !tx_pos || !rx_pos) return invalid("null state or receiver pointer");
-  if (P > 0 && (!geom_state || !means3D || !emission_mlps || !opacities || !scales || !rotations))
+  if (P > 0 && (!geom_state || !means3D || !opacities || !scales || !rotations))
     return invalid("null Gaussian pointer");
   cudaStream_t s = (cudaStream_t)stream;
   TileGrid grid(H, W, tile_h, tile_w);
@@ -276,10 +277,11 @@ int gsparc_rasterize_backward(int P, int R, int H, int W, int tile_h, int tile_w
   if (!image_state || !dL_dout_real || !dL_dout_imag || !viewmatrices || !tx_pos || !rx_pos)
     return invalid("null image state, upstream gradient or receiver pointer");
   if (P == 0) return GSPARC_OK;
-  if (!geom_state || !means3D || !emission_mlps || !scales || !rotations || !dL_dmeans2D || !dL_dconic ||
-      !dL_dsignal || !dL_dopacity || !dL_dmeans3D || !dL_dcov3D || !dL_dscales || !dL_drotations ||
-      !dL_demission_mlps)
+  if (!geom_state || !means3D || !scales || !rotations || !dL_dmeans2D || !dL_dconic || !dL_dsignal ||
+      !dL_dopacity || !dL_dmeans3D || !dL_dcov3D || !dL_dscales || !dL_drotations)
     return invalid("null Gaussian input or gradient output");
+  if ((emission_mlps == nullptr) != (dL_demission_mlps == nullptr))
+    return invalid("emission_mlps and dL_demission_mlps: give both (per-Gaussian MLP) or neither (shared MLP)");
   if (binning_capacity > 0 && !binning_state) return invalid("null binning state");
   cudaStream_t s = (cudaStream_t)stream;
   TileGrid grid(H, W, tile_h, tile_w);
@@ -307,12 +309,77 @@ int gsparc_rasterize_backward(int P, int R, int H, int W, int tile_h, int tile_w
                                       dL_drotations, s),
              "geometry backward");
   }
-  {
+  if (emission_mlps) {
     Timed t(KID_MLP_BWD, s);
     GS_CHECK(launch_emission_backward(P, R, means3D, emission_mlps, tx_pos, rx_pos, geo.radii, dL_dsignal,
                                       dL_demission_mlps, dL_dmeans3D, s),
              "emission backward");
   }
+  return GSPARC_OK;
+}
+
+// ---- shared emission MLP -------------------------------------------------------
+
+namespace {
+int check_mlp_spec(int layers, int width, int act, int out, int precision) {
+  if (layers < 1 || layers > kMaxMlpLayers) return invalid("layers must be in [1, 6]");
+  if (width < 8 || width > 256) return invalid("width must be in [8, 256]");
+  if (act != GSPARC_ACT_RELU && act != GSPARC_ACT_GELU) return invalid("act must be GSPARC_ACT_RELU or _GELU");
+  if (out != 1) return invalid("out must be 1 (one amplitude per pair)");
+  if (precision != GSPARC_MLP_FP32) return invalid("precision must be GSPARC_MLP_FP32");
+  return GSPARC_OK;
+}
+}  // namespace
+
+size_t gsparc_shared_mlp_param_floats(int layers, int width, int out) {
+  if (layers < 1 || layers > kMaxMlpLayers || width < 1 || out < 1) return 0;
+  return shared_mlp_layout(layers, width, out, 0).params;
+}
+
+size_t gsparc_shared_mlp_workspace_floats(int P, int R, int layers, int width, int out) {
+  if (P < 0 || R < 0 || layers < 1 || layers > kMaxMlpLayers || width < 1 || out < 1) return 0;
+  return shared_mlp_layout(layers, width, out, (size_t)P * R).work;
+}
+
+int gsparc_shared_mlp_forward(int P, int R, int layers, int width, int act, int out, int precision,
+                              const float* means3D, const float* rx_pos, const float* params, void* geom_state,
+                              float* workspace, void* stream) {
+  if (P < 0 || R < 1) return invalid("sizes");
+  int st = check_mlp_spec(layers, width, act, out, precision);
+  if (st != GSPARC_OK) return st;
+  if (P == 0) return GSPARC_OK;
+  if (!means3D || !rx_pos || !params || !geom_state || !workspace) return invalid("null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  GeomView geo;
+  carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
+  Timed t(KID_SHARED_MLP, s);
+  GS_CHECK(launch_shared_mlp_forward(P, R, layers, width, act, out, means3D, rx_pos, params, geo, workspace, s),
+           "shared mlp forward");
+  return GSPARC_OK;
+}
+
+int gsparc_shared_mlp_backward(int P, int R, int layers, int width, int act, int out, int precision,
+                               const float* means3D, const float* rx_pos, const float* params,
+                               const void* geom_state, float* workspace, const float* dL_dsignal,
+                               float* dL_dparams, float* dL_dmeans3D, void* stream) {
+  if (P < 0 || R < 1) return invalid("sizes");
+  int st = check_mlp_spec(layers, width, act, out, precision);
+  if (st != GSPARC_OK) return st;
+  if (!dL_dparams) return invalid("null dL_dparams");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (P == 0) {
+    GS_CHECK(cudaMemsetAsync(dL_dparams, 0, shared_mlp_layout(layers, width, out, 0).params * sizeof(float), s),
+             "memset dL_dparams");
+    return GSPARC_OK;
+  }
+  if (!means3D || !rx_pos || !params || !geom_state || !workspace || !dL_dsignal || !dL_dmeans3D)
+    return invalid("null pointer");
+  GeomView geo;
+  carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
+  Timed t(KID_SHARED_MLP_BWD, s);
+  GS_CHECK(launch_shared_mlp_backward(P, R, layers, width, act, out, means3D, rx_pos, params, geo, workspace,
+                                      dL_dsignal, dL_dparams, dL_dmeans3D, s),
+           "shared mlp backward");
   return GSPARC_OK;
 }
 

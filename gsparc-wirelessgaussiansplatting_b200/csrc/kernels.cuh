@@ -79,4 +79,23 @@ cudaError_t launch_ssim_backward(int planes, int H, int W, const float* img1, co
                                  const float* dmu1, const float* ds11, const float* ds12, float* dL_dimg1,
                                  cudaStream_t stream);
 
+// Shared emission MLP (shared_mlp.cu): parameter and workspace offsets in
+// floats; layers = hidden layers (at most kMaxMlpLayers).
+constexpr int kMaxMlpLayers = 6;
+struct SharedMlpLayout {
+  int layers, width, out;
+  size_t w[kMaxMlpLayers + 1], b[kMaxMlpLayers + 1], params;
+  size_t x0, z[kMaxMlpLayers + 1], a[kMaxMlpLayers + 1], o, s, d0, d1, work;
+};
+SharedMlpLayout shared_mlp_layout(int layers, int width, int out, size_t rows);
+
+cudaError_t launch_shared_mlp_forward(int P, int R, int layers, int width, int act, int out, const float* means3D,
+                                      const float* rx_pos, const float* params, const GeomView& geo, float* work,
+                                      cudaStream_t s);
+
+cudaError_t launch_shared_mlp_backward(int P, int R, int layers, int width, int act, int out, const float* means3D,
+                                       const float* rx_pos, const float* params, const GeomView& geo, float* work,
+                                       const float* dL_dsignal, float* dL_dparams, float* dL_dmeans3D,
+                                       cudaStream_t s);
+
 }  // namespace gsparc

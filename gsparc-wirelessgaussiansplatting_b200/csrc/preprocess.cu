@@ -205,7 +205,8 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
     for (int pass = 0; pass < 4; ++pass) atomicAdd(&dhist[pass * 256 + ((dkey >> (8 * pass)) & 255u)], 1u);
   }
   // emission MLP of the visible Gaussians, from the warp's staged parameters
-  if (__any_sync(0xffffffffu, vis)) {
+  // (no per-Gaussian MLP: the signal is written later by the shared MLP)
+  if (mlp != nullptr && __any_sync(0xffffffffu, vis)) {
     stage_mlp<kVec>(sm_mlp, mlp, P, blockIdx.x * blockDim.x + wid * 32, lane);
     __syncwarp();
     if (vis) {

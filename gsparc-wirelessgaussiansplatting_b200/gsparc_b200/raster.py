@@ -91,13 +91,16 @@ def _receivers(viewmatrices, rx_pos, device):
 
 def forward(means3D, emission_mlps, opacities, scales, rotations, H, W, scale_modifier,
             viewmatrices, tx_pos, rx_pos, tile=None, capacity=None, binning=None,
-            out_real=None, out_imag=None, radii=None, geom=None, image=None):
+            out_real=None, out_imag=None, radii=None, geom=None, image=None, shared=None, shared_params=None):
     """Render R spectra.  Returns (out_real [R,H,W], out_imag [R,H,W], radii [R,P] int32, ForwardState).
 
     With ``capacity=None`` the instance count K is read back (one host sync,
     as the reference does) and the binning arena is sized exactly.  With a
     capacity the call stays asynchronous (graph-capturable); an overflow is
-    reported by ``read_status``.  Preallocated arenas/outputs may be passed."""
+    reported by ``read_status``.  Preallocated arenas/outputs may be passed.
+    With ``shared`` (a ``SharedMLP``) and its flat ``shared_params`` the
+    signals come from the shared emission MLP and ``emission_mlps`` must be
+    None."""
     if means3D.dim() != 2 or means3D.shape[1] != 3:
         raise RuntimeError("means3D must have dimensions (num_points, 3)")
     device = means3D.device
@@ -110,10 +113,19 @@ def forward(means3D, emission_mlps, opacities, scales, rotations, H, W, scale_mo
     tx = _dev_f32(tx_pos, "tx_pos", device).reshape(-1)
     if tx.numel() != 3:
         raise ValueError("tx_pos must have 3 elements")
+    if shared is not None and emission_mlps is not None:
+        raise ValueError("pass either emission_mlps (per-Gaussian MLP) or shared (shared MLP), not both")
     if P > 0:
-        mlp = _dev_f32(emission_mlps, "emission_mlps", device).reshape(-1)
-        if mlp.numel() != MLP_FLOATS * P:
-            raise ValueError(f"emission_mlps must hold {MLP_FLOATS}*P = {MLP_FLOATS * P} floats, got {mlp.numel()}")
+        if shared is None:
+            mlp = _dev_f32(emission_mlps, "emission_mlps", device).reshape(-1)
+            if mlp.numel() != MLP_FLOATS * P:
+                raise ValueError(f"emission_mlps must hold {MLP_FLOATS}*P = {MLP_FLOATS * P} floats, "
+                                 f"got {mlp.numel()}")
+        else:
+            mlp = None
+            shared_params = _dev_f32(shared_params, "shared_params", device).reshape(-1)
+            if shared_params.numel() != shared.n_params:
+                raise ValueError(f"shared_params must hold {shared.n_params} floats")
         op = _dev_f32(opacities, "opacities", device).reshape(-1)
         sc = _dev_f32(scales, "scales", device).reshape(P, 3)
         rot = _dev_f32(rotations, "rotations", device).reshape(P, 4)
@@ -138,6 +150,8 @@ def forward(means3D, emission_mlps, opacities, scales, rotations, H, W, scale_mo
         P, R, H, W, tile[0], tile[1], float(scale_modifier), ptr(m), ptr(mlp), ptr(op), ptr(sc), ptr(rot),
         ptr(v), ptr(tx), ptr(rx), ptr(radii), ptr(geom), ptr(image),
         ctypes.byref(K) if capacity is None else None, stream))
+    if shared is not None:
+        shared.forward(P, R, m, rx, shared_params, geom)
     if capacity is None:
         capacity = int(K.value)
         num_rendered = capacity
@@ -163,10 +177,12 @@ def read_status(st: ForwardState):
 
 
 def backward(st: ForwardState, means3D, emission_mlps, scales, rotations, scale_modifier,
-             viewmatrices, tx_pos, rx_pos, dL_dout_real, dL_dout_imag, grad_mode=None, out=None):
+             viewmatrices, tx_pos, rx_pos, dL_dout_real, dL_dout_imag, grad_mode=None, out=None,
+             shared=None, shared_params=None):
     """Adjoint of ``forward``.  Returns a dict of gradient tensors:
     dmeans2D [R,P,3], dconic [R,P,4], dsignal [R,P,2], dopacity [P],
-    dmeans3D [P,3], dcov3D [P,6], dscales [P,3], drotations [P,4], dmlp [194*P]."""
+    dmeans3D [P,3], dcov3D [P,6], dscales [P,3], drotations [P,4], dmlp [194*P]
+    (per-Gaussian MLP) or dshared [n_params] (``shared``)."""
     device = means3D.device
     P, R, H, W = st.P, st.R, st.H, st.W
     mode = _grad_mode if grad_mode is None else {"reference": _lib.GRAD_REFERENCE, "exact": _lib.GRAD_EXACT}.get(grad_mode, grad_mode)
@@ -178,13 +194,16 @@ def backward(st: ForwardState, means3D, emission_mlps, scales, rotations, scale_
     if out is None:
         z = lambda *s: torch.empty(s, dtype=torch.float32, device=device)
         out = dict(dmeans2D=z(R, P, 3), dconic=z(R, P, 4), dsignal=z(R, P, 2), dopacity=z(P),
-                   dmeans3D=z(P, 3), dcov3D=z(P, 6), dscales=z(P, 3), drotations=z(P, 4),
-                   dmlp=z(MLP_FLOATS * P))
+                   dmeans3D=z(P, 3), dcov3D=z(P, 6), dscales=z(P, 3), drotations=z(P, 4))
+        if shared is None:
+            out["dmlp"] = z(MLP_FLOATS * P)
+        else:
+            out["dshared"] = z(shared.n_params)
     if P == 0:
         for t in out.values():
             t.zero_()
         return out
-    mlp = _dev_f32(emission_mlps, "emission_mlps", device).reshape(-1)
+    mlp = _dev_f32(emission_mlps, "emission_mlps", device).reshape(-1) if shared is None else None
     sc = _dev_f32(scales, "scales", device).reshape(P, 3)
     rot = _dev_f32(rotations, "rotations", device).reshape(P, 4)
     L = _lib.lib()
@@ -194,7 +213,10 @@ def backward(st: ForwardState, means3D, emission_mlps, scales, rotations, scale_
         ptr(st.geom), ptr(st.image), ptr(st.binning), int(st.capacity), ptr(g_r), ptr(g_i),
         ptr(out["dmeans2D"]), ptr(out["dconic"]), ptr(out["dsignal"]), ptr(out["dopacity"]),
         ptr(out["dmeans3D"]), ptr(out["dcov3D"]), ptr(out["dscales"]), ptr(out["drotations"]),
-        ptr(out["dmlp"]), stream_of(device)))
+        ptr(out["dmlp"]) if shared is None else None, stream_of(device)))
+    if shared is not None:
+        sp = _dev_f32(shared_params, "shared_params", device).reshape(-1)
+        shared.backward(P, R, m, rx, sp, st.geom, out["dsignal"], out["dshared"], out["dmeans3D"])
     return out
 
 

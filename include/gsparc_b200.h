@@ -182,6 +182,41 @@ GSPARC_API int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float
                          const float* dm_dmu1, const float* dm_dsigma1_sq,
                          const float* dm_dsigma12, float* dL_dimg1, void* stream);
 
+/* ---- shared emission MLP ------------------------------------------------ */
+
+/* The benchmark configurations' emission model: one MLP shared by all
+ * Gaussians, evaluated per (receiver, Gaussian) pair on 32 features (centre,
+ * 4-frequency positional encoding of the centre, receiver-relative
+ * direction, 1/d^2, one zero pad), `layers` hidden layers of `width` with
+ * ReLU or GELU, a linear output; the pair's signal is sigmoid(output), real
+ * channel (imaginary 0).  No counterpart in the reference, whose emission
+ * model is the per-Gaussian 3-32-2 MLP (forward.cu:17-75); to use it, call
+ * gsparc_rasterize_prepare with emission_mlps = NULL (signal left unset),
+ * then gsparc_shared_mlp_forward, then gsparc_rasterize_render; in the
+ * backward pass emission_mlps = dL_demission_mlps = NULL and follow
+ * gsparc_rasterize_backward with gsparc_shared_mlp_backward.
+ * params: flat fp32, per layer W [out, in] row-major then b [out].
+ * workspace: gsparc_shared_mlp_workspace_floats floats; the forward keeps
+ * the activations there for the backward.  out must be 1. */
+#define GSPARC_ACT_RELU 1
+#define GSPARC_ACT_GELU 2
+#define GSPARC_MLP_FP32 0
+GSPARC_API size_t gsparc_shared_mlp_param_floats(int layers, int width, int out);
+GSPARC_API size_t gsparc_shared_mlp_workspace_floats(int P, int R, int layers, int width, int out);
+/* Writes the signal of every visible pair into the geometry arena of a
+ * prepared forward. */
+GSPARC_API int gsparc_shared_mlp_forward(int P, int R, int layers, int width, int act, int out,
+                                         int precision, const float* means3D, const float* rx_pos,
+                                         const float* params, void* geom_state, float* workspace,
+                                         void* stream);
+/* dL_dsignal [R,P,2] as gsparc_rasterize_backward returns it; dL_dparams is
+ * overwritten; dL/dmeans3D through the features is ADDED to dL_dmeans3D. */
+GSPARC_API int gsparc_shared_mlp_backward(int P, int R, int layers, int width, int act, int out,
+                                          int precision, const float* means3D, const float* rx_pos,
+                                          const float* params, const void* geom_state, float* workspace,
+                                          const float* dL_dsignal, float* dL_dparams,
+                                          float* dL_dmeans3D, void* stream);
+
 /* ---- training loss ------------------------------------------------------ */
 
 /* Scratch floats gsparc_splat_loss needs for R spectra of H x W and a

@@ -1,0 +1,95 @@
+"""GPU tests of the shared emission MLP (the benchmark configurations' model)
+against a plain PyTorch fp32 reference of the same network with autograd:
+features (centre, 4-frequency positional encoding, receiver-relative
+direction, 1/d^2), hidden layers, sigmoid of the output.
+
+Tolerances (fp32): signals within 2e-6 absolute (they lie in (0, 1));
+parameter and centre gradients within 1e-4 of each tensor's largest
+magnitude."""
+import math
+
+import numpy as np
+import pytest
+import torch
+import torch.nn.functional as F
+
+from gsparc_b200 import raster, scenes
+from gsparc_b200.shared_mlp import SharedMLP
+
+pytestmark = pytest.mark.gpu
+
+
+def torch_features(means, rxs, radii):
+    R, P = radii.shape
+    m = means[None].expand(R, P, 3)
+    v = m - rxs[:, None, :]
+    d2 = (v * v).sum(-1, keepdim=True)
+    d = d2.sqrt()
+    pe = []
+    for k in range(4):
+        w = (2 ** k) * math.pi
+        for j in range(3):
+            pe += [torch.sin(w * m[..., j]), torch.cos(w * m[..., j])]
+    x = torch.cat([m, torch.stack(pe, -1), v / d, 1.0 / d2, torch.zeros_like(d)], -1)
+    return torch.where((radii > 0)[..., None], x, torch.zeros_like(x))
+
+
+def torch_signal(mlp, params, means, rxs, radii):
+    h = torch_features(means, rxs, radii)
+    layers = mlp.unflatten(params)
+    act = F.relu if mlp.act == "relu" else F.gelu
+    for w, b in layers[:-1]:
+        h = act(h @ w.T + b)
+    w, b = layers[-1]
+    return torch.sigmoid((h @ w.T + b)[..., 0])
+
+
+def _scene(P, R, seed):
+    dev = torch.device("cuda")
+    sc = scenes.make_scene(P, seed=seed)
+    rx = scenes.make_receivers(R)
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
+    m, s, q, o = sc.activated()
+    return dict(means=t(m), scales=t(s), rots=t(q), opac=t(o.reshape(-1)), views=t(scenes.view_matrices(rx)),
+                rxs=t(rx), tx=t(scenes.TX_POS))
+
+
+@pytest.mark.parametrize("layers,width,act,R", [(2, 64, "relu", 1), (3, 128, "gelu", 3), (2, 64, "relu", 2)])
+def test_shared_mlp_forward_and_backward_match_torch(layers, width, act, R):
+    torch.backends.cuda.matmul.allow_tf32 = False
+    P = 3001
+    sc = _scene(P, R, seed=4)
+    mlp = SharedMLP(layers, width, act)
+    params = mlp.init_params(seed=layers * 10 + R)
+    out_r, _, radii, st = raster.forward(sc["means"], None, sc["opac"], sc["scales"], sc["rots"], 90, 360, 1.0,
+                                         sc["views"], sc["tx"], sc["rxs"], shared=mlp, shared_params=params)
+    torch.cuda.synchronize()
+    assert st.num_rendered > 0
+    sig = raster.state_views(st)["signal"]
+    ref = torch_signal(mlp, params, sc["means"], sc["rxs"], radii)
+    vis = radii > 0
+    assert vis.any()
+    assert (sig[..., 0][vis] - ref[vis]).abs().max().item() <= 2e-6
+    assert (sig[..., 1][vis] == 0).all()
+    # backward of sum(dsig * signal) through the MLP and the features
+    gen = torch.Generator().manual_seed(5)
+    dsig = torch.randn((R, P, 2), generator=gen).cuda() * vis[..., None]
+    dparams = torch.empty_like(params)
+    dmeans = torch.zeros_like(sc["means"])
+    mlp.backward(P, R, sc["means"], sc["rxs"], params, st.geom, dsig.contiguous(), dparams, dmeans)
+    torch.cuda.synchronize()
+    p = params.detach().clone().requires_grad_(True)
+    mm = sc["means"].detach().clone().requires_grad_(True)
+    (dsig[..., 0] * torch_signal(mlp, p, mm, sc["rxs"], radii)).sum().backward()
+    for (gw, gb), (rw, rb) in zip(mlp.unflatten(dparams), mlp.unflatten(p.grad)):
+        for a, b in ((gw, rw), (gb, rb)):
+            assert (a - b).abs().max().item() <= 1e-4 * b.abs().max().item() + 1e-7
+    assert (dmeans - mm.grad).abs().max().item() <= 1e-4 * mm.grad.abs().max().item()
+
+
+def test_shared_mlp_render_rejects_both_models():
+    sc = _scene(64, 1, seed=1)
+    mlp = SharedMLP()
+    with pytest.raises(ValueError, match="either"):
+        raster.forward(sc["means"], torch.zeros(194 * 64, device="cuda"), sc["opac"], sc["scales"], sc["rots"],
+                       90, 360, 1.0, sc["views"], sc["tx"], sc["rxs"], shared=mlp, shared_params=mlp.init_params())
