@@ -108,7 +108,7 @@ int report_cuda(cudaError_t e, const char* where) { return cuda_fail(e, where); 
 
 extern "C" {
 
-int gsparc_abi_version(void) { return 2; }
+int gsparc_abi_version(void) { return 3; }
 
 const char* gsparc_status_string(int status) {
   switch (status) {
@@ -451,14 +451,14 @@ int gsparc_splat_loss(int R, int H, int W, int hidden, float lambda1, float alph
 
 // ---- fused optimizer ---------------------------------------------------------
 
-size_t gsparc_gaussian_state_floats(int P, int conf_floats) {
-  if (P < 0 || conf_floats < 0) return 0;
-  return gaussian_layout((size_t)P, (size_t)conf_floats).total;
+size_t gsparc_gaussian_state_floats(int P, long long mlp_floats, int conf_floats) {
+  if (P < 0 || mlp_floats < 0 || conf_floats < 0) return 0;
+  return gaussian_layout((size_t)P, (size_t)mlp_floats, (size_t)conf_floats).total;
 }
 
-int gsparc_gaussian_state_layout(int P, int conf_floats, size_t* offsets6) {
-  if (P < 0 || conf_floats < 0 || !offsets6) return invalid("gaussian state layout");
-  const GaussianLayout L = gaussian_layout((size_t)P, (size_t)conf_floats);
+int gsparc_gaussian_state_layout(int P, long long mlp_floats, int conf_floats, size_t* offsets6) {
+  if (P < 0 || mlp_floats < 0 || conf_floats < 0 || !offsets6) return invalid("gaussian state layout");
+  const GaussianLayout L = gaussian_layout((size_t)P, (size_t)mlp_floats, (size_t)conf_floats);
   offsets6[0] = L.centre; offsets6[1] = L.scale; offsets6[2] = L.quat; offsets6[3] = L.opacity;
   offsets6[4] = L.mlp; offsets6[5] = L.conf;
   return GSPARC_OK;
@@ -475,13 +475,14 @@ int gsparc_gaussian_activate(int P, const float* params, float* scales, float* r
   return GSPARC_OK;
 }
 
-int gsparc_gaussian_adam_step(int P, int conf_floats, float* params, const float* grads, float* exp_avg,
+int gsparc_gaussian_adam_step(int P, long long mlp_floats, int conf_floats, float* params, const float* grads,
+                              float* exp_avg,
                               float* exp_avg_sq, float* step_count, const float* lr6, float beta1, float beta2,
                               float eps, const float* centre_lo3, const float* centre_hi3, float* scales,
                               float* rotations, float* opacities, void* stream) {
-  if (P < 0 || conf_floats < 0) return invalid("P or conf_floats");
+  if (P < 0 || mlp_floats < 0 || conf_floats < 0) return invalid("P, mlp_floats or conf_floats");
   if (!step_count || !lr6 || !centre_lo3 || !centre_hi3) return invalid("null step, learning-rate or clamp pointer");
-  if ((P > 0 || conf_floats > 0) && (!params || !grads || !exp_avg || !exp_avg_sq))
+  if ((P > 0 || mlp_floats > 0 || conf_floats > 0) && (!params || !grads || !exp_avg || !exp_avg_sq))
     return invalid("null state pointer");
   if ((((uintptr_t)params) | ((uintptr_t)grads) | ((uintptr_t)exp_avg) | ((uintptr_t)exp_avg_sq)) & 15u)
     return invalid("state buffers must be 16-byte aligned");
@@ -490,7 +491,7 @@ int gsparc_gaussian_adam_step(int P, int conf_floats, float* params, const float
   if (!(beta1 >= 0.f && beta1 < 1.f && beta2 >= 0.f && beta2 < 1.f && eps >= 0.f)) return invalid("Adam betas/eps");
   cudaStream_t s = (cudaStream_t)stream;
   Timed t(KID_ADAM, s);
-  GS_CHECK(launch_gaussian_adam(P, conf_floats, params, grads, exp_avg, exp_avg_sq, step_count, lr6, beta1, beta2,
+  GS_CHECK(launch_gaussian_adam(P, mlp_floats, conf_floats, params, grads, exp_avg, exp_avg_sq, step_count, lr6, beta1, beta2,
                                 eps, centre_lo3, centre_hi3, scales, rotations, opacities, s),
            "gaussian adam");
   return GSPARC_OK;

@@ -167,9 +167,10 @@ struct GaussianLayout {
   size_t centre, scale, quat, opacity, mlp, conf, total;
 };
 
-// conf_floats: size of the trailing segment for a global (not per-Gaussian)
-// parameter block such as the confidence MLP; 0 for none.
-__host__ __device__ inline GaussianLayout gaussian_layout(size_t P, size_t conf_floats = 0) {
+// mlp_floats: size of the emission-MLP segment (194 P for the per-Gaussian
+// MLP, the shared MLP's parameter count otherwise); conf_floats: size of the
+// trailing segment for a global parameter block such as the confidence MLP.
+__host__ __device__ inline GaussianLayout gaussian_layout(size_t P, size_t mlp_floats, size_t conf_floats = 0) {
   auto a = [](size_t x) { return (x + 63) / 64 * 64; };
   GaussianLayout L;
   L.centre = 0;
@@ -177,7 +178,7 @@ __host__ __device__ inline GaussianLayout gaussian_layout(size_t P, size_t conf_
   L.quat = L.scale + a(3 * P);
   L.opacity = L.quat + a(4 * P);
   L.mlp = L.opacity + a(P);
-  L.conf = L.mlp + a((size_t)kMlpFloats * P);
+  L.conf = L.mlp + a(mlp_floats);
   L.total = L.conf + a(conf_floats);
   return L;
 }

@@ -57,7 +57,8 @@ cudaError_t launch_emission_backward(int P, int R, const float* means3D, const f
                                      const float* rx_pos, const int* radii, const float* dsig, float* dL_dmlp,
                                      float* dL_dmeans3D, cudaStream_t stream);
 
-cudaError_t launch_gaussian_adam(int P, int conf_floats, float* params, const float* grads, float* m, float* v,
+cudaError_t launch_gaussian_adam(int P, long long mlp_floats, int conf_floats, float* params, const float* grads,
+                                 float* m, float* v,
                                  float* step, const float* lr6, float beta1, float beta2, float eps,
                                  const float* lo3, const float* hi3, float* act_scales, float* act_rots,
                                  float* act_opac, cudaStream_t stream);

@@ -22,7 +22,8 @@
 //
 // Flat layout of parameters, gradients and both moments (floats), each
 // segment starting on a 256-byte boundary (gaussian_layout):
-//   [centre 3P | log_scale 3P | quaternion 4P | opacity_logit P | mlp 194P | conf]
+//   [centre 3P | log_scale 3P | quaternion 4P | opacity_logit P | mlp | conf]
+// (mlp: the per-Gaussian MLPs, 194 P floats, or the shared MLP's parameters)
 // With activation outputs given, the per-Gaussian kernel also writes the
 // activated values of the updated parameters (exp(log_scale),
 // normalize(quaternion), sigmoid(logit)) -- the rasterizer inputs of the next
@@ -223,12 +224,13 @@ train_adam_kernel(int P, GaussianLayout L, int nb_g, size_t n, size_t n_mlp, flo
   }
 }
 
-cudaError_t launch_gaussian_adam(int P, int conf_floats, float* params, const float* grads, float* m, float* v,
+cudaError_t launch_gaussian_adam(int P, long long mlp_floats, int conf_floats, float* params, const float* grads,
+                                 float* m, float* v,
                                  float* step, const float* lr6, float beta1, float beta2, float eps,
                                  const float* lo3, const float* hi3, float* act_scales, float* act_rots,
                                  float* act_opac, cudaStream_t stream) {
-  const GaussianLayout L = gaussian_layout((size_t)P, (size_t)conf_floats);
-  const size_t n_mlp = (size_t)kMlpFloats * P;
+  const GaussianLayout L = gaussian_layout((size_t)P, (size_t)mlp_floats, (size_t)conf_floats);
+  const size_t n_mlp = (size_t)mlp_floats;
   const size_t n = conf_floats > 0 ? (L.conf - L.mlp) + (size_t)conf_floats : n_mlp;
   const int nb_g = (P + 255) / 256;
   int nb_m = (int)((n / 4 + 255) / 256);
@@ -242,7 +244,7 @@ cudaError_t launch_gaussian_adam(int P, int conf_floats, float* params, const fl
 cudaError_t launch_gaussian_activate(int P, const float* params, float* act_scales, float* act_rots,
                                      float* act_opac, cudaStream_t stream) {
   if (P == 0) return cudaSuccess;
-  const GaussianLayout L = gaussian_layout((size_t)P);
+  const GaussianLayout L = gaussian_layout((size_t)P, 0);   // the segments before the MLP's
   gaussian_activate_kernel<<<(P + 255) / 256, 256, 0, stream>>>(P, L, params, act_scales, act_rots, act_opac);
   return cudaGetLastError();
 }

@@ -62,11 +62,11 @@ _SIGS = {
     "gsparc_splat_loss_scratch_floats": (_c_size, [_c_int, _c_int, _c_int, _c_int]),
     "gsparc_splat_loss": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_float, _c_float, _c_float, _c_float,
                                    _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
-    "gsparc_gaussian_state_floats": (_c_size, [_c_int, _c_int]),
-    "gsparc_gaussian_state_layout": (_c_int, [_c_int, _c_int, ctypes.POINTER(_c_size)]),
+    "gsparc_gaussian_state_floats": (_c_size, [_c_int, _c_ll, _c_int]),
+    "gsparc_gaussian_state_layout": (_c_int, [_c_int, _c_ll, _c_int, ctypes.POINTER(_c_size)]),
     "gsparc_gaussian_activate": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _vp]),
-    "gsparc_gaussian_adam_step": (_c_int, [_c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_float, _c_float,
-                                           _c_float, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gsparc_gaussian_adam_step": (_c_int, [_c_int, _c_ll, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_float,
+                                           _c_float, _c_float, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gsparc_timing_enable": (_c_int, [_c_int]),
     "gsparc_timing_kernel_count": (_c_int, []),
     "gsparc_timing_kernel_name": (ctypes.c_char_p, [_c_int]),

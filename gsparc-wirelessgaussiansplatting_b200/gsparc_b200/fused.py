@@ -44,11 +44,11 @@ LR = (0.00016, 0.005, 0.001, 0.0055, 0.002, 0.001)
 CONF_HIDDEN = 32   # optimizer.py:35
 
 
-def state_layout(P, n_conf=0):
+def state_layout(P, n_mlp, n_conf=0):
     L = _lib.lib()
     out = (ctypes.c_size_t * 6)()
-    check("gaussian state layout", L.gsparc_gaussian_state_layout(int(P), int(n_conf), out))
-    return [int(v) for v in out], int(L.gsparc_gaussian_state_floats(int(P), int(n_conf)))
+    check("gaussian state layout", L.gsparc_gaussian_state_layout(int(P), int(n_mlp), int(n_conf), out))
+    return [int(v) for v in out], int(L.gsparc_gaussian_state_floats(int(P), int(n_mlp), int(n_conf)))
 
 
 class FusedTrainer:
@@ -56,7 +56,11 @@ class FusedTrainer:
     confidence_alpha = 0.3
 
     def __init__(self, scene: scenes.Scene, H=scenes.H, W=scenes.W, device="cuda", group=None, seed=0,
-                 grad_mode="reference", lr=LR, betas=(0.9, 0.999), eps=1e-15, conf_hidden=CONF_HIDDEN):
+                 grad_mode="reference", lr=LR, betas=(0.9, 0.999), eps=1e-15, conf_hidden=CONF_HIDDEN,
+                 shared=None):
+        """``shared``: a ``SharedMLP`` to use the benchmark's shared emission
+        MLP (initialised from ``seed``) instead of the scene's per-Gaussian
+        3-32-2 MLPs."""
         self.H, self.W, self.device, self.group = H, W, torch.device(device), group
         self.grad_mode = grad_mode
         self.betas, self.eps = betas, eps
@@ -64,7 +68,9 @@ class FusedTrainer:
         self.n_conf = conf_floats(self.conf_hidden)
         P = scene.P
         self.P = P
-        (oC, oS, oQ, oO, oM, oG), total = state_layout(P, self.n_conf)
+        self.shared = shared
+        self.n_mlp = 194 * P if shared is None else shared.n_params
+        (oC, oS, oQ, oO, oM, oG), total = state_layout(P, self.n_mlp, self.n_conf)
         dev = self.device
         self.params = torch.zeros(total, dtype=torch.float32, device=dev)
         self.grads = torch.zeros(total, dtype=torch.float32, device=dev)
@@ -78,7 +84,7 @@ class FusedTrainer:
         self.log_scale = seg(self.params, oS, 3 * P, (P, 3))
         self.rotation = seg(self.params, oQ, 4 * P, (P, 4))
         self.opacity_logit = seg(self.params, oO, P, (P,))
-        self.mlp = seg(self.params, oM, 194 * P, (194 * P,))
+        self.mlp = seg(self.params, oM, self.n_mlp, (self.n_mlp,))
         self.conf_params = seg(self.params, oG, self.n_conf, (self.n_conf,))
         self.conf_grads = seg(self.grads, oG, self.n_conf, (self.n_conf,))
         t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
@@ -87,7 +93,7 @@ class FusedTrainer:
             self.log_scale.copy_(t(scene.log_scales))
             self.rotation.copy_(t(scene.quats))
             self.opacity_logit.copy_(t(scene.opacity_logits).reshape(-1))
-            self.mlp.copy_(t(scene.mlp))
+            self.mlp.copy_(t(scene.mlp) if shared is None else shared.init_params(seed, dev))
         torch.manual_seed(seed)
         self.confidence = ConfidenceMLP(self.conf_hidden).to(dev)
         off = 0
@@ -100,7 +106,7 @@ class FusedTrainer:
                 off += n
         self.gout = dict(dmeans3D=seg(self.grads, oC, 3 * P, (P, 3)), dscales=seg(self.grads, oS, 3 * P, (P, 3)),
                          drotations=seg(self.grads, oQ, 4 * P, (P, 4)), dopacity=seg(self.grads, oO, P, (P,)),
-                         dmlp=seg(self.grads, oM, 194 * P, (194 * P,)))
+                         dmlp=seg(self.grads, oM, self.n_mlp, (self.n_mlp,)))
         self.act_scales = torch.empty((P, 3), dtype=torch.float32, device=dev)
         self.act_rots = torch.empty((P, 4), dtype=torch.float32, device=dev)
         self.act_opac = torch.empty((P,), dtype=torch.float32, device=dev)
@@ -138,22 +144,35 @@ class FusedTrainer:
         plan = self.plan
         self._buffers(plan.R)
         out_r, _, _, st = raster.forward(
-            self.centre, self.mlp, self.act_opac, self.act_scales, self.act_rots, self.H, self.W, 1.0, views, tx,
+            self.centre, self._mlp_arg(), self.act_opac, self.act_scales, self.act_rots, self.H, self.W, 1.0, views, tx,
             rxs, tile=plan.tile, capacity=plan.capacity, binning=plan.binning, geom=plan.geom, image=plan.image,
-            out_real=self._out_r, out_imag=self._out_i, radii=self._radii)
+            out_real=self._out_r, out_imag=self._out_i, radii=self._radii, **self._shared_kw())
         plan.record_status()
         loss, dpred = self._lossfn(out_r, targets, rxs, self.conf_params, self.conf_grads)
-        raster.backward(st, self.centre, self.mlp, self.act_scales, self.act_rots, 1.0, views, tx, rxs, dpred,
-                        self._zero_imag, grad_mode=self.grad_mode, out=dict(self._scratch, **self.gout))
+        raster.backward(st, self.centre, self._mlp_arg(), self.act_scales, self.act_rots, 1.0, views, tx, rxs,
+                        dpred, self._zero_imag, grad_mode=self.grad_mode, out=self._bwd_out(),
+                        **self._shared_kw())
         if self.group is not None:
             import torch.distributed as dist
             dist.all_reduce(self.grads, op=dist.ReduceOp.SUM, group=self.group)
         b1, b2 = self.betas
         check("gaussian_adam_step", _lib.lib().gsparc_gaussian_adam_step(
-            self.P, self.n_conf, ptr(self.params), ptr(self.grads), ptr(self.exp_avg), ptr(self.exp_avg_sq),
+            self.P, self.n_mlp, self.n_conf, ptr(self.params), ptr(self.grads), ptr(self.exp_avg), ptr(self.exp_avg_sq),
             ptr(self.step_count), ptr(self.lr6), b1, b2, self.eps, ptr(self.lo3), ptr(self.hi3),
             ptr(self.act_scales), ptr(self.act_rots), ptr(self.act_opac), stream_of(self.device)))
         return loss
+
+    def _mlp_arg(self):
+        return self.mlp if self.shared is None else None
+
+    def _shared_kw(self):
+        return {} if self.shared is None else dict(shared=self.shared, shared_params=self.mlp)
+
+    def _bwd_out(self):
+        out = dict(self._scratch, **self.gout)
+        if self.shared is not None:
+            out["dshared"] = out.pop("dmlp")
+        return out
 
     def terms(self):
         """Per-receiver (l1, ssim, conf, loss_r) of the last step, [R,4] on the device."""
@@ -165,8 +184,9 @@ class FusedTrainer:
         kmax = 0
         with torch.no_grad():
             for r in range(views.shape[0]):
-                _, _, _, st = raster.forward(self.centre, self.mlp, self.act_opac, self.act_scales, self.act_rots,
-                                             self.H, self.W, 1.0, views[r], tx, rxs[r])
+                _, _, _, st = raster.forward(self.centre, self._mlp_arg(), self.act_opac, self.act_scales,
+                                             self.act_rots, self.H, self.W, 1.0, views[r], tx, rxs[r],
+                                             **self._shared_kw())
                 kmax = max(kmax, st.num_rendered)
         return int(kmax * margin) + slack
 
@@ -221,6 +241,9 @@ class FusedTrainer:
 
     def raw_parameters(self):
         P = self.P
+        if self.shared is not None:
+            return dict(centre=self.centre, log_scale=self.log_scale, rotation=self.rotation,
+                        opacity_logit=self.opacity_logit.view(P, 1), shared_mlp=self.mlp)
         return dict(centre=self.centre, log_scale=self.log_scale, rotation=self.rotation,
                     opacity_logit=self.opacity_logit.view(P, 1), fc1_w=self.mlp[:96 * P].view(P, 32, 3),
                     fc1_b=self.mlp[96 * P:128 * P].view(P, 32), fc2_w=self.mlp[128 * P:192 * P].view(P, 2, 32),

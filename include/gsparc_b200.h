@@ -248,15 +248,16 @@ GSPARC_API int gsparc_splat_loss(int R, int H, int W, int hidden, float lambda1,
 
 /* ---- fused optimizer over the per-Gaussian parameters ------------------- */
 
-/* Floats in a flat training-state buffer for P Gaussians plus a global block
- * of conf_floats floats (the confidence MLP; 0 for none), and the float
- * offsets of its six segments: centre [P,3], log-scale [P,3], quaternion
- * [P,4], opacity logit [P], emission MLP [194*P] in the layout of
- * EmissionMLPs.get_all_params, global block [conf_floats].  Each segment
- * starts on a 256-byte boundary; the padding between segments must stay
- * zero in the gradient buffer. */
-GSPARC_API size_t gsparc_gaussian_state_floats(int P, int conf_floats);
-GSPARC_API int gsparc_gaussian_state_layout(int P, int conf_floats, size_t* offsets6);
+/* Floats in a flat training-state buffer for P Gaussians, an emission-MLP
+ * segment of mlp_floats floats (194*P: the per-Gaussian MLPs in the layout
+ * of EmissionMLPs.get_all_params; or the shared MLP's parameter count) and a
+ * global block of conf_floats floats (the confidence MLP; 0 for none), and
+ * the float offsets of its six segments: centre [P,3], log-scale [P,3],
+ * quaternion [P,4], opacity logit [P], emission MLP, global block.  Each
+ * segment starts on a 256-byte boundary; the padding between segments must
+ * stay zero in the gradient buffer. */
+GSPARC_API size_t gsparc_gaussian_state_floats(int P, long long mlp_floats, int conf_floats);
+GSPARC_API int gsparc_gaussian_state_layout(int P, long long mlp_floats, int conf_floats, size_t* offsets6);
 
 /* Activated per-Gaussian values of a flat state buffer (gaussian.py:33-38):
  * scales [P,3] = exp(log-scale), rotations [P,4] = normalize(quaternion),
@@ -280,7 +281,8 @@ GSPARC_API int gsparc_gaussian_activate(int P, const float* params, float* scale
  * rotations, opacities: optional (all or none) outputs of the activated
  * updated parameters, as gsparc_gaussian_activate writes them.  State buffers
  * 16-byte aligned. */
-GSPARC_API int gsparc_gaussian_adam_step(int P, int conf_floats, float* params, const float* grads,
+GSPARC_API int gsparc_gaussian_adam_step(int P, long long mlp_floats, int conf_floats, float* params,
+                                         const float* grads,
                                          float* exp_avg, float* exp_avg_sq, float* step_count,
                                          const float* lr6, float beta1, float beta2, float eps,
                                          const float* centre_lo3, const float* centre_hi3,

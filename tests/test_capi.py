@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     L = _lib.lib()
-    assert L.gsparc_abi_version() == 2
+    assert L.gsparc_abi_version() == 3
     for code, text in [(0, b"ok"), (1, b"invalid argument"), (2, b"CUDA error"), (3, b"binning capacity exceeded")]:
         assert L.gsparc_status_string(code) == text
 
@@ -112,17 +112,17 @@ def test_grad_mode_and_tile_switches():
 
 def test_training_state_layout_with_global_block():
     L = _lib.lib()
-    for P, nc in [(0, 0), (1, 161), (20000, 161), (3, 0)]:
+    for P, nm, nc in [(0, 0, 0), (1, 194, 161), (20000, 194 * 20000, 161), (3, 0, 0), (20000, 6337, 161)]:
         out = (ctypes.c_size_t * 6)()
-        assert L.gsparc_gaussian_state_layout(P, nc, out) == 0
+        assert L.gsparc_gaussian_state_layout(P, nm, nc, out) == 0
         off = list(out)
-        total = L.gsparc_gaussian_state_floats(P, nc)
-        sizes = [3 * P, 3 * P, 4 * P, P, 194 * P, nc]
+        total = L.gsparc_gaussian_state_floats(P, nm, nc)
+        sizes = [3 * P, 3 * P, 4 * P, P, nm, nc]
         assert off[0] == 0 and all(o % 64 == 0 for o in off)          # 256-byte aligned segments
         for i in range(5):
             assert off[i] + sizes[i] <= off[i + 1]
         assert off[5] + nc <= total and total % 64 == 0
-    assert L.gsparc_gaussian_state_layout(-1, 0, (ctypes.c_size_t * 6)()) == 1
+    assert L.gsparc_gaussian_state_layout(-1, 0, 0, (ctypes.c_size_t * 6)()) == 1
 
 
 def test_splat_loss_rejects_bad_arguments_without_cuda():
@@ -144,6 +144,6 @@ def test_splat_loss_rejects_bad_arguments_without_cuda():
 def test_adam_step_rejects_partial_activation_outputs():
     L = _lib.lib()
     d = ctypes.c_void_p(256)
-    st = L.gsparc_gaussian_adam_step(10, 161, d, d, d, d, d, d, 0.9, 0.999, 1e-15, d, d, d, None, None, None)
+    st = L.gsparc_gaussian_adam_step(10, 1940, 161, d, d, d, d, d, d, 0.9, 0.999, 1e-15, d, d, d, None, None, None)
     assert st == 1
     assert b"all three" in L.gsparc_last_error_detail()
