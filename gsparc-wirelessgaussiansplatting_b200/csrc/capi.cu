@@ -326,7 +326,9 @@ int check_mlp_spec(int layers, int width, int act, int out, int precision) {
   if (width < 8 || width > 256) return invalid("width must be in [8, 256]");
   if (act != GSPARC_ACT_RELU && act != GSPARC_ACT_GELU) return invalid("act must be GSPARC_ACT_RELU or _GELU");
   if (out != 1) return invalid("out must be 1 (one amplitude per pair)");
-  if (precision != GSPARC_MLP_FP32) return invalid("precision must be GSPARC_MLP_FP32");
+  if (precision != GSPARC_MLP_FP32 && precision != GSPARC_MLP_BF16) return invalid("precision");
+  if (precision == GSPARC_MLP_BF16 && (width != 128 || layers > 3))
+    return invalid("the BF16 tensor-core path needs width 128 and at most 3 hidden layers");
   return GSPARC_OK;
 }
 }  // namespace
@@ -336,14 +338,15 @@ size_t gsparc_shared_mlp_param_floats(int layers, int width, int out) {
   return shared_mlp_layout(layers, width, out, 0).params;
 }
 
-size_t gsparc_shared_mlp_workspace_floats(int P, int R, int layers, int width, int out) {
+size_t gsparc_shared_mlp_workspace_floats(int P, int R, int layers, int width, int out, int precision) {
   if (P < 0 || R < 0 || layers < 1 || layers > kMaxMlpLayers || width < 1 || out < 1) return 0;
+  if (precision == GSPARC_MLP_BF16) return shared_mlp_layout_bf16(layers, (size_t)P * R).work;
   return shared_mlp_layout(layers, width, out, (size_t)P * R).work;
 }
 
 int gsparc_shared_mlp_forward(int P, int R, int layers, int width, int act, int out, int precision,
                               const float* means3D, const float* rx_pos, const float* params, void* geom_state,
-                              float* workspace, void* stream) {
+                              void* image_state, float* workspace, void* stream) {
   if (P < 0 || R < 1) return invalid("sizes");
   int st = check_mlp_spec(layers, width, act, out, precision);
   if (st != GSPARC_OK) return st;
@@ -353,15 +356,21 @@ int gsparc_shared_mlp_forward(int P, int R, int layers, int width, int act, int 
   GeomView geo;
   carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
   Timed t(KID_SHARED_MLP, s);
-  GS_CHECK(launch_shared_mlp_forward(P, R, layers, width, act, out, means3D, rx_pos, params, geo, workspace, s),
-           "shared mlp forward");
+  if (precision == GSPARC_MLP_BF16) {
+    GS_CHECK(launch_shared_mlp_bf16(true, P, R, layers, act, means3D, rx_pos, params, geo, workspace, nullptr,
+                                    nullptr, nullptr, (ImageHeader*)image_state, s),
+             "shared mlp forward (bf16)");
+  } else {
+    GS_CHECK(launch_shared_mlp_forward(P, R, layers, width, act, out, means3D, rx_pos, params, geo, workspace, s),
+             "shared mlp forward");
+  }
   return GSPARC_OK;
 }
 
 int gsparc_shared_mlp_backward(int P, int R, int layers, int width, int act, int out, int precision,
                                const float* means3D, const float* rx_pos, const float* params,
-                               const void* geom_state, float* workspace, const float* dL_dsignal,
-                               float* dL_dparams, float* dL_dmeans3D, void* stream) {
+                               const void* geom_state, void* image_state, float* workspace,
+                               const float* dL_dsignal, float* dL_dparams, float* dL_dmeans3D, void* stream) {
   if (P < 0 || R < 1) return invalid("sizes");
   int st = check_mlp_spec(layers, width, act, out, precision);
   if (st != GSPARC_OK) return st;
@@ -377,9 +386,15 @@ int gsparc_shared_mlp_backward(int P, int R, int layers, int width, int act, int
   GeomView geo;
   carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
   Timed t(KID_SHARED_MLP_BWD, s);
-  GS_CHECK(launch_shared_mlp_backward(P, R, layers, width, act, out, means3D, rx_pos, params, geo, workspace,
-                                      dL_dsignal, dL_dparams, dL_dmeans3D, s),
-           "shared mlp backward");
+  if (precision == GSPARC_MLP_BF16) {
+    GS_CHECK(launch_shared_mlp_bf16(false, P, R, layers, act, means3D, rx_pos, params, geo, workspace, dL_dsignal,
+                                    dL_dparams, dL_dmeans3D, (ImageHeader*)image_state, s),
+             "shared mlp backward (bf16)");
+  } else {
+    GS_CHECK(launch_shared_mlp_backward(P, R, layers, width, act, out, means3D, rx_pos, params, geo, workspace,
+                                        dL_dsignal, dL_dparams, dL_dmeans3D, s),
+             "shared mlp backward");
+  }
   return GSPARC_OK;
 }
 

@@ -35,6 +35,7 @@ constexpr uint32_t kErrCapacity = 1u << 0;   // K exceeded the binning capacity
 constexpr uint32_t kErrSegment = 1u << 1;    // a tile segment exceeded the sort limit
 constexpr uint32_t kErrBadIndex = 1u << 2;   // a point list held an id >= P (arena mismatch)
 constexpr uint32_t kErrSortWait = 1u << 3;   // a depth-sort look-back wait gave up (bounded spin)
+constexpr uint32_t kErrMlpWait = 1u << 4;    // a tensor-core MLP wait on its MMAs gave up (bounded)
 
 struct ImageHeader {
   unsigned long long num_rendered;   // K, written by the preprocess's last CTA (segment scan)

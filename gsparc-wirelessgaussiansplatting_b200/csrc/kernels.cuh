@@ -90,6 +90,17 @@ struct SharedMlpLayout {
 };
 SharedMlpLayout shared_mlp_layout(int layers, int width, int out, size_t rows);
 
+// BF16 / tcgen05 path (shared_mlp_tc.cu): width 128, one output, 1-3 layers;
+// workspace: BF16 pre-activations [layers][rows][128] at z[1], signal at s,
+// feature gradient [rows][32] at d0.
+SharedMlpLayout shared_mlp_layout_bf16(int layers, size_t rows);
+cudaError_t launch_shared_mlp_bf16(bool fwd, int P, int R, int layers, int act, const float* means3D,
+                                   const float* rx_pos, const float* params, const GeomView& geo, float* work,
+                                   const float* dL_dsignal, float* dparams, float* dL_dmeans3D, ImageHeader* hdr,
+                                   cudaStream_t s);
+cudaError_t launch_mlp_features_backward(int P, int R, const float* means3D, const float* rx_pos, const int* radii,
+                                         const float* dX, float* dL_dmeans3D, cudaStream_t s);
+
 cudaError_t launch_shared_mlp_forward(int P, int R, int layers, int width, int act, int out, const float* means3D,
                                       const float* rx_pos, const float* params, const GeomView& geo, float* work,
                                       cudaStream_t s);

@@ -245,27 +245,48 @@ SharedMlpLayout shared_mlp_layout(int layers, int width, int out, size_t rows) {
     p += o;
   }
   L.params = p;
+  auto al = [](size_t x) { return (x + 63) / 64 * 64; };   // 256-byte aligned segments
   size_t w = 0;
   L.x0 = w;
-  w += rows * kFeat;
+  w += al(rows * kFeat);
   for (int l = 1; l <= layers; ++l) {
     L.z[l] = w;
-    w += rows * width;
+    w += al(rows * width);
     L.a[l] = w;
-    w += rows * width;
+    w += al(rows * width);
   }
   L.o = w;
-  w += rows * out;
+  w += al(rows * out);
   L.s = w;
-  w += rows;
+  w += al(rows);
   size_t dw = width > kFeat ? width : kFeat;
   if ((size_t)out > dw) dw = out;
   L.d0 = w;
-  w += rows * dw;
+  w += al(rows * dw);
   L.d1 = w;
-  w += rows * dw;
+  w += al(rows * dw);
   L.work = w;
   return L;
+}
+
+SharedMlpLayout shared_mlp_layout_bf16(int layers, size_t rows) {
+  SharedMlpLayout L = shared_mlp_layout(layers, 128, 1, 0);   // parameter offsets as the FP32 path
+  auto a = [](size_t x) { return (x + 63) / 64 * 64; };         // 256-byte aligned segments (vector access)
+  size_t w = 0;
+  L.z[1] = w;
+  w += a((size_t)layers * rows * 128 / 2);   // BF16 pre-activations, two per float
+  L.s = w;
+  w += a(rows);
+  L.d0 = w;
+  w += a(rows * kFeat);
+  L.work = w;
+  return L;
+}
+
+cudaError_t launch_mlp_features_backward(int P, int R, const float* means3D, const float* rx_pos, const int* radii,
+                                         const float* dX, float* dL_dmeans3D, cudaStream_t s) {
+  mlp_features_backward_kernel<<<(P + 255) / 256, 256, 0, s>>>(P, R, means3D, rx_pos, radii, dX, dL_dmeans3D);
+  return cudaGetLastError();
 }
 
 static cudaError_t gemm_fwd(size_t M, int N, int K, const float* A, const float* W, const float* bias, float* Z,

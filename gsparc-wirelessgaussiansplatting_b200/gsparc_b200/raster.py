@@ -151,7 +151,7 @@ def forward(means3D, emission_mlps, opacities, scales, rotations, H, W, scale_mo
         ptr(v), ptr(tx), ptr(rx), ptr(radii), ptr(geom), ptr(image),
         ctypes.byref(K) if capacity is None else None, stream))
     if shared is not None:
-        shared.forward(P, R, m, rx, shared_params, geom)
+        shared.forward(P, R, m, rx, shared_params, geom, image)
     if capacity is None:
         capacity = int(K.value)
         num_rendered = capacity
@@ -216,7 +216,7 @@ def backward(st: ForwardState, means3D, emission_mlps, scales, rotations, scale_
         ptr(out["dmlp"]) if shared is None else None, stream_of(device)))
     if shared is not None:
         sp = _dev_f32(shared_params, "shared_params", device).reshape(-1)
-        shared.backward(P, R, m, rx, sp, st.geom, out["dsignal"], out["dshared"], out["dmeans3D"])
+        shared.backward(P, R, m, rx, sp, st.geom, out["dsignal"], out["dshared"], out["dmeans3D"], st.image)
     return out
 
 

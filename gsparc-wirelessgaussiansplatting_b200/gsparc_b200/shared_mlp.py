@@ -23,7 +23,7 @@ from ._lib import check, ptr, stream_of
 
 FEATURES = 32
 ACTS = {"relu": 1, "gelu": 2}
-PRECISIONS = {"fp32": 0}
+PRECISIONS = {"fp32": 0, "bf16": 1}
 
 
 class SharedMLP:
@@ -74,7 +74,8 @@ class SharedMLP:
     def workspace(self, P, R, device):
         key = (int(P), int(R), str(device))
         if self._work_key != key:
-            n = int(_lib.lib().gsparc_shared_mlp_workspace_floats(int(P), int(R), self.layers, self.width, self.out))
+            n = int(_lib.lib().gsparc_shared_mlp_workspace_floats(int(P), int(R), self.layers, self.width, self.out,
+                                                                  PRECISIONS[self.precision]))
             self._work = torch.empty(max(n, 1), dtype=torch.float32, device=device)
             self._work_key = key
         return self._work
@@ -82,18 +83,20 @@ class SharedMLP:
     def _spec(self):
         return (self.layers, self.width, ACTS[self.act], self.out, PRECISIONS[self.precision])
 
-    def forward(self, P, R, means3D, rx_pos, params, geom):
-        """Write the signal of every visible pair into a prepared forward's geometry arena."""
+    def forward(self, P, R, means3D, rx_pos, params, geom, image=None):
+        """Write the signal of every visible pair into a prepared forward's
+        geometry arena (``image``: its image arena, for the error word)."""
         dev = means3D.device
         work = self.workspace(P, R, dev)
         check("shared_mlp_forward", _lib.lib().gsparc_shared_mlp_forward(
-            int(P), int(R), *self._spec(), ptr(means3D), ptr(rx_pos), ptr(params), ptr(geom), ptr(work),
-            stream_of(dev)))
+            int(P), int(R), *self._spec(), ptr(means3D), ptr(rx_pos), ptr(params), ptr(geom),
+            ptr(image) if image is not None else None, ptr(work), stream_of(dev)))
 
-    def backward(self, P, R, means3D, rx_pos, params, geom, dsignal, dparams, dmeans3D):
+    def backward(self, P, R, means3D, rx_pos, params, geom, dsignal, dparams, dmeans3D, image=None):
         """dparams is overwritten; dL/dmeans3D through the features is added to dmeans3D."""
         dev = means3D.device
         work = self.workspace(P, R, dev)
         check("shared_mlp_backward", _lib.lib().gsparc_shared_mlp_backward(
-            int(P), int(R), *self._spec(), ptr(means3D), ptr(rx_pos), ptr(params), ptr(geom), ptr(work),
-            ptr(dsignal), ptr(dparams), ptr(dmeans3D), stream_of(dev)))
+            int(P), int(R), *self._spec(), ptr(means3D), ptr(rx_pos), ptr(params), ptr(geom),
+            ptr(image) if image is not None else None, ptr(work), ptr(dsignal), ptr(dparams), ptr(dmeans3D),
+            stream_of(dev)))

@@ -197,24 +197,31 @@ GSPARC_API int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float
  * gsparc_rasterize_backward with gsparc_shared_mlp_backward.
  * params: flat fp32, per layer W [out, in] row-major then b [out].
  * workspace: gsparc_shared_mlp_workspace_floats floats; the forward keeps
- * the activations there for the backward.  out must be 1. */
+ * what the backward needs there.  out must be 1.
+ * precision GSPARC_MLP_FP32: SIMT FP32 layers (any width 8..256, 1-6
+ * layers).  GSPARC_MLP_BF16: BF16 operands on the tcgen05 tensor cores with
+ * FP32 accumulation (width 128, 1-3 layers); the forward and the backward
+ * are one fused kernel each.  image_state (optional) receives the error bit
+ * of a bounded tensor-core wait that gave up. */
 #define GSPARC_ACT_RELU 1
 #define GSPARC_ACT_GELU 2
 #define GSPARC_MLP_FP32 0
+#define GSPARC_MLP_BF16 1
 GSPARC_API size_t gsparc_shared_mlp_param_floats(int layers, int width, int out);
-GSPARC_API size_t gsparc_shared_mlp_workspace_floats(int P, int R, int layers, int width, int out);
+GSPARC_API size_t gsparc_shared_mlp_workspace_floats(int P, int R, int layers, int width, int out,
+                                                     int precision);
 /* Writes the signal of every visible pair into the geometry arena of a
  * prepared forward. */
 GSPARC_API int gsparc_shared_mlp_forward(int P, int R, int layers, int width, int act, int out,
                                          int precision, const float* means3D, const float* rx_pos,
-                                         const float* params, void* geom_state, float* workspace,
-                                         void* stream);
+                                         const float* params, void* geom_state, void* image_state,
+                                         float* workspace, void* stream);
 /* dL_dsignal [R,P,2] as gsparc_rasterize_backward returns it; dL_dparams is
  * overwritten; dL/dmeans3D through the features is ADDED to dL_dmeans3D. */
 GSPARC_API int gsparc_shared_mlp_backward(int P, int R, int layers, int width, int act, int out,
                                           int precision, const float* means3D, const float* rx_pos,
-                                          const float* params, const void* geom_state, float* workspace,
-                                          const float* dL_dsignal, float* dL_dparams,
+                                          const float* params, const void* geom_state, void* image_state,
+                                          float* workspace, const float* dL_dsignal, float* dL_dparams,
                                           float* dL_dmeans3D, void* stream);
 
 /* ---- training loss ------------------------------------------------------ */

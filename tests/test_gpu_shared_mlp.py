@@ -93,3 +93,88 @@ def test_shared_mlp_render_rejects_both_models():
     with pytest.raises(ValueError, match="either"):
         raster.forward(sc["means"], torch.zeros(194 * 64, device="cuda"), sc["opac"], sc["scales"], sc["rots"],
                        90, 360, 1.0, sc["views"], sc["tx"], sc["rxs"], shared=mlp, shared_params=mlp.init_params())
+
+
+def _bf(x):
+    return x.bfloat16().float()
+
+
+def torch_bf16_emulation(mlp, params, means, rxs, radii, dsig):
+    """The BF16 tensor-core path's arithmetic restated in torch: operands
+    rounded to BF16 where the kernels round them, FP32 accumulation.
+    Returns (signal, dparams, dmeans)."""
+    act = (lambda z: F.relu(z)) if mlp.act == "relu" else (lambda z: F.gelu(z))
+    layers = mlp.unflatten(params)
+    L = len(layers) - 1
+    p = params.detach().clone().requires_grad_(True)
+    m = means.detach().clone().requires_grad_(True)
+    lay = mlp.unflatten(p)
+    x = torch_features(m, rxs, radii)
+    h = _bf(x)
+    zs = []
+    for l in range(L):
+        w, b = lay[l]
+        z = _bf(h @ _bf(w).T + b)
+        zs.append(z)
+        h = _bf(act(z)) if l + 1 < L else act(z)
+    wo, bo = lay[L]
+    s = torch.sigmoid(h @ wo.T + bo)[..., 0]
+    # adjoint with the kernels' roundings
+    with torch.no_grad():
+        dO = dsig[..., 0] * s * (1 - s)
+        grads = [None] * (2 * L + 2)
+        aL = act(zs[-1])
+        grads[2 * L] = (dO[..., None] * aL).sum((0, 1))[None]
+        grads[2 * L + 1] = dO.sum()[None]
+        dz = _bf(dO[..., None] * wo[0] * torch.func.grad(lambda q: act(q).sum())(zs[-1]))
+        for l in range(L - 1, -1, -1):
+            w, _ = lay[l]
+            a_in = _bf(x) if l == 0 else _bf(act(zs[l - 1]))
+            grads[2 * l] = torch.einsum("rpo,rpi->oi", dz, a_in)
+            grads[2 * l + 1] = dz.sum((0, 1))
+            dA = dz @ _bf(w)
+            if l == 0:
+                dX0 = dA
+            else:
+                dz = _bf(dA * torch.func.grad(lambda q: act(q).sum())(zs[l - 1]))
+        dparams = torch.cat([g.reshape(-1) for g in grads])
+    # centres: through the features only
+    mm = means.detach().clone().requires_grad_(True)
+    (torch_features(mm, rxs, radii) * dX0).sum().backward()
+    return s.detach(), dparams, mm.grad
+
+
+@pytest.mark.parametrize("layers,act,R", [(3, "gelu", 2), (2, "relu", 1), (1, "gelu", 3)])
+def test_shared_mlp_bf16_tensor_cores_match_bf16_emulation(layers, act, R):
+    """BF16 operands on tcgen05 with FP32 accumulation, against the same
+    roundings restated in torch: signals within 1e-4 absolute, gradients within
+    2e-3 of each tensor's largest magnitude (FP32 accumulation order and the
+    kernels' atomics differ); against the FP32 network: signals within 1e-2."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    P = 2999
+    sc = _scene(P, R, seed=7)
+    mlp = SharedMLP(layers, 128, act, precision="bf16")
+    params = mlp.init_params(seed=11 + layers)
+    out_r, _, radii, st = raster.forward(sc["means"], None, sc["opac"], sc["scales"], sc["rots"], 90, 360, 1.0,
+                                         sc["views"], sc["tx"], sc["rxs"], shared=mlp, shared_params=params)
+    K, err = raster.read_status(st)
+    assert err == 0 and K > 0
+    sig = raster.state_views(st)["signal"]
+    vis = radii > 0
+    gen = torch.Generator().manual_seed(8)
+    dsig = (torch.randn((R, P, 2), generator=gen).cuda() * vis[..., None]).contiguous()
+    ref_s, ref_dp, ref_dm = torch_bf16_emulation(mlp, params, sc["means"], sc["rxs"], radii, dsig)
+    # a pre-activation within FP32 rounding of a BF16 rounding boundary may round
+    # the other way (accumulation order), which moves a signal by ~1e-5
+    assert (sig[..., 0][vis] - ref_s[vis]).abs().max().item() <= 1e-4
+    fp32 = torch_signal(SharedMLP(layers, 128, act), params, sc["means"], sc["rxs"], radii)
+    assert (sig[..., 0][vis] - fp32[vis]).abs().max().item() <= 1e-2
+    dparams = torch.empty_like(params)
+    dmeans = torch.zeros_like(sc["means"])
+    mlp.backward(P, R, sc["means"], sc["rxs"], params, st.geom, dsig, dparams, dmeans, st.image)
+    K, err = raster.read_status(st)
+    assert err == 0
+    for (gw, gb), (rw, rb) in zip(mlp.unflatten(dparams), mlp.unflatten(ref_dp)):
+        for a, b in ((gw, rw), (gb, rb)):
+            assert (a - b).abs().max().item() <= 2e-3 * b.abs().max().item() + 1e-6
+    assert (dmeans - ref_dm).abs().max().item() <= 2e-3 * ref_dm.abs().max().item()
