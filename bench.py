@@ -9,18 +9,24 @@ loss, the full hand-written adjoint, Adam.  Each step uses the next receiver
 of a pool; targets are spectra of a second seeded scene at those receivers.
 Synthetic data (no dataset in the container).
 
-value: steps/s of the step captured in one CUDA graph (FusedTrainer: flat
-training state, fused L1+SSIM+confidence loss, fused activation-adjoint Adam;
-16 kernel launches per step, all of them this library's) with inputs
-resident in HBM; per-step CUDA events on the compute stream, L2 flushed
-(256 MiB write) between steps outside the events.
-e2e: the same step through FusedTrainer.step with the receiver's
-target spectrum, view matrix and position copied from pinned host memory
-every step and the loss and rasterizer status read back to the host, inside
-the timed region.  Also reported: the eager drop-in path (reference call
-surface), a 16-receiver batched step, and per-kernel device times of the
-same kernels (from eager runs of the same step; graph replays bypass the
-library's event hooks).
+value: steps/s of configs[1] (20,000 Gaussians, shared emission MLP 2x64 ReLU,
+FP32, one receiver per step) captured in one CUDA graph (FusedTrainer: flat
+training state, fused L1+SSIM+confidence loss, fused activation-adjoint
+Adam; every launch one of this library's kernels) with inputs resident in
+HBM; per-step CUDA events on the compute stream, L2 flushed (256 MiB write)
+between steps outside the events.
+e2e: the same step through FusedTrainer.step with the receiver's target
+spectrum, view matrix and position copied from pinned host memory every
+step and the loss and rasterizer status read back to the host, inside the
+timed region.
+cfg3_batched_bf16_vs_plain_fp32: configs[3]'s model (200,000 Gaussians,
+shared MLP 3x128 GELU): the training step with 32 receivers per step and the
+MLP in BF16 on the tcgen05 tensor cores, against the plain per-receiver FP32
+step, in spectra/s, with the SSIM difference of their renders.
+Also reported: the same step with the reference's per-Gaussian emission MLPs,
+the eager drop-in path (reference call surface), a 16-receiver batched step
+and per-kernel device times (eager runs of the same step; graph replays
+bypass the library's event hooks).
 N > 1: one process per GPU (torchrun), receivers sharded, Gaussians
 replicated, gradients all-reduced over NCCL every step (weak scaling).
 --impl reference: the CPU restatement of the same step (oracle/) on the
@@ -46,9 +52,12 @@ METRIC = "train steps/s & spectra/s on 1 B200: batched BF16 vs plain FP32, ΔSSI
 UNIT = "train steps/s"
 P_GAUSS = 20000
 POOL = 16
-WORKLOAD = ("cfg1_train_20k: per-receiver training step (forward+SSIM/L1/confidence loss+adjoint+Adam), "
-            "P=20000 Gaussians uniform in a 10x3x8 m room, 90x360 spectrum, 16x16 tiles, per-Gaussian 3-32-2 "
-            "emission MLP, FP32")
+SHARED_CFG1 = dict(layers=2, width=64, act="relu")    # emission MLP of configs 0-1
+SHARED_CFG3 = dict(layers=3, width=128, act="gelu")   # emission MLP of config 3
+P_CFG3, R_CFG3 = 200000, 32
+WORKLOAD = ("cfg1_train_20k: per-receiver training step (forward + L1/SSIM/confidence loss + hand-written adjoint "
+            "+ Adam), P=20000 Gaussians uniform in a 10x8x3 m room, one 90x360 spectrum per step, 16x16 tiles, "
+            "shared emission MLP 2x64 ReLU from [position PE, rx-relative direction, 1/d^2] to 1 amplitude, FP32")
 
 
 def _peaks():
@@ -138,6 +147,12 @@ def _dist_setup():
     return world, rank, local, group
 
 
+def _oracle_shared(spec):
+    """(layers, width, act, flat params) of the shared MLP as FusedTrainer initialises it (seed 0)."""
+    from gsparc_b200.shared_mlp import init_params_host
+    return (spec["layers"], spec["width"], spec["act"], init_params_host(spec["layers"], spec["width"], 1, seed=0))
+
+
 def run_reference(args):
     """CPU restatement of the step (oracle/train_step.py), timed on the host."""
     rank = int(os.environ.get("RANK", "0"))
@@ -154,7 +169,7 @@ def run_reference(args):
     n_tgt = min(POOL, args.warmup + args.steps)
     targets = [oraster.render(tm, ts, tq, to, tg.mlp, scenes.view_matrix(rxs[i]), scenes.TX_POS, rxs[i], 90,
                               360)["out"][0] for i in range(n_tgt)]
-    tr = OracleTrainer(sc)
+    tr = OracleTrainer(sc, shared=_oracle_shared(SHARED_CFG1))
     # bounded sample: at most ~150 s of timed CPU work
     for i in range(min(args.warmup, 1)):
         tr.step(scenes.view_matrix(rxs[i % n_tgt]), rxs[i % n_tgt], scenes.TX_POS, targets[i % n_tgt])
@@ -173,12 +188,31 @@ def run_reference(args):
             "steps": len(times), "warmup": min(args.warmup, 1), "ms_per_step": 1000.0 / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "gaussians": P_GAUSS, "receivers_per_step": 1, "spectrum": "90x360",
-                       "implementation": "CPU restatement of the reference path (oracle/train_step.py, numpy)"},
+                       "implementation": "CPU restatement of the same step (oracle/train_step.py with "
+                                         "oracle/shared_mlp.py, numpy)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": ncores, "kind": "port",
                              "sample": f"{len(times)} of {args.steps} requested steps (capped at {budget:.0f} s)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def _scene_data(P, n_rx, dev, cluster_frac=0.0):
+    """Seeded scene, receivers, views and target spectra (a second seeded scene) on the device."""
+    import numpy as np
+    import torch
+    from gsparc_b200 import raster, scenes
+    sc = scenes.make_scene(P, scenes.SEED_SCENE, cluster_frac=cluster_frac)
+    tg = scenes.make_scene(P, scenes.SEED_TARGET, cluster_frac=cluster_frac)
+    rxs = scenes.make_receivers(n_rx)
+    views = scenes.view_matrices(rxs)
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
+    tm, ts, tq, to = tg.activated()
+    with torch.no_grad():
+        targets, _, _, _ = raster.forward(t(tm), t(tg.mlp), t(to.reshape(-1)), t(ts), t(tq), 90, 360, 1.0, t(views),
+                                          t(scenes.TX_POS), t(rxs))
+    return dict(scene=sc, rxs=rxs, views=views, views_d=t(views), rxs_d=t(rxs), tx=t(scenes.TX_POS),
+                targets_d=targets.contiguous())
 
 
 def run_ours(args):
@@ -187,47 +221,24 @@ def run_ours(args):
     import torch.distributed as dist
     from gsparc_b200 import _lib, raster, scenes
     from gsparc_b200.fused import FusedTrainer
+    from gsparc_b200.shared_mlp import SharedMLP
     from gsparc_b200.trainer import SplatTrainer
 
     world, rank, local, group = _dist_setup()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    sc = scenes.make_scene(P_GAUSS, scenes.SEED_SCENE)
-    tg = scenes.make_scene(P_GAUSS, scenes.SEED_TARGET)
-    rxs = scenes.make_receivers(POOL * world)[rank * POOL:(rank + 1) * POOL]   # receivers sharded over ranks
-    views = scenes.view_matrices(rxs)
-    t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
-    tx = t(scenes.TX_POS)
-    views_d, rxs_d = t(views), t(rxs)
-    tm, ts, tq, to = tg.activated()
-    with torch.no_grad():
-        targets_d, _, _, _ = raster.forward(t(tm), t(tg.mlp), t(to.reshape(-1)), t(ts), t(tq), 90, 360, 1.0,
-                                            views_d, tx, rxs_d)
+    # receivers sharded over ranks
+    d = _scene_data(P_GAUSS, POOL * world, dev)
+    sc = d["scene"]
+    sl = slice(rank * POOL, (rank + 1) * POOL)
+    views, rxs = d["views"][sl], d["rxs"][sl]
+    views_d, rxs_d, tx = d["views_d"][sl].contiguous(), d["rxs_d"][sl].contiguous(), d["tx"]
+    targets_d = d["targets_d"][sl].contiguous()
     targets_h = targets_d.cpu().pin_memory()
     views_h = torch.tensor(views).pin_memory()
     rxs_h = torch.tensor(rxs).pin_memory()
-    # the product path: the whole step captured in one CUDA graph, one receiver per step
-    trainer = FusedTrainer(sc, device=dev, group=group)
-    capacity = trainer.probe_capacity(views_d, rxs_d, tx)
-    trainer.capture(1, capacity, tx, views_d[0:1], rxs_d[0:1], targets_d[0:1])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
-
-    def dev_step(i):
-        j = i % POOL
-        return trainer.step(views_d[j:j + 1], rxs_d[j:j + 1], targets_d[j:j + 1])
-
-    loss_h = torch.empty((), dtype=torch.float32).pin_memory()
-
-    def host_step(i):
-        # target spectrum, view matrix and receiver position copied from pinned
-        # host memory into the graph's inputs; loss and rasterizer status back
-        j = i % POOL
-        loss = trainer.step(views_h[j:j + 1], rxs_h[j:j + 1], targets_h[j:j + 1])
-        loss_h.copy_(loss, non_blocking=True)
-        stream.synchronize()
-        trainer.plan.check()
-        return float(loss_h)
 
     def timed(fn, steps):
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
@@ -248,6 +259,27 @@ def run_ours(args):
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         return float(tt)
 
+    # ---- the product path on configs[1]: shared 2x64 ReLU MLP, FP32, one receiver per step, one CUDA graph
+    trainer = FusedTrainer(sc, device=dev, group=group, shared=SharedMLP(**SHARED_CFG1))
+    capacity = trainer.probe_capacity(views_d, rxs_d, tx)
+    trainer.capture(1, capacity, tx, views_d[0:1], rxs_d[0:1], targets_d[0:1])
+
+    def dev_step(i):
+        j = i % POOL
+        return trainer.step(views_d[j:j + 1], rxs_d[j:j + 1], targets_d[j:j + 1])
+
+    loss_h = torch.empty((), dtype=torch.float32).pin_memory()
+
+    def host_step(i):
+        # target spectrum, view matrix and receiver position copied from pinned
+        # host memory into the graph's inputs; loss and rasterizer status back
+        j = i % POOL
+        loss = trainer.step(views_h[j:j + 1], rxs_h[j:j + 1], targets_h[j:j + 1])
+        loss_h.copy_(loss, non_blocking=True)
+        stream.synchronize()
+        trainer.plan.check()
+        return float(loss_h)
+
     for i in range(args.warmup):
         dev_step(i)
     torch.cuda.synchronize()
@@ -257,25 +289,14 @@ def run_ours(args):
             timed(dev_step, max(1, args.steps // 4))
     trainer.plan.check()                      # the capacity held for every timed step
     value = args.steps * world / sec
-    # end to end through the public API with host buffers
     for i in range(min(args.warmup, 3)):
         host_step(i)
     e2e_sec = timed(host_step, args.steps)
     e2e = args.steps * world / e2e_sec
     h2d = (90 * 360 + 16 + 3) * 4
-    # the eager drop-in path (reference call surface, instance-count readback per step)
-    eager = SplatTrainer(sc, device=dev, group=group)
-
-    def eager_step(i):
-        j = i % POOL
-        return eager.step(views_d[j], rxs_d[j], tx, targets_d[j])
-
-    for i in range(3):
-        eager_step(i)
-    n_eager = max(1, min(args.steps, 50))
-    dropin = n_eager * world / timed(eager_step, n_eager)
-    # per-kernel device times from the same step run eagerly (graph replays
+    # per-kernel device times from eager runs of the same step (graph replays
     # bypass the library's event hooks; the kernels and their work are the same)
+    n_eager = max(1, min(args.steps, 50))
     for i in range(3):
         trainer.step_eager(views_d[i:i + 1], rxs_d[i:i + 1], tx, targets_d[i:i + 1])
     torch.cuda.synchronize()
@@ -285,49 +306,110 @@ def run_ours(args):
             trainer.step_eager(views_d[j:j + 1], rxs_d[j:j + 1], tx, targets_d[j:j + 1])
         torch.cuda.synchronize()
     ktimes = {k: v for k, v in kt.results().items() if v[1] > 0}
-    # kernels per timed call: the loss is two launches (the depth sort is one
-    # cooperative launch at this size, the optimizer one)
-    per_call = {"splat_loss_kernels": 2}
+    # kernels per timed call (the depth sort is one cooperative launch at this size, the optimizer one)
+    per_call = {"splat_loss_kernels": 2, "shared_mlp_forward_kernels": 5, "shared_mlp_backward_kernels": 11}
     launches = sum(c * per_call.get(k, 1) for k, (_, c) in ktimes.items()) // n_eager
     dom = max(ktimes, key=lambda k: ktimes[k][0])
-    # batched: every receiver of the pool in one captured step
-    btr = FusedTrainer(sc, device=dev, group=group)
-    btr.capture(POOL, capacity * POOL, tx, views_d, rxs_d, targets_d)
-    n_b = max(1, args.steps // 4)
-    bsec = timed(lambda i: btr.step(views_d, rxs_d, targets_d), n_b)
-    btr.plan.check()
-    batched = {"receivers_per_step": POOL, "steps_per_s": n_b * world / bsec,
-               "spectra_per_s": n_b * POOL * world / bsec}
     dom_ms = ktimes[dom][0] / ktimes[dom][1]
-    # algorithmic bytes per launch of the dominant kernel
     with torch.no_grad():
-        _, _, _, st = raster.forward(trainer.centre, trainer.mlp, trainer.act_opac, trainer.act_scales,
-                                     trainer.act_rots, 90, 360, 1.0, views_d[0], tx, rxs_d[0])
+        _, _, _, st = raster.forward(trainer.centre, None, trainer.act_opac, trainer.act_scales, trainer.act_rots,
+                                     90, 360, 1.0, views_d[0], tx, rxs_d[0], shared=trainer.shared,
+                                     shared_params=trainer.mlp)
     K = st.num_rendered
     vis = int((raster.state_views(st)["radii"] > 0).sum())
     npix = 90 * 360
-    alg = {
+    alg = {   # algorithmic bytes per launch, see DESIGN.md section 4
         "blend_backward_kernel": K * 36 + npix * 16 + vis * 40,
-        "blend_forward_kernel": K * 36 + npix * 16,
-        "preprocess_kernel": P_GAUSS * 44 + vis * 776 + P_GAUSS * 44,
+        "blend_forward_kernel": K * 36 + npix * 24,
+        "preprocess_kernel": P_GAUSS * 44 + P_GAUSS * 76,
         "depth_sort_kernels": P_GAUSS * 16 * 4,
         "segment_place_kernel": K * 12 + 138 * 8,
         "scatter_kernel": vis * 24 + K * 4,
-        "emission_backward_kernel": vis * (776 + 12 + 8) + P_GAUSS * 776,
         "geometry_backward_kernel": vis * (12 + 40 + 24 + 24 + 24) + P_GAUSS * 64,
-        "ssim_forward_kernel": npix * 8 + npix * 16,
-        "ssim_backward_kernel": npix * (8 + 16 + 4),
         "splat_loss_kernels": npix * (8 + 12) + npix * (8 + 12 + 4),
-        "gaussian_adam_kernels": P_GAUSS * (11 * 4 * 7 + 8 * 4) + P_GAUSS * 194 * 4 * 7,
+        "gaussian_adam_kernels": P_GAUSS * (11 * 4 * 7 + 8 * 4) + trainer.n_mlp * 4 * 7,
+        "shared_mlp_forward_kernels": P_GAUSS * (12 + 32 * 4 + 2 * 64 * 4 * 2 + 8),
+        "shared_mlp_backward_kernels": P_GAUSS * (32 * 4 + 2 * 64 * 4 * 3 + 8),
     }
     peak, peak_kind = _peaks()
     achieved = alg.get(dom, 0) / (dom_ms / 1000.0) / 1e9
     traffic = _traffic_per_launch().get(dom)
+
+    # ---- the reference's own emission model (per-Gaussian 3-32-2 MLPs) on the same step
+    ref_tr = FusedTrainer(sc, device=dev, group=group)
+    ref_tr.capture(1, capacity, tx, views_d[0:1], rxs_d[0:1], targets_d[0:1])
+    n_ref = max(1, args.steps // 2)
+    ref_sec = timed(lambda i: ref_tr.step(views_d[i % POOL:i % POOL + 1], rxs_d[i % POOL:i % POOL + 1],
+                                          targets_d[i % POOL:i % POOL + 1]), n_ref)
+    ref_tr.plan.check()
+    del ref_tr
+    # the eager drop-in path (reference call surface, instance-count readback per step)
+    eager = SplatTrainer(sc, device=dev, group=group)
+
+    def eager_step(i):
+        j = i % POOL
+        return eager.step(views_d[j], rxs_d[j], tx, targets_d[j])
+
+    for i in range(3):
+        eager_step(i)
+    dropin = n_eager * world / timed(eager_step, n_eager)
+    del eager
+    # 16 receivers per step, same model
+    btr = FusedTrainer(sc, device=dev, group=group, shared=SharedMLP(**SHARED_CFG1))
+    btr.capture(POOL, capacity * POOL, tx, views_d, rxs_d, targets_d)
+    n_b = max(1, args.steps // 4)
+    bsec = timed(lambda i: btr.step(views_d, rxs_d, targets_d), n_b)
+    btr.plan.check()
+    batched16 = {"receivers_per_step": POOL, "steps_per_s": n_b * world / bsec,
+                 "spectra_per_s": n_b * POOL * world / bsec}
+    del btr
+
+    # ---- batched BF16 (tcgen05) vs the plain per-receiver FP32 path on the same GPU
+    torch.cuda.empty_cache()
+    d3 = _scene_data(P_CFG3, R_CFG3 * world, dev)
+    s3 = slice(rank * R_CFG3, (rank + 1) * R_CFG3)
+    v3, r3, t3 = d3["views_d"][s3].contiguous(), d3["rxs_d"][s3].contiguous(), d3["targets_d"][s3].contiguous()
+    sc3 = d3["scene"]
+    # SSIM of BF16 and FP32 renders of the same parameters against the targets
+    from fused_ssim import fused_ssim
+    with torch.no_grad():
+        m3 = FusedTrainer(sc3, device=dev, shared=SharedMLP(**SHARED_CFG3, precision="fp32"))
+        ssim_d = []
+        for prec in ("fp32", "bf16"):
+            out, _, _, _ = raster.forward(m3.centre, None, m3.act_opac, m3.act_scales, m3.act_rots, 90, 360, 1.0,
+                                          v3[:4], tx, r3[:4], shared=SharedMLP(**SHARED_CFG3, precision=prec),
+                                          shared_params=m3.mlp)
+            ssim_d.append([float(fused_ssim(out[i][None, None], t3[i][None, None])) for i in range(4)])
+        dssim = max(abs(a - b) for a, b in zip(*ssim_d))
+        cap3 = m3.probe_capacity(v3, r3, tx)
+        del m3
+    plain = FusedTrainer(sc3, device=dev, group=group, shared=SharedMLP(**SHARED_CFG3, precision="fp32"))
+    plain.capture(1, cap3, tx, v3[0:1], r3[0:1], t3[0:1])
+    n_p = max(3, args.steps // 10)
+    psec = timed(lambda i: plain.step(v3[i % R_CFG3:i % R_CFG3 + 1], r3[i % R_CFG3:i % R_CFG3 + 1],
+                                      t3[i % R_CFG3:i % R_CFG3 + 1]), n_p)
+    plain.plan.check()
+    del plain
+    torch.cuda.empty_cache()
+    bf = FusedTrainer(sc3, device=dev, group=group, shared=SharedMLP(**SHARED_CFG3, precision="bf16"))
+    bf.capture(R_CFG3, cap3 * R_CFG3, tx, v3, r3, t3)
+    n_bf = max(3, args.steps // 20)
+    bfsec = timed(lambda i: bf.step(v3, r3, t3), n_bf)
+    bf.plan.check()
+    del bf
+    plain_sps = n_p * world / psec
+    bf_sps = n_bf * R_CFG3 * world / bfsec
+    cfg3 = {"workload": f"cfg3: P={P_CFG3}, shared emission MLP 3x128 GELU, 90x360, training step with adjoint",
+            "plain_fp32": {"receivers_per_step": 1, "steps_per_s": plain_sps, "spectra_per_s": plain_sps},
+            "batched_bf16": {"receivers_per_step": R_CFG3, "steps_per_s": n_bf * world / bfsec,
+                             "spectra_per_s": bf_sps},
+            "speedup_spectra_per_s": bf_sps / plain_sps,
+            "delta_ssim_bf16_vs_fp32": dssim}
+
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import raster as oraster
         from oracle.train_step import OracleTrainer
-        otr = OracleTrainer(sc)
+        otr = OracleTrainer(sc, shared=_oracle_shared(SHARED_CFG1))
         tgt0 = targets_d[0].cpu().numpy()
         t0 = time.perf_counter()
         otr.step(views[0], rxs[0], scenes.TX_POS, tgt0)
@@ -349,11 +431,13 @@ def run_ours(args):
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                              "avg_launch_ms": dom_ms, "algorithmic_bytes": alg.get(dom)},
                 "kernel_ms_per_step": {k: v[0] / n_eager for k, v in sorted(ktimes.items())},
+                "cfg3_batched_bf16_vs_plain_fp32": cfg3,
+                "reference_mlp_steps_per_s": n_ref * world / ref_sec,
                 "dropin_eager_steps_per_s": dropin,
-                "batched": batched,
-                "path": "CUDA-graph-captured step with flat training state, the fused L1+SSIM+confidence loss "
-                        "and the fused activation-adjoint Adam (gsparc_b200.fused.FusedTrainer), binning capacity "
-                        f"{capacity}",
+                "batched": batched16,
+                "path": "CUDA-graph-captured step (gsparc_b200.fused.FusedTrainer): flat training state, shared "
+                        "emission MLP, fused L1+SSIM+confidence loss, fused activation-adjoint Adam; binning "
+                        f"capacity {capacity}",
                 "cpu_baseline": cpu_base}
         print(json.dumps(line))
     if group is not None:

@@ -20,6 +20,8 @@
 //
 // This is the FP32 (SIMT) path: the layers are tiled SIMT GEMMs over the
 // R*P pair rows with the activations kept in a workspace for the adjoint.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -333,16 +335,21 @@ cudaError_t launch_shared_mlp_backward(int P, int R, int layers, int width, int 
   mlp_signal_backward_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(rows, out, work + L.s, geo.radii,
                                                                              dL_dsignal, dcur);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const int kchunk = 4096;
-  const unsigned zsplit = (unsigned)((rows + kchunk - 1) / kchunk);
   for (int l = layers; l >= 0; --l) {
     const int o = l == layers ? out : width;
     const int in = l == 0 ? kFeat : width;
     const float* xin = l == 0 ? work + L.x0 : work + L.a[l];
-    // dW_l[o, in] += sum_rows dZ[row, o] * X[row, in]
+    // dW_l[o, in] += sum_rows dZ[row, o] * X[row, in]: the row sum is split
+    // over grid.z so that about four CTAs per SM run, each folding its partial
+    // tile into dW with one atomic per element; chunks stay >= 128 rows.
     {
+      const unsigned gxy = (unsigned)(((o + kBM - 1) / kBM) * ((in + kBN - 1) / kBN));
+      const long long want_z = std::max<long long>(1, (4 * 148) / gxy);
+      long long kchunk = (rows + want_z - 1) / want_z;
+      kchunk = std::max<long long>(128, (kchunk + kBK - 1) / kBK * kBK);
+      const unsigned zsplit = (unsigned)((rows + kchunk - 1) / kchunk);
       dim3 grid((o + kBM - 1) / kBM, (in + kBN - 1) / kBN, zsplit);
-      mlp_gemm_kernel<kEpiAtomic><<<grid, 256, 0, s>>>(o, in, (int)rows, kchunk, dcur, 1, o, xin, in, 1,
+      mlp_gemm_kernel<kEpiAtomic><<<grid, 256, 0, s>>>(o, in, (int)rows, (int)kchunk, dcur, 1, o, xin, in, 1,
                                                        dL_dparams + L.w[l], in, nullptr, 0, nullptr, nullptr);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       mlp_colsum_kernel<<<dim3((o + 31) / 32, (unsigned)((rows + 2047) / 2048)), 256, 0, s>>>(

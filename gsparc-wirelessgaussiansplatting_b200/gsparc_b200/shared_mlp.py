@@ -26,6 +26,23 @@ ACTS = {"relu": 1, "gelu": 2}
 PRECISIONS = {"fp32": 0, "bf16": 1}
 
 
+def _shapes(layers, width, out):
+    dims = [FEATURES] + [width] * layers + [out]
+    return [(dims[i + 1], dims[i]) for i in range(len(dims) - 1)]
+
+
+def init_params_host(layers, width, out=1, seed=0):
+    """nn.Linear's default initialisation (uniform +-1/sqrt(fan_in)) per
+    layer, flat fp32 on the host (torch CPU generator, seeded)."""
+    g = torch.Generator().manual_seed(seed)
+    parts = []
+    for o, i in _shapes(layers, width, out):
+        bound = 1.0 / math.sqrt(i)
+        parts.append(((torch.rand((o, i), generator=g) * 2 - 1) * bound).reshape(-1))
+        parts.append((torch.rand((o,), generator=g) * 2 - 1) * bound)
+    return torch.cat(parts).numpy()
+
+
 class SharedMLP:
     """Spec of the shared MLP plus the workspace its forward keeps for the
     backward (sized per (P, R) on first use)."""
@@ -45,18 +62,11 @@ class SharedMLP:
 
     def shapes(self):
         """[(out, in)] per layer, input layer first."""
-        dims = [FEATURES] + [self.width] * self.layers + [self.out]
-        return [(dims[i + 1], dims[i]) for i in range(len(dims) - 1)]
+        return _shapes(self.layers, self.width, self.out)
 
     def init_params(self, seed=0, device="cuda"):
         """nn.Linear's default initialisation (uniform +-1/sqrt(fan_in)) per layer."""
-        g = torch.Generator().manual_seed(seed)
-        parts = []
-        for o, i in self.shapes():
-            bound = 1.0 / math.sqrt(i)
-            parts.append((torch.rand((o, i), generator=g) * 2 - 1) * bound)
-            parts.append((torch.rand((o,), generator=g) * 2 - 1) * bound)
-        flat = torch.cat([p.reshape(-1) for p in parts]).to(device)
+        flat = torch.from_numpy(init_params_host(self.layers, self.width, self.out, seed)).to(device)
         assert flat.numel() == self.n_params
         return flat
 

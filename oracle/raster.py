@@ -655,9 +655,15 @@ def mark_visible(means, view):
 
 
 def render(means, scales, rots, opac, mlp, view, tx, rx, H, W, mod=1.0,
-           tile_h=16, tile_w=16, dtype=np.float32):
-    """Whole forward for one receiver: preprocess -> bin/sort -> blend."""
+           tile_h=16, tile_w=16, dtype=np.float32, signal_fn=None):
+    """Whole forward for one receiver: preprocess -> bin/sort -> blend.
+    ``signal_fn(radii) -> [P,2]`` replaces the per-Gaussian MLP's signals
+    (the shared emission MLP); ``mlp`` may then be None."""
+    if mlp is None:
+        mlp = np.zeros(194 * means.shape[0], np.float32)
     pre = preprocess(means, scales, rots, opac, mlp, view, tx, rx, H, W, mod, tile_h, tile_w, dtype)
+    if signal_fn is not None:
+        pre["signal"] = signal_fn(pre["radii"]).astype(pre["signal"].dtype)
     keys, vals, ranges = bin_and_sort(pre["means2D"].astype(np.float32), pre["depth"].astype(np.float32),
                                       pre["radii"], H, W, tile_h, tile_w)
     out, fT, nc = blend_forward(ranges, vals, pre["means2D"], pre["conic_opacity"], pre["signal"],
@@ -676,7 +682,10 @@ def render_backward(fwd, means, scales, rots, opac, mlp, view, tx, rx, dL_dout, 
         fwd["final_T"], fwd["n_contrib"], dL_dout, H, W, tile_h, tile_w, dtype, ref_compat)
     dmean3_geo, dcov, dscale, drot = geometry_backward(
         means, scales, rots, view, pre["radii"], pre["cov3D"], dmean2, dconic, H, W, mod, dtype, ref_compat)
-    dmlp, dmean3_mlp = emission_backward(means, mlp, tx, rx, pre["radii"], dsig, dtype)
+    if mlp is None:   # shared emission MLP: its adjoint is the caller's (dL_dsignal)
+        dmlp, dmean3_mlp = None, np.zeros_like(dmean3_geo)
+    else:
+        dmlp, dmean3_mlp = emission_backward(means, mlp, tx, rx, pre["radii"], dsig, dtype)
     return dict(dL_dmeans2D=dmean2, dL_dmeans3D=dmean3_geo + dmean3_mlp, dL_dmlp=dmlp,
                 dL_dopacity=dopac.reshape(-1, 1), dL_dcov3D=dcov, dL_dscales=dscale,
                 dL_drotations=drot, dL_dconic=dconic, dL_dsignal=dsig)

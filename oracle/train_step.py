@@ -16,15 +16,21 @@ from __future__ import annotations
 import numpy as np
 
 from . import raster, ssim
+from . import shared_mlp as smlp
 
 LR = dict(centre=0.00016, log_scale=0.005, rotation=0.001, opacity_logit=0.0055, mlp=0.002, conf=0.001)
 
 
 class OracleTrainer:
-    def __init__(self, scene, H=90, W=360, seed=0):
+    """``shared=(layers, width, act, params)`` selects the shared emission MLP
+    (oracle/shared_mlp.py) instead of the scene's per-Gaussian MLPs."""
+
+    def __init__(self, scene, H=90, W=360, seed=0, shared=None):
         self.H, self.W = H, W
+        self.shared = shared
+        mlp = scene.mlp.copy() if shared is None else np.asarray(shared[3], np.float32).copy()
         self.p = dict(centre=scene.means.copy(), log_scale=scene.log_scales.copy(), rotation=scene.quats.copy(),
-                      opacity_logit=scene.opacity_logits.copy(), mlp=scene.mlp.copy())
+                      opacity_logit=scene.opacity_logits.copy(), mlp=mlp)
         rng = np.random.default_rng(seed)
         lim1 = np.sqrt(6.0 / (3 + 32))
         lim2 = np.sqrt(6.0 / (32 + 1))
@@ -41,7 +47,19 @@ class OracleTrainer:
         qn = np.linalg.norm(p["rotation"], axis=1, keepdims=True)
         rots = (p["rotation"] / qn).astype(f32)
         opac = (1.0 / (1.0 + np.exp(-p["opacity_logit"]))).astype(f32)
-        fwd = raster.render(p["centre"], scales, rots, opac, p["mlp"], view, tx, rx, self.H, self.W, dtype=f32)
+        if self.shared is None:
+            fwd = raster.render(p["centre"], scales, rots, opac, p["mlp"], view, tx, rx, self.H, self.W, dtype=f32)
+        else:
+            layers, width, act = self.shared[:3]
+            cache = {}
+
+            def signal_fn(radii):
+                s, cache["c"] = smlp.forward(p["mlp"], layers, width, act, p["centre"], rx, radii)
+                cache["radii"] = radii
+                return np.stack([s * (radii > 0), np.zeros_like(s)], 1)
+
+            fwd = raster.render(p["centre"], scales, rots, opac, None, view, tx, rx, self.H, self.W, dtype=f32,
+                                signal_fn=signal_fn)
         pred = fwd["out"][0]
         N = pred.size
         l1 = np.abs(pred - target).mean()
@@ -62,8 +80,14 @@ class OracleTrainer:
         gc["w1"] = dh[:, None] * rx[None, :]
         gc["b1"] = dh
         dL = np.stack([dpred, np.zeros_like(dpred)]).astype(f32)
-        g = raster.render_backward(fwd, p["centre"], scales, rots, opac, p["mlp"], view, tx, rx, dL, self.H, self.W,
-                                   dtype=f32, ref_compat=True)
+        g = raster.render_backward(fwd, p["centre"], scales, rots, opac, p["mlp"] if self.shared is None else None,
+                                   view, tx, rx, dL, self.H, self.W, dtype=f32, ref_compat=True)
+        if self.shared is not None:
+            layers, width, act = self.shared[:3]
+            dmlp, dm = smlp.backward(p["mlp"], layers, width, act, p["centre"], rx, cache["radii"], cache["c"],
+                                     g["dL_dsignal"][:, 0])
+            g["dL_dmlp"] = dmlp
+            g["dL_dmeans3D"] = g["dL_dmeans3D"] + dm
         gp = dict(centre=np.nan_to_num(g["dL_dmeans3D"], nan=0.0), mlp=g["dL_dmlp"],
                   log_scale=g["dL_dscales"] * scales,
                   opacity_logit=g["dL_dopacity"] * opac * (1 - opac))
