@@ -2,28 +2,36 @@
 //
 // Same network as shared_mlp.cu (features, hidden layers of width 128,
 // sigmoid of one output) with BF16 operands and FP32 accumulation in tensor
-// memory.  Two fused kernels, each a persistent loop over tiles of 128
-// (receiver, Gaussian) rows with one row per thread of a 128-thread CTA:
+// memory.  Two fused persistent kernels over tiles of 128 (receiver, Gaussian)
+// rows, one row per thread of a 128-thread warpgroup:
 //
-//   forward:  features -> [MMA -> +bias, act] x layers -> output dot on the
-//             CUDA cores -> sigmoid.  The layer weights stay in shared memory
-//             for the whole launch; only the BF16 pre-activations of each
-//             hidden layer (for the adjoint) and the signal go to HBM.
-//   backward: from dL/dsignal, per tile and layer l (last first):
-//               dW_l (+ db_l)  += dZ_l^T [A_{l-1} | 1]   (M = 128 outputs,
-//                                 K = 128 rows, accumulated in TMEM over all
-//                                 of the CTA's tiles; the ones row yields db)
-//               dA_{l-1}        = dZ_l W_l             (M = 128 rows)
-//             with A_{l-1} = act(Z_{l-1}) recomputed from the stored
-//             pre-activations and the features recomputed from the centres;
-//             the output layer's gradient is reduced on the CUDA cores.  At
-//             the end every CTA adds its TMEM accumulators to the global
-//             gradient.
+//   forward:  four warpgroups per CTA, each with its own tile in flight and
+//             its own 128 TMEM columns; per layer the group's leader issues
+//             the MMA, the group runs the +bias/activation epilogue.  The
+//             weights are staged in shared memory once per CTA; only the BF16
+//             pre-activations (for the adjoint) and the signal go to HBM.
+//   backward: two compute warpgroups, each with its own tile, and one MMA
+//             warp that issues every MMA of the CTA (so all accumulation into
+//             the shared weight-gradient columns is in issue order).  Per tile
+//             and hidden layer l (last first):
+//               dW_l | db_l += dZ_l^T [A_{l-1} | 1]   (M = 128 outputs, K = the
+//                              128 rows; accumulated in TMEM over all tiles)
+//               dA_{l-1}     = dZ_l W_l              (M = 128 rows; one
+//                              shared scratch accumulator)
+//             A_{l-1} = act(Z_{l-1}) and act'(Z_{l-1}) come from one pass over
+//             the stored pre-activations (one CDF evaluation per element;
+//             act' is held in registers as FP16 until dA arrives); the output
+//             layer's gradient is reduced on the CUDA cores.  At the end the
+//             CTA adds its TMEM accumulators to the global gradient.
 //
-// Operands use the no-swizzle core-matrix layouts of tcgen05.cuh.  One thread
-// issues the MMAs; completion is signalled through an mbarrier (bounded wait:
-// on give-up the error word gets kErrMlpWait and the CTA stops).
+// Operands use the no-swizzle core-matrix layouts of tcgen05.cuh.  A buffer
+// written row-per-thread in the K-major layout of a [rows x cols] matrix is
+// also the MN-major layout of its transpose (same core matrices, LBO and SBO
+// exchanged), which is how dZ and A feed the weight-gradient MMA without a
+// transposed copy.  Every wait is bounded: on give-up the error word gets
+// kErrMlpWait and the CTA stops.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -36,16 +44,50 @@ namespace {
 constexpr int kH = 128;        // hidden width of the BF16 path
 constexpr int kFin = 32;       // features
 constexpr int kRows = 128;     // rows per tile (= MMA M)
+constexpr int kFwdGroups = 4;  // forward: warpgroups (tiles in flight) per CTA
+constexpr int kBwdGroups = 2;  // backward: compute warpgroups per CTA (+ one MMA warp)
+constexpr int kBwdThreads = kBwdGroups * 128 + 32;
 constexpr uint32_t kLbo = 128; // core matrices along K are adjacent
+constexpr uint32_t kSboX = (kFin / 8) * 128u;         // [rows x 32] K-major
+constexpr uint32_t kSboH = (kH / 8) * 128u;           // [rows x 128] K-major
+constexpr uint32_t kSboA = ((kH + 16) / 8) * 128u;    // [rows x 144] K-major (activations | ones)
 constexpr uint32_t kPolls = 1u << 24;
 constexpr float kPiF = 3.14159265358979323846f;
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_d(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+// GELU's normal CDF Phi(z) = (1 + erf(z / sqrt 2)) / 2 by Abramowitz & Stegun
+// 7.1.26 (Hastings' rational approximation, |error of erf| <= 1.5e-7, three
+// orders below the BF16 rounding the results go through):
+//   erf(x) = 1 - t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2),
+//   t = 1 / (1 + p x), x >= 0, odd extension for x < 0.
+// exp(-z^2 / 2) is returned too: it is also the density term of GELU'.
+__device__ __forceinline__ float gelu_cdf(float z, float& ez) {
+  const float ax = fabsf(z) * 0.70710678118654752f;
+  ez = __expf(-0.5f * z * z);
+  const float tt = __fdividef(1.0f, fmaf(0.3275911f, ax, 1.0f));
+  float p = fmaf(tt, 1.061405429f, -1.453152027f);
+  p = fmaf(tt, p, 1.421413741f);
+  p = fmaf(tt, p, -0.284496736f);
+  p = fmaf(tt, p, 0.254829592f);
+  const float e = fmaf(-(tt * p), ez, 1.0f);   // erf(|z| / sqrt 2)
+  return 0.5f + copysignf(0.5f * e, z);
 }
-__device__ __forceinline__ float actf(int act, float z) { return act == 1 ? fmaxf(z, 0.0f) : gelu(z); }
-__device__ __forceinline__ float actd(int act, float z) { return act == 1 ? (z > 0.0f ? 1.0f : 0.0f) : gelu_d(z); }
+__device__ __forceinline__ float actf(int act, float z) {
+  if (act == 1) return fmaxf(z, 0.0f);
+  float ez;
+  return z * gelu_cdf(z, ez);
+}
+// activation and its derivative from one evaluation
+__device__ __forceinline__ void act_and_grad(int act, float z, float& a, float& d) {
+  if (act == 1) {
+    a = fmaxf(z, 0.0f);
+    d = z > 0.0f ? 1.0f : 0.0f;
+  } else {
+    float ez;
+    const float ph = gelu_cdf(z, ez);
+    a = z * ph;
+    d = fmaf(z * 0.39894228040143268f, ez, ph);
+  }
+}
 
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
   const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -65,29 +107,48 @@ __device__ __forceinline__ void unpack8(uint4 u, float* v) {
   }
 }
 
-// Features of one pair (as mlp_features_kernel), zero for culled pairs.
+// (receiver, Gaussian) of row row0 + t, with one 64-bit division per tile.
+__device__ __forceinline__ void row_pair(size_t row0, int t, int P, int& r, int& g) {
+  const size_t rr = row0 / (size_t)P;
+  int gg = (int)(row0 - rr * (size_t)P) + t;
+  int ri = (int)rr;
+  while (gg >= P) {   // at most 128 / P + 1 steps
+    gg -= P;
+    ++ri;
+  }
+  r = ri;
+  g = gg;
+}
+
+// Features of one pair (as mlp_features_kernel), zero for culled pairs.  The
+// positional encoding's higher octaves come from the first by the double-angle
+// identities: the arguments are exact power-of-two multiples of the first, so
+// only a few FP32 ulps separate them from direct sin/cos, far below BF16.
 __device__ __forceinline__ void pair_features(const float* __restrict__ means3D, const float* __restrict__ rx_pos,
-                                              int P, size_t row, bool vis, float* x) {
+                                              int g, int r, bool vis, float* x) {
   if (!vis) {
 #pragma unroll
     for (int i = 0; i < kFin; ++i) x[i] = 0.0f;
     return;
   }
-  const int g = (int)(row % P), r = (int)(row / P);
   const float m[3] = {means3D[3 * g], means3D[3 * g + 1], means3D[3 * g + 2]};
   const float v[3] = {m[0] - rx_pos[3 * r], m[1] - rx_pos[3 * r + 1], m[2] - rx_pos[3 * r + 2]};
   const float d2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
   const float d = sqrtf(d2);
   x[0] = m[0]; x[1] = m[1]; x[2] = m[2];
 #pragma unroll
-  for (int k = 0; k < 4; ++k)
+  for (int j = 0; j < 3; ++j) {
+    float s, c;
+    sincosf(kPiF * m[j], &s, &c);
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      float s, c;
-      sincosf((float)(1 << k) * kPiF * m[j], &s, &c);
+    for (int k = 0; k < 4; ++k) {
       x[3 + 6 * k + 2 * j] = s;
       x[4 + 6 * k + 2 * j] = c;
+      const float s2 = 2.0f * s * c, c2 = fmaf(c, c, -s * s);
+      s = s2;
+      c = c2;
     }
+  }
   x[27] = v[0] / d; x[28] = v[1] / d; x[29] = v[2] / d;
   x[30] = 1.0f / d2;
   x[31] = 0.0f;
@@ -108,59 +169,49 @@ __device__ __forceinline__ float warp_transpose_sum32(float (&v)[32], int lane) 
   return v[0];
 }
 
-struct TileSync {
-  uint64_t* mbar;
-  uint32_t phase;
-  // all threads: make generic smem writes visible to the MMA and order TMEM use
-  __device__ __forceinline__ void publish() {
-    tc::fence_async_smem();
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-  }
-  __device__ __forceinline__ bool wait() {
-    const bool ok = tc::mbar_wait(mbar, phase, kPolls);
-    phase ^= 1u;
-    tc::fence_after_sync();
-    return ok;
-  }
-};
+// Warpgroup-local ordering of generic shared-memory writes and TMEM reads
+// before the group's leader issues MMAs that read / overwrite them.
+__device__ __forceinline__ void group_publish(uint32_t bar_id) {
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  tc::named_sync(bar_id, 128);
+  tc::fence_after_sync();
+}
 
 }  // namespace
 
 // ---- forward ------------------------------------------------------------------
-// dynamic smem: W_l K-major [128 x in_l] bf16 (l < layers), X [128 x 32],
-// H [128 x 128] K-major bf16, biases and the output row in fp32.
-template <int kLayers>
-__global__ void __launch_bounds__(128)
-mlp_bf16_forward_kernel(int P, size_t rows, int act, const float* __restrict__ means3D,
+// dynamic smem: W_l K-major [128 x in_l] bf16 (the B operand: n = output,
+// k = input), then per warpgroup an activation tile H [128 x 128] K-major bf16
+// whose first 8 KB also hold the feature tile X [128 x 32]; biases and the
+// output row in fp32.
+template <int kLayers, int act>
+__global__ void __launch_bounds__(128 * kFwdGroups, 1)
+mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                         const float* __restrict__ rx_pos, const float* __restrict__ params,
                         const int* __restrict__ radii, __nv_bfloat16* __restrict__ zb, float* __restrict__ S,
                         float2* __restrict__ signal, ImageHeader* __restrict__ hdr) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar[kFwdGroups];
   __shared__ uint32_t tbase;
-  const int t = threadIdx.x, warp = t >> 5;
+  const int tid = threadIdx.x, t = tid & 127, grp = tid >> 7, warp = tid >> 5;
   unsigned char* Ws[kLayers];
   size_t off = 0;
   for (int l = 0; l < kLayers; ++l) {
     Ws[l] = smem + off;
     off += (size_t)kH * (l == 0 ? kFin : kH) * 2;
   }
-  unsigned char* Xs = smem + off;
-  off += (size_t)kRows * kFin * 2;
-  unsigned char* Hs = smem + off;
-  off += (size_t)kRows * kH * 2;
-  float* bias = reinterpret_cast<float*>(smem + off);   // [kLayers][128], then w_out[128], b_out
+  unsigned char* Hs = smem + off + (size_t)grp * kRows * kH * 2;
+  off += (size_t)kFwdGroups * kRows * kH * 2;
+  float* bias = reinterpret_cast<float*>(smem + off);   // [kLayers][128], then w_out[128]
   float* wout = bias + kLayers * kH;
 
-  // weights -> bf16 K-major (B operand: n = output, k = input), once per CTA
   size_t poff = 0;
   for (int l = 0; l < kLayers; ++l) {
     const int in = l == 0 ? kFin : kH;
     const float* W = params + poff;
     const uint32_t sbo = (uint32_t)(in / 8) * 128u;
-    for (int c = t; c < kH * (in / 8); c += blockDim.x) {
+    for (int c = tid; c < kH * (in / 8); c += blockDim.x) {
       const int n = c / (in / 8), kc = c % (in / 8);
       float v[8];
 #pragma unroll
@@ -168,44 +219,54 @@ mlp_bf16_forward_kernel(int P, size_t rows, int act, const float* __restrict__ m
       *reinterpret_cast<uint4*>(Ws[l] + tc::kmajor_off(n, kc * 8, kLbo, sbo)) = pack8(v);
     }
     poff += (size_t)kH * in;
-    for (int j = t; j < kH; j += blockDim.x) bias[l * kH + j] = params[poff + j];
+    for (int j = tid; j < kH; j += blockDim.x) bias[l * kH + j] = params[poff + j];
     poff += kH;
   }
-  for (int j = t; j < kH; j += blockDim.x) wout[j] = params[poff + j];
+  for (int j = tid; j < kH; j += blockDim.x) wout[j] = params[poff + j];
   const float bout = params[poff + kH];
-  if (t == 0) tc::mbar_init(&mbar, 1);
-  if (warp == 0) tc::tmem_alloc(&tbase, kH);
-  TileSync sync{&mbar, 0u};
-  sync.publish();
-  const uint32_t tmem = tbase;
-  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  if (tid == 0)
+    for (int q = 0; q < kFwdGroups; ++q) tc::mbar_init(&mbar[q], 1);
+  if (warp == 0) tc::tmem_alloc(&tbase, kFwdGroups * kH);
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tbase + (uint32_t)(grp * kH);
+  const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+  const uint32_t bar_id = 1u + (uint32_t)grp;
+  uint32_t phase = 0;
   bool ok = true;
   const size_t ntiles = (rows + kRows - 1) / kRows;
-  for (size_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const size_t row = tile * kRows + t;
+  for (size_t tile = (size_t)blockIdx.x * kFwdGroups + grp; tile < ntiles; tile += (size_t)gridDim.x * kFwdGroups) {
+    const size_t row0 = tile * kRows, row = row0 + t;
     const bool valid = row < rows;
     const bool vis = valid && radii[row] > 0;
     {
+      int r, g;
+      row_pair(row0, t, P, r, g);
       float x[kFin];
-      pair_features(means3D, rx_pos, P, row, vis, x);
+      pair_features(means3D, rx_pos, g, r, vis, x);
 #pragma unroll
       for (int kc = 0; kc < kFin / 8; ++kc)
-        *reinterpret_cast<uint4*>(Xs + tc::kmajor_off(t, kc * 8, kLbo, (kFin / 8) * 128u)) = pack8(x + kc * 8);
+        *reinterpret_cast<uint4*>(Hs + tc::kmajor_off(t, kc * 8, kLbo, kSboX)) = pack8(x + kc * 8);
     }
-    sync.publish();
     float o = bout;
-    for (int l = 0; l < kLayers && ok; ++l) {
+    for (int l = 0; l < kLayers; ++l) {
       const int in = l == 0 ? kFin : kH;
+      group_publish(bar_id);
       if (t == 0) {
         const uint32_t sbo = (uint32_t)(in / 8) * 128u;
-        const uint32_t a0 = tc::smem_u32(l == 0 ? Xs : Hs), b0 = tc::smem_u32(Ws[l]);
+        const uint32_t a0 = tc::smem_u32(Hs), b0 = tc::smem_u32(Ws[l]);
         const uint32_t idesc = tc::idesc_bf16(kRows, kH, false, false);
         for (int kk = 0; kk < in / 16; ++kk)
           tc::mma_bf16(tmem, tc::smem_desc(a0 + kk * 2 * kLbo, kLbo, sbo),
                        tc::smem_desc(b0 + kk * 2 * kLbo, kLbo, sbo), idesc, kk > 0 ? 1u : 0u);
-        tc::commit(&mbar);
+        tc::commit(&mbar[grp]);
       }
-      if (!sync.wait()) {
+      const bool got = tc::mbar_wait(&mbar[grp], phase, kPolls);
+      phase ^= 1u;
+      tc::fence_after_sync();
+      if (!tc::named_all(bar_id, 128, got)) {
         ok = false;
         break;
       }
@@ -227,16 +288,16 @@ mlp_bf16_forward_kernel(int P, size_t rows, int act, const float* __restrict__ m
 #pragma unroll
           for (int i = 0; i < 8; ++i) a[i] = actf(act, zr[i]);
           if (l + 1 < kLayers) {
-            *reinterpret_cast<uint4*>(Hs + tc::kmajor_off(t, c0 + q * 8, kLbo, (kH / 8) * 128u)) = pack8(a);
+            *reinterpret_cast<uint4*>(Hs + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = pack8(a);
           } else {
 #pragma unroll
             for (int i = 0; i < 8; ++i) o += wout[c0 + q * 8 + i] * a[i];
           }
         }
       }
-      sync.publish();
     }
-    if (ok && valid) {
+    if (!ok) break;
+    if (valid) {
       const float s = 1.0f / (1.0f + expf(-o));
       S[row] = s;
       if (vis) signal[row] = make_float2(s, 0.0f);
@@ -245,43 +306,43 @@ mlp_bf16_forward_kernel(int P, size_t rows, int act, const float* __restrict__ m
   if (!ok && t == 0 && hdr) atomic_or_error(hdr, kErrMlpWait);
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, kH);
+  if (warp == 0) tc::tmem_dealloc(tbase, kFwdGroups * kH);
 }
 
 // ---- backward -----------------------------------------------------------------
 // dynamic smem: W_l as the MN-major B operand of dA = dZ W ([n = in_l] x
-// [k = 128 outputs]) for every layer; dZ K-major and MN-major [128 x 128];
-// A_{l-1} MN-major [(in + 16) x 128 rows] (row `in` = ones, the rest of the
-// 16 extra rows zero); the output row and its gradient in fp32.
-// TMEM columns: dW_l accumulators of (in_l + 16) columns each, then a
-// 144-column scratch accumulator.
-template <int kLayers>
-__global__ void __launch_bounds__(128)
-mlp_bf16_backward_kernel(int P, size_t rows, int act, const float* __restrict__ means3D,
+// [k = 128 outputs]) for every layer; per compute warpgroup dZ [128 rows x 128]
+// and A [128 rows x 144] (activations, then a ones column and 15 zero columns),
+// both K-major by row; the output row in fp32.
+// TMEM columns: dW_l accumulators of (in_l + 16) columns each (last layer
+// first), then one 128-column scratch accumulator for dA.
+template <int kLayers, int act>
+__global__ void __launch_bounds__(kBwdThreads, 1)
+mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                          const float* __restrict__ rx_pos, const float* __restrict__ params,
                          const int* __restrict__ radii, const __nv_bfloat16* __restrict__ zb,
                          const float* __restrict__ S, const float* __restrict__ dL_dsignal,
                          float* __restrict__ dX0, float* __restrict__ dparams, ImageHeader* __restrict__ hdr) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t bar_ready[kBwdGroups];
+  __shared__ __align__(8) uint64_t bar_done[kBwdGroups];
+  __shared__ __align__(8) uint64_t bar_free;
   __shared__ uint32_t tbase;
+  __shared__ int s_fail;
   __shared__ float s_dwo[kH + 1];
-  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int grp = tid >> 7;   // compute warpgroup 0..kBwdGroups-1; kBwdGroups = the MMA warp
+  const int t = tid & 127;
+  constexpr size_t kGroupBytes = (size_t)kRows * kH * 2 + (size_t)kRows * (kH + 16) * 2;
   unsigned char* Wb[kLayers];
   size_t off = 0;
   for (int l = 0; l < kLayers; ++l) {
     Wb[l] = smem + off;
     off += (size_t)(l == 0 ? kFin : kH) * kH * 2;
   }
-  unsigned char* dZk = smem + off;
-  off += (size_t)kRows * kH * 2;
-  unsigned char* dZm = smem + off;
-  off += (size_t)kH * kRows * 2;
-  unsigned char* Am = smem + off;
-  off += (size_t)(kH + 16) * kRows * 2;
+  unsigned char* const groups = smem + off;
+  off += kBwdGroups * kGroupBytes;
   float* wout = reinterpret_cast<float*>(smem + off);
-  constexpr uint32_t kSboRows = (kRows / 8) * 128u;   // MN-major, K = 128 rows
-  constexpr uint32_t kSboH = (kH / 8) * 128u;         // K-major / MN-major with K = 128
 
   // W_l [out][in] -> MN-major B operand (n = in, k = out), once per CTA
   size_t poff = 0;
@@ -290,7 +351,7 @@ mlp_bf16_backward_kernel(int P, size_t rows, int act, const float* __restrict__ 
     const int in = l == 0 ? kFin : kH;
     woff[l] = poff;
     const float* W = params + poff;
-    for (int c = t; c < kH * (in / 8); c += blockDim.x) {
+    for (int c = tid; c < kH * (in / 8); c += blockDim.x) {
       const int k = c / (in / 8), nc = c % (in / 8);   // k = output row of W, nc = group of 8 inputs
       float v[8];
 #pragma unroll
@@ -303,171 +364,253 @@ mlp_bf16_backward_kernel(int P, size_t rows, int act, const float* __restrict__ 
   }
   woff[kLayers] = poff;
   boff[kLayers] = poff + kH;
-  for (int j = t; j < kH; j += blockDim.x) wout[j] = params[woff[kLayers] + j];
-  for (int j = t; j <= kH; j += blockDim.x) s_dwo[j] = 0.0f;
-  if (t == 0) tc::mbar_init(&mbar, 1);
+  for (int j = tid; j < kH; j += blockDim.x) wout[j] = params[woff[kLayers] + j];
+  for (int j = tid; j <= kH; j += blockDim.x) s_dwo[j] = 0.0f;
+  unsigned char* const dZ = groups + (size_t)(grp < kBwdGroups ? grp : 0) * kGroupBytes;
+  unsigned char* const Ab = dZ + (size_t)kRows * kH * 2;
+  if (grp < kBwdGroups) {   // the constant ones column (db) of the activation tile
+    const uint4 one = make_uint4(pack2(1.0f, 0.0f), 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kH, kLbo, kSboA)) = one;
+    *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kH + 8, kLbo, kSboA)) = make_uint4(0u, 0u, 0u, 0u);
+  }
+  if (tid == 0) {
+    for (int q = 0; q < kBwdGroups; ++q) {
+      tc::mbar_init(&bar_ready[q], 128);
+      tc::mbar_init(&bar_done[q], 1);
+    }
+    tc::mbar_init(&bar_free, 128);
+    s_fail = 0;
+  }
   if (warp == 0) tc::tmem_alloc(&tbase, 512);
-  TileSync sync{&mbar, 0u};
-  sync.publish();
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
   const uint32_t tmem = tbase;
-  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
   uint32_t dwcol[kLayers];
   uint32_t col = 0;
   for (int l = kLayers - 1; l >= 0; --l) {
     dwcol[l] = col;
     col += (l == 0 ? kFin : kH) + 16;
   }
-  const uint32_t scratch = col;   // <= 144 + 144 + 48 = 336; scratch needs 128 more
-  bool ok = true;
-  bool any_tile = false;
+  const uint32_t scratch = col;   // <= 144 + 144 + 48 = 336; the scratch needs 128 more
   const size_t ntiles = (rows + kRows - 1) / kRows;
-  for (size_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const size_t row = tile * kRows + t;
-    const bool valid = row < rows;
-    const bool vis = valid && radii[row] > 0;
-    // output layer: dO, its weight gradient (reduced over the warp's rows), dZ of the last hidden layer
-    const float s = valid ? S[row] : 0.0f;
-    const float dO = vis ? dL_dsignal[2 * row] * s * (1.0f - s) : 0.0f;
-    {
-      const __nv_bfloat16* zl = zb + (size_t)(kLayers - 1) * rows * kH;
-#pragma unroll 1
-      for (int c0 = 0; c0 < kH; c0 += 32) {
-        float z[32], red[32];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          if (valid) unpack8(*reinterpret_cast<const uint4*>(zl + row * kH + c0 + q * 8), z + q * 8);
-          else
-#pragma unroll
-            for (int i = 0; i < 8; ++i) z[q * 8 + i] = 0.0f;
+  const size_t tile_stride = (size_t)gridDim.x * kBwdGroups;
+
+  if (grp == kBwdGroups) {
+    // ---- MMA warp: one thread issues every MMA of the CTA, in the order
+    // (tile round, layer, group), so both groups' weight gradients accumulate
+    // into the same TMEM columns in issue order.
+    if (lane == 0) {
+      uint32_t ph_ready[kBwdGroups] = {};
+      bool first[kLayers];
+      for (int l = 0; l < kLayers; ++l) first[l] = true;
+      uint32_t n_da = 0;
+      bool ok = true;
+      for (size_t base = (size_t)blockIdx.x * kBwdGroups; base < ntiles && ok; base += tile_stride) {
+        for (int l = kLayers - 1; l >= 0 && ok; --l) {
+          const int in = l == 0 ? kFin : kH;
+          for (int q = 0; q < kBwdGroups; ++q) {
+            if (base + q >= ntiles) break;
+            if (!tc::mbar_wait(&bar_ready[q], ph_ready[q], kPolls)) {
+              ok = false;
+              break;
+            }
+            ph_ready[q] ^= 1u;
+            tc::fence_after_sync();
+            const uint32_t zq = tc::smem_u32(groups + (size_t)q * kGroupBytes);
+            const uint32_t aq = zq + (uint32_t)(kRows * kH * 2);
+            // dW_l | db_l += dZ^T [A | 1]: A operand dZ^T (M = outputs, K = rows) and
+            // B operand [A | 1]^T (N = in + 16, K = rows), both MN-major views of the
+            // row-major tiles (core-matrix stride 128 B along M/N, one row group along K)
+            const uint32_t id_w = tc::idesc_bf16(kH, in + 16, true, true);
+            for (int kk = 0; kk < kRows / 16; ++kk)
+              tc::mma_bf16(tmem + dwcol[l], tc::smem_desc(zq + kk * 2 * kSboH, kSboH, 128u),
+                           tc::smem_desc(aq + kk * 2 * kSboA, kSboA, 128u), id_w,
+                           (!first[l] || kk > 0) ? 1u : 0u);
+            first[l] = false;
+            // dA_{l-1} = dZ_l W_l into the scratch, once its previous reader has drained it
+            if (n_da > 0) {
+              if (!tc::mbar_wait(&bar_free, (n_da - 1) & 1u, kPolls)) {
+                ok = false;
+                break;
+              }
+              tc::fence_after_sync();
+            }
+            const uint32_t id_x = tc::idesc_bf16(kRows, in, false, true);
+            const uint32_t wb = tc::smem_u32(Wb[l]);
+            for (int kk = 0; kk < kH / 16; ++kk)
+              tc::mma_bf16(tmem + scratch, tc::smem_desc(zq + kk * 2 * kLbo, kLbo, kSboH),
+                           tc::smem_desc(wb + kk * 2 * kLbo, kLbo, kSboH), id_x, kk > 0 ? 1u : 0u);
+            ++n_da;
+            tc::commit(&bar_done[q]);
+          }
         }
-#pragma unroll
-        for (int i = 0; i < 32; ++i) red[i] = dO * actf(act, z[i]);
-        const float sum = warp_transpose_sum32(red, lane);
-        atomicAdd(&s_dwo[c0 + lane], sum);
-        float dz[32];
-#pragma unroll
-        for (int i = 0; i < 32; ++i) dz[i] = dO * wout[c0 + i] * actd(act, z[i]);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const uint4 p = pack8(dz + q * 8);
-          *reinterpret_cast<uint4*>(dZk + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = p;
-        }
-        // MN-major copy: element (m = output c0 + i, k = row t)
-#pragma unroll
-        for (int i = 0; i < 32; ++i)
-          *reinterpret_cast<__nv_bfloat16*>(dZm + tc::mnmajor_off(c0 + i, t, kLbo, kSboRows)) =
-              __float2bfloat16_rn(dz[i]);
       }
-      float dsum = dO;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
-      if (lane == 0) atomicAdd(&s_dwo[kH], dsum);
+      if (!ok) s_fail = 1;
     }
-    for (int l = kLayers - 1; l >= 0 && ok; --l) {
-      const int in = l == 0 ? kFin : kH;
-      // A_{l-1}: features (l == 0) or act(Z_{l-1}), MN-major with the ones row at n = in
-      if (l == 0) {
-        float x[kFin];
-        pair_features(means3D, rx_pos, P, row, vis, x);
-#pragma unroll
-        for (int i = 0; i < kFin; ++i)
-          *reinterpret_cast<__nv_bfloat16*>(Am + tc::mnmajor_off(i, t, kLbo, kSboRows)) = __float2bfloat16_rn(x[i]);
-      } else {
-        const __nv_bfloat16* zp = zb + (size_t)(l - 1) * rows * kH;
-#pragma unroll 1
-        for (int c0 = 0; c0 < kH; c0 += 8) {
-          float z[8];
-          if (valid) unpack8(*reinterpret_cast<const uint4*>(zp + row * kH + c0), z);
-          else
-#pragma unroll
-            for (int i = 0; i < 8; ++i) z[i] = 0.0f;
-#pragma unroll
-          for (int i = 0; i < 8; ++i)
-            *reinterpret_cast<__nv_bfloat16*>(Am + tc::mnmajor_off(c0 + i, t, kLbo, kSboRows)) =
-                __float2bfloat16_rn(actf(act, z[i]));
+  } else {
+    // ---- compute warpgroup
+    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+    const uint32_t bar_id = 1u + (uint32_t)grp;
+    uint32_t ph_done = 0;
+    bool ok = true;
+    for (size_t tile = (size_t)blockIdx.x * kBwdGroups + grp; tile < ntiles && ok; tile += tile_stride) {
+      const size_t row0 = tile * kRows, row = row0 + t;
+      const bool valid = row < rows;
+      if (t == 0) {
+        // into L2 ahead of use: this tile's remaining pre-activation slabs (one
+        // contiguous 32 KB range per layer), then the next tile's first inputs
+        const uint32_t n = (uint32_t)(rows - row0 < (size_t)kRows ? rows - row0 : (size_t)kRows);
+        for (int l = 0; l + 1 < kLayers; ++l) tc::prefetch_l2(zb + (size_t)l * rows * kH + row0 * kH, n * kH * 2);
+        const size_t nt = tile + tile_stride;
+        if (nt < ntiles) {
+          const size_t r1 = nt * kRows;
+          const uint32_t n1 = (uint32_t)(rows - r1 < (size_t)kRows ? rows - r1 : (size_t)kRows);
+          tc::prefetch_l2(zb + (size_t)(kLayers - 1) * rows * kH + r1 * kH, n1 * kH * 2);
+          tc::prefetch_l2(S + r1, n1 * 4);
+          tc::prefetch_l2(radii + r1, n1 * 4);
+          tc::prefetch_l2(dL_dsignal + 2 * r1, n1 * 8);
         }
       }
-#pragma unroll
-      for (int i = 0; i < 16; ++i)
-        *reinterpret_cast<__nv_bfloat16*>(Am + tc::mnmajor_off(in + i, t, kLbo, kSboRows)) =
-            __float2bfloat16_rn(i == 0 ? 1.0f : 0.0f);
-      sync.publish();
-      if (t == 0) {
-        const uint32_t zm = tc::smem_u32(dZm), zk = tc::smem_u32(dZk), am = tc::smem_u32(Am), wb = tc::smem_u32(Wb[l]);
-        // dW_l | db_l  (M = 128 outputs, N = in + 16, K = 128 rows; both operands MN-major)
-        const uint32_t id_w = tc::idesc_bf16(kH, in + 16, true, true);
-        for (int kk = 0; kk < kRows / 16; ++kk)
-          tc::mma_bf16(tmem + dwcol[l], tc::smem_desc(zm + kk * 2 * kLbo, kLbo, kSboRows),
-                       tc::smem_desc(am + kk * 2 * kLbo, kLbo, kSboRows), id_w, (any_tile || kk > 0) ? 1u : 0u);
-        // dA_{l-1} = dZ_l W_l  (M = 128 rows, N = in, K = 128 outputs)
-        const uint32_t id_x = tc::idesc_bf16(kRows, in, false, true);
-        for (int kk = 0; kk < kH / 16; ++kk)
-          tc::mma_bf16(tmem + scratch, tc::smem_desc(zk + kk * 2 * kLbo, kLbo, kSboH),
-                       tc::smem_desc(wb + kk * 2 * kLbo, kLbo, kSboH), id_x, kk > 0 ? 1u : 0u);
-        tc::commit(&mbar);
-      }
-      if (!sync.wait()) {
-        ok = false;
-        break;
-      }
-      if (l == 0) {
-        float v[32];
-        tc::tmem_ld32(tmem + lane_base + scratch, v);
-        if (valid)
-#pragma unroll
-          for (int q = 0; q < 8; ++q)
-            *reinterpret_cast<float4*>(dX0 + row * kFin + q * 4) =
-                make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-      } else {
-        const __nv_bfloat16* zp = zb + (size_t)(l - 1) * rows * kH;
+      const bool vis = valid && radii[row] > 0;
+      // output layer: dO, its weight gradient (reduced over the warp's rows), dZ of the last hidden layer
+      const float s = valid ? S[row] : 0.0f;
+      const float dO = vis ? dL_dsignal[2 * row] * s * (1.0f - s) : 0.0f;
+      {
+        const uint4* zl = reinterpret_cast<const uint4*>(zb + (size_t)(kLayers - 1) * rows * kH + row * kH);
 #pragma unroll 1
         for (int c0 = 0; c0 < kH; c0 += 32) {
-          float v[32], z[32];
-          tc::tmem_ld32(tmem + lane_base + scratch + c0, v);
+          uint4 zq[4];   // a 32-column chunk of the row in flight at once
+#pragma unroll
+          for (int q = 0; q < 4; ++q) zq[q] = valid ? zl[c0 / 8 + q] : make_uint4(0u, 0u, 0u, 0u);
+          float red[32];
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            if (valid) unpack8(*reinterpret_cast<const uint4*>(zp + row * kH + c0 + q * 8), z + q * 8);
+            float z[8], dz[8];
+            unpack8(zq[q], z);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              float a, d;
+              act_and_grad(act, z[i], a, d);
+              red[q * 8 + i] = dO * a;
+              dz[i] = dO * wout[c0 + q * 8 + i] * d;
+            }
+            *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = pack8(dz);
+          }
+          const float sum = warp_transpose_sum32(red, lane);
+          atomicAdd(&s_dwo[c0 + lane], sum);
+        }
+        float dsum = dO;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+        if (lane == 0) atomicAdd(&s_dwo[kH], dsum);
+      }
+      for (int l = kLayers - 1; l >= 0; --l) {
+        // act'(Z_{l-1}) of this row, kept for dZ_{l-1} after the MMAs as FP16 pairs
+        // (nine warps leave 168 registers a thread; the FP16 rounding, 2^-11
+        // relative, sits below the BF16 rounding of dZ that follows)
+        __half2 ad[kH / 2];
+        // A_{l-1}: features (l == 0) or act(Z_{l-1}); the ones column sits at `in`
+        if (l == 0) {
+          int r, g;
+          row_pair(row0, t, P, r, g);
+          float x[kFin];
+          pair_features(means3D, rx_pos, g, r, vis, x);
+#pragma unroll
+          for (int kc = 0; kc < kFin / 8; ++kc)
+            *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kc * 8, kLbo, kSboA)) = pack8(x + kc * 8);
+          *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kFin, kLbo, kSboA)) =
+              make_uint4(pack2(1.0f, 0.0f), 0u, 0u, 0u);
+          *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kFin + 8, kLbo, kSboA)) = make_uint4(0u, 0u, 0u, 0u);
+        } else {
+          const __nv_bfloat16* zp = zb + (size_t)(l - 1) * rows * kH + row * kH;
+#pragma unroll
+          for (int c0 = 0; c0 < kH; c0 += 8) {
+            float z[8], a[8];
+            if (valid) unpack8(*reinterpret_cast<const uint4*>(zp + c0), z);
             else
 #pragma unroll
-              for (int i = 0; i < 8; ++i) z[q * 8 + i] = 0.0f;
+              for (int i = 0; i < 8; ++i) z[i] = 0.0f;
+            float d[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) act_and_grad(act, z[i], a[i], d[i]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) ad[c0 / 2 + i] = __floats2half2_rn(d[2 * i], d[2 * i + 1]);
+            *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, c0, kLbo, kSboA)) = pack8(a);
           }
+        }
+        // hand dZ_l and A_{l-1} to the MMA warp
+        tc::fence_async_smem();
+        tc::mbar_arrive(&bar_ready[grp]);
+        const bool got = tc::mbar_wait(&bar_done[grp], ph_done, kPolls);
+        ph_done ^= 1u;
+        tc::fence_after_sync();
+        if (!tc::named_all(bar_id, 128, got)) {
+          ok = false;
+          break;
+        }
+        if (l == 0) {
+          float v[32];
+          tc::tmem_ld32(tmem + lane_base + scratch, v);
+          tc::fence_before_sync();
+          tc::mbar_arrive(&bar_free);
+          if (valid)
 #pragma unroll
-          for (int i = 0; i < 32; ++i) v[i] = valid ? v[i] * actd(act, z[i]) : 0.0f;
+            for (int q = 0; q < 8; ++q)
+              *reinterpret_cast<float4*>(dX0 + row * kFin + q * 4) =
+                  make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        } else {
+          // dZ_{l-1} = dA_{l-1} * act'(Z_{l-1}); the MMAs that read dZ_l are done
 #pragma unroll
-          for (int q = 0; q < 4; ++q)
-            *reinterpret_cast<uint4*>(dZk + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = pack8(v + q * 8);
+          for (int c0 = 0; c0 < kH; c0 += 32) {
+            float v[32];
+            tc::tmem_ld32(tmem + lane_base + scratch + c0, v);
+            if (c0 + 32 == kH) {
+              tc::fence_before_sync();
+              tc::mbar_arrive(&bar_free);
+            }
 #pragma unroll
-          for (int i = 0; i < 32; ++i)
-            *reinterpret_cast<__nv_bfloat16*>(dZm + tc::mnmajor_off(c0 + i, t, kLbo, kSboRows)) =
-                __float2bfloat16_rn(v[i]);
+            for (int i = 0; i < 16; ++i) {
+              const float2 d = __half22float2(ad[c0 / 2 + i]);
+              v[2 * i] *= d.x;
+              v[2 * i + 1] *= d.y;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = pack8(v + q * 8);
+          }
         }
       }
-      sync.publish();
     }
-    any_tile = true;
+    if (!ok && t == 0) s_fail = 1;
   }
-  // the CTA's weight and bias gradients -> global (rows of dW_l are TMEM lanes)
-  if (ok && any_tile) {
+  __syncthreads();
+  tc::fence_after_sync();
+  // the CTA's weight and bias gradients -> global (rows of dW_l are TMEM lanes);
+  // (layer, 32-column chunk) items are split over the compute warpgroups
+  if (!s_fail && grp < kBwdGroups) {
+    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+    int item = 0;
     for (int l = 0; l < kLayers; ++l) {
       const int in = l == 0 ? kFin : kH;
-      const int m = warp * 32 + lane;
 #pragma unroll 1
-      for (int c0 = 0; c0 <= in; c0 += 32) {
+      for (int c0 = 0; c0 <= in; c0 += 32, ++item) {
+        if (item % kBwdGroups != grp) continue;
         float v[32];
         tc::tmem_ld32(tmem + lane_base + dwcol[l] + c0, v);
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
           const int n = c0 + i;
-          if (n < in) atomicAdd(&dparams[woff[l] + (size_t)m * in + n], v[i]);
-          else if (n == in) atomicAdd(&dparams[boff[l] + m], v[i]);
+          if (n < in) atomicAdd(&dparams[woff[l] + (size_t)t * in + n], v[i]);
+          else if (n == in) atomicAdd(&dparams[boff[l] + t], v[i]);
         }
       }
     }
-    __syncthreads();
-    for (int j = t; j <= kH; j += blockDim.x)
-      atomicAdd(&dparams[j < kH ? woff[kLayers] + j : boff[kLayers]], s_dwo[j]);
+    if (grp == 0)
+      for (int j = t; j <= kH; j += 128) atomicAdd(&dparams[j < kH ? woff[kLayers] + j : boff[kLayers]], s_dwo[j]);
   }
-  if (!ok && t == 0 && hdr) atomic_or_error(hdr, kErrMlpWait);
+  if (s_fail && tid == 0 && hdr) atomic_or_error(hdr, kErrMlpWait);
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tmem, 512);
@@ -476,41 +619,62 @@ mlp_bf16_backward_kernel(int P, size_t rows, int act, const float* __restrict__ 
 // ---- launchers ------------------------------------------------------------------
 
 size_t mlp_bf16_forward_smem(int layers) {
-  return (size_t)kH * kFin * 2 + (size_t)(layers - 1) * kH * kH * 2 + (size_t)kRows * kFin * 2 +
-         (size_t)kRows * kH * 2 + (size_t)(layers * kH + kH + 4) * sizeof(float);
+  return (size_t)kH * kFin * 2 + (size_t)(layers - 1) * kH * kH * 2 + (size_t)kFwdGroups * kRows * kH * 2 +
+         (size_t)(layers * kH + kH + 4) * sizeof(float);
 }
 size_t mlp_bf16_backward_smem(int layers) {
-  return (size_t)kFin * kH * 2 + (size_t)(layers - 1) * kH * kH * 2 + 2 * (size_t)kRows * kH * 2 +
-         (size_t)(kH + 16) * kRows * 2 + (size_t)kH * sizeof(float);
+  return (size_t)kFin * kH * 2 + (size_t)(layers - 1) * kH * kH * 2 +
+         (size_t)kBwdGroups * ((size_t)kRows * kH * 2 + (size_t)kRows * (kH + 16) * 2) + (size_t)kH * sizeof(float);
 }
 
-template <int L>
-static cudaError_t launch_bf16_layers(bool fwd, int P, size_t rows, int act, const float* means3D,
-                                      const float* rx_pos, const float* params, const GeomView& geo,
-                                      const SharedMlpLayout& Lt, float* work, const float* dL_dsignal,
-                                      float* dparams, ImageHeader* hdr, cudaStream_t s) {
+template <int L, int A>
+static cudaError_t launch_bf16_layers(bool fwd, int P, size_t rows, const float* means3D, const float* rx_pos,
+                                      const float* params, const GeomView& geo, const SharedMlpLayout& Lt,
+                                      float* work, const float* dL_dsignal, float* dparams, ImageHeader* hdr,
+                                      cudaStream_t s) {
   const size_t smem = fwd ? mlp_bf16_forward_smem(L) : mlp_bf16_backward_smem(L);
-  static bool attr_done[2][64] = {};
+  static bool attr_done[2][64] = {};   // per instantiation
+  static int sm_count[64] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
+  int sms = dev >= 0 && dev < 64 ? sm_count[dev] : 0;
+  if (sms == 0) {
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64) sm_count[dev] = sms;
+  }
   if (dev < 0 || dev >= 64 || !attr_done[fwd][dev]) {
-    e = fwd ? cudaFuncSetAttribute(mlp_bf16_forward_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-            : cudaFuncSetAttribute(mlp_bf16_backward_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = fwd ? cudaFuncSetAttribute(mlp_bf16_forward_kernel<L, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem)
+            : cudaFuncSetAttribute(mlp_bf16_backward_kernel<L, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem);
     if (e != cudaSuccess) return e;
     if (dev >= 0 && dev < 64) attr_done[fwd][dev] = true;
   }
+  // persistent: at most one CTA per SM, and every CTA's first warpgroup owns a tile
   const size_t ntiles = (rows + kRows - 1) / kRows;
-  const unsigned grid = (unsigned)(ntiles < 148 ? ntiles : 148);
+  const size_t per = fwd ? kFwdGroups : kBwdGroups;
+  const size_t want = (ntiles + per - 1) / per;
+  const unsigned grid = (unsigned)(want < (size_t)sms ? want : (size_t)sms);
   __nv_bfloat16* zb = reinterpret_cast<__nv_bfloat16*>(work + Lt.z[1]);
   if (fwd)
-    mlp_bf16_forward_kernel<L><<<grid, 128, smem, s>>>(P, rows, act, means3D, rx_pos, params, geo.radii, zb,
-                                                       work + Lt.s, geo.signal, hdr);
+    mlp_bf16_forward_kernel<L, A><<<grid, 128 * kFwdGroups, smem, s>>>(P, rows, means3D, rx_pos, params, geo.radii,
+                                                                       zb, work + Lt.s, geo.signal, hdr);
   else
-    mlp_bf16_backward_kernel<L><<<grid, 128, smem, s>>>(P, rows, act, means3D, rx_pos, params, geo.radii, zb,
-                                                        work + Lt.s, dL_dsignal, work + Lt.d0, dparams, hdr);
+    mlp_bf16_backward_kernel<L, A><<<grid, kBwdThreads, smem, s>>>(P, rows, means3D, rx_pos, params, geo.radii, zb,
+                                                                   work + Lt.s, dL_dsignal, work + Lt.d0, dparams,
+                                                                   hdr);
   return cudaGetLastError();
+}
+
+template <int L>
+static cudaError_t launch_bf16_act(bool fwd, int P, size_t rows, int act, const float* means3D, const float* rx_pos,
+                                   const float* params, const GeomView& geo, const SharedMlpLayout& Lt, float* work,
+                                   const float* dL_dsignal, float* dparams, ImageHeader* hdr, cudaStream_t s) {
+  return act == 1 ? launch_bf16_layers<L, 1>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work, dL_dsignal,
+                                             dparams, hdr, s)
+                  : launch_bf16_layers<L, 2>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work, dL_dsignal,
+                                             dparams, hdr, s);
 }
 
 cudaError_t launch_shared_mlp_bf16(bool fwd, int P, int R, int layers, int act, const float* means3D,
@@ -525,9 +689,9 @@ cudaError_t launch_shared_mlp_bf16(bool fwd, int P, int R, int layers, int act, 
     if (e != cudaSuccess) return e;
   }
   switch (layers) {
-    case 1: e = launch_bf16_layers<1>(fwd, P, rows, act, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
-    case 2: e = launch_bf16_layers<2>(fwd, P, rows, act, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
-    case 3: e = launch_bf16_layers<3>(fwd, P, rows, act, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
+    case 1: e = launch_bf16_act<1>(fwd, P, rows, act, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
+    case 2: e = launch_bf16_act<2>(fwd, P, rows, act, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
+    case 3: e = launch_bf16_act<3>(fwd, P, rows, act, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
     default: return cudaErrorInvalidValue;
   }
   if (e != cudaSuccess || fwd) return e;

@@ -101,7 +101,9 @@ def _bf(x):
 
 def torch_bf16_emulation(mlp, params, means, rxs, radii, dsig):
     """The BF16 tensor-core path's arithmetic restated in torch: operands
-    rounded to BF16 where the kernels round them, FP32 accumulation.
+    rounded to BF16 where the kernels round them (and the hidden layers'
+    activation derivatives to FP16, as the adjoint holds them), FP32
+    accumulation.
     Returns (signal, dparams, dmeans)."""
     act = (lambda z: F.relu(z)) if mlp.act == "relu" else (lambda z: F.gelu(z))
     layers = mlp.unflatten(params)
@@ -136,7 +138,7 @@ def torch_bf16_emulation(mlp, params, means, rxs, radii, dsig):
             if l == 0:
                 dX0 = dA
             else:
-                dz = _bf(dA * torch.func.grad(lambda q: act(q).sum())(zs[l - 1]))
+                dz = _bf(dA * torch.func.grad(lambda q: act(q).sum())(zs[l - 1]).half().float())
         dparams = torch.cat([g.reshape(-1) for g in grads])
     # centres: through the features only
     mm = means.detach().clone().requires_grad_(True)
