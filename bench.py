@@ -9,7 +9,7 @@ loss, the full hand-written adjoint, Adam.  Each step uses the next receiver
 of a pool; targets are spectra of a second seeded scene at those receivers.
 Synthetic data (no dataset in the container).
 
-value: steps/s of configs[1] (20,000 Gaussians, shared emission MLP 2x64 ReLU,
+value: steps/s of the 20,000-Gaussian training workload (shared emission MLP 2x64 ReLU,
 FP32, one receiver per step) captured in one CUDA graph (FusedTrainer: flat
 training state, fused L1+SSIM+confidence loss, fused activation-adjoint
 Adam; every launch one of this library's kernels) with inputs resident in
@@ -19,7 +19,11 @@ e2e: the same step through FusedTrainer.step with the receiver's target
 spectrum, view matrix and position copied from pinned host memory every
 step and the loss and rasterizer status read back to the host, inside the
 timed region.
-cfg3_batched_bf16_vs_plain_fp32: configs[3]'s model (200,000 Gaussians,
+cfg2_batched_clustered_autotuned: the clustered batched workload (50,000 Gaussians, 30% in five
+clusters, 64 receivers per step, shared 2x64 ReLU MLP, FP32): the tile shape
+picked by FusedTrainer.autotune_tile from {16x16, 8x32, 32x8} (graph replays
+timed per shape), then spectra/s of the captured step at that shape.
+cfg3_batched_bf16_vs_plain_fp32: the 200,000-Gaussian workload's model (200,000 Gaussians,
 shared MLP 3x128 GELU): the training step with 32 receivers per step and the
 MLP in BF16 on the tcgen05 tensor cores, against the plain per-receiver FP32
 step, in spectra/s, with the SSIM difference of their renders.
@@ -54,6 +58,7 @@ P_GAUSS = 20000
 POOL = 16
 SHARED_CFG1 = dict(layers=2, width=64, act="relu")    # emission MLP of configs 0-1
 SHARED_CFG3 = dict(layers=3, width=128, act="gelu")   # emission MLP of config 3
+P_CFG2, R_CFG2 = 50000, 64
 P_CFG3, R_CFG3 = 200000, 32
 WORKLOAD = ("cfg1_train_20k: per-receiver training step (forward + L1/SSIM/confidence loss + hand-written adjoint "
             "+ Adam), P=20000 Gaussians uniform in a 10x8x3 m room, one 90x360 spectrum per step, 16x16 tiles, "
@@ -259,7 +264,7 @@ def run_ours(args):
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         return float(tt)
 
-    # ---- the product path on configs[1]: shared 2x64 ReLU MLP, FP32, one receiver per step, one CUDA graph
+    # ---- the product path on the 20k workload: shared 2x64 ReLU MLP, FP32, one receiver per step, one CUDA graph
     trainer = FusedTrainer(sc, device=dev, group=group, shared=SharedMLP(**SHARED_CFG1))
     capacity = trainer.probe_capacity(views_d, rxs_d, tx)
     trainer.capture(1, capacity, tx, views_d[0:1], rxs_d[0:1], targets_d[0:1])
@@ -307,7 +312,7 @@ def run_ours(args):
         torch.cuda.synchronize()
     ktimes = {k: v for k, v in kt.results().items() if v[1] > 0}
     # kernels per timed call (the depth sort is one cooperative launch at this size, the optimizer one)
-    per_call = {"splat_loss_kernels": 2, "shared_mlp_forward_kernels": 5, "shared_mlp_backward_kernels": 11}
+    per_call = {"splat_loss_kernels": 2, "shared_mlp_forward_kernels": 1, "shared_mlp_backward_kernels": 2}
     launches = sum(c * per_call.get(k, 1) for k, (_, c) in ktimes.items()) // n_eager
     dom = max(ktimes, key=lambda k: ktimes[k][0])
     dom_ms = ktimes[dom][0] / ktimes[dom][1]
@@ -318,7 +323,7 @@ def run_ours(args):
     K = st.num_rendered
     vis = int((raster.state_views(st)["radii"] > 0).sum())
     npix = 90 * 360
-    alg = {   # algorithmic bytes per launch, see DESIGN.md section 4
+    alg = {   # algorithmic bytes per launch (per-unit figures x the launch's units)
         "blend_backward_kernel": K * 36 + npix * 16 + vis * 40,
         "blend_forward_kernel": K * 36 + npix * 24,
         "preprocess_kernel": P_GAUSS * 44 + P_GAUSS * 76,
@@ -364,7 +369,25 @@ def run_ours(args):
                  "spectra_per_s": n_b * POOL * world / bsec}
     del btr
 
-    # ---- batched BF16 (tcgen05) vs the plain per-receiver FP32 path on the same GPU
+    # ---- 50,000 clustered Gaussians, 64 receivers per step, tile shape autotuned
+    torch.cuda.empty_cache()
+    d2 = _scene_data(P_CFG2, R_CFG2 * world, dev, cluster_frac=0.3)
+    s2 = slice(rank * R_CFG2, (rank + 1) * R_CFG2)
+    v2, r2, t2 = d2["views_d"][s2].contiguous(), d2["rxs_d"][s2].contiguous(), d2["targets_d"][s2].contiguous()
+    tr2 = FusedTrainer(d2["scene"], device=dev, group=group, shared=SharedMLP(**SHARED_CFG1))
+    tune = tr2.autotune_tile(tx, v2, r2, t2, steps=3)
+    n2 = max(3, args.steps // 20)
+    sec2 = timed(lambda i: tr2.step(v2, r2, t2), n2)
+    K2, _ = tr2.plan.host_status()
+    tr2.plan.check()
+    cfg2 = {"workload": f"cfg2: P={P_CFG2} (30% in 5 N(c_k, 0.3 m) clusters), {R_CFG2} receivers per step, shared "
+                        "emission MLP 2x64 ReLU, FP32, training step with adjoint, CUDA graph",
+            "tile_ms_per_step": {f"{h}x{w}": ms for (h, w), ms in tune.items()},
+            "tile": "%dx%d" % tr2.tile, "instances_K": K2,
+            "steps_per_s": n2 * world / sec2, "spectra_per_s": n2 * R_CFG2 * world / sec2}
+    del tr2, d2
+
+    # ---- 200,000 Gaussians, 3x128 GELU: batched BF16 (tcgen05) vs the plain per-receiver FP32 path on the same GPU
     torch.cuda.empty_cache()
     d3 = _scene_data(P_CFG3, R_CFG3 * world, dev)
     s3 = slice(rank * R_CFG3, (rank + 1) * R_CFG3)
@@ -431,6 +454,7 @@ def run_ours(args):
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                              "avg_launch_ms": dom_ms, "algorithmic_bytes": alg.get(dom)},
                 "kernel_ms_per_step": {k: v[0] / n_eager for k, v in sorted(ktimes.items())},
+                "cfg2_batched_clustered_autotuned": cfg2,
                 "cfg3_batched_bf16_vs_plain_fp32": cfg3,
                 "reference_mlp_steps_per_s": n_ref * world / ref_sec,
                 "dropin_eager_steps_per_s": dropin,

@@ -180,22 +180,30 @@ class FusedTrainer:
 
     # ---- capacity, capture, replay -----------------------------------------------
 
-    def probe_capacity(self, views, rxs, tx, margin=1.25, slack=4096):
+    def probe_capacity(self, views, rxs, tx, margin=1.25, slack=4096, tile=(16, 16)):
+        """Binning capacity per receiver: the largest instance count over the
+        given receivers (current parameters, tile shape `tile`) with margin."""
         kmax = 0
         with torch.no_grad():
             for r in range(views.shape[0]):
                 _, _, _, st = raster.forward(self.centre, self._mlp_arg(), self.act_opac, self.act_scales,
-                                             self.act_rots, self.H, self.W, 1.0, views[r], tx, rxs[r],
+                                             self.act_rots, self.H, self.W, 1.0, views[r], tx, rxs[r], tile=tile,
                                              **self._shared_kw())
                 kmax = max(kmax, st.num_rendered)
         return int(kmax * margin) + slack
 
-    def capture(self, R, capacity, tx, views=None, rxs=None, targets=None, warmup=3):
-        """Capture the step for R receivers per step in a CUDA graph.  Warm-up
+    def _state(self):
+        return (self.params, self.exp_avg, self.exp_avg_sq, self.step_count)
+
+    def capture(self, R, capacity, tx, views=None, rxs=None, targets=None, warmup=3, tile=(16, 16)):
+        """Capture the step for R receivers per step in a CUDA graph (binning
+        capacity `capacity` instances in total, tile shape `tile`).  Warm-up
         steps (on a side stream, as capture requires) use the given batch;
         parameters and optimizer state are restored afterwards."""
         dev = self.device
-        self.plan = RasterPlan(self.P, R, self.H, self.W, capacity, dev, grad_mode=self.grad_mode)
+        self.graph = None
+        self.tile = tuple(tile)
+        self.plan = RasterPlan(self.P, R, self.H, self.W, capacity, dev, tile=tile, grad_mode=self.grad_mode)
         self._buffers(R)
         self._s_views = torch.eye(4, device=dev).repeat(R, 1, 1).contiguous()
         self._s_rxs = torch.zeros((R, 3), device=dev)
@@ -205,7 +213,7 @@ class FusedTrainer:
             self._s_views.copy_(views.reshape(self._s_views.shape))
             self._s_rxs.copy_(rxs.reshape(self._s_rxs.shape))
             self._s_targets.copy_(targets.reshape(self._s_targets.shape))
-        state = (self.params, self.exp_avg, self.exp_avg_sq, self.step_count)
+        state = self._state()
         saved = [t.clone() for t in state]
         side = torch.cuda.Stream(dev)
         side.wait_stream(torch.cuda.current_stream(dev))
@@ -222,6 +230,38 @@ class FusedTrainer:
                 t.copy_(s)
         self.activate()
         torch.cuda.synchronize(dev)
+
+    def autotune_tile(self, tx, views, rxs, targets, shapes=((16, 16), (8, 32), (32, 8)), steps=5, margin=1.25):
+        """Pick the tile shape of the R-receiver step (R = len(views)) by
+        measurement: for each shape, probe the binning capacity, capture the
+        step and time `steps` graph replays with CUDA events; parameters and
+        optimizer state are restored after every trial.  Leaves the fastest
+        shape captured and returns {shape: ms per step}."""
+        R = views.shape[0]
+        dev = self.device
+        state = self._state()
+        saved = [t.clone() for t in state]
+        stream = torch.cuda.current_stream(dev)
+        times, caps = {}, {}
+        for tile in shapes:
+            caps[tile] = self.probe_capacity(views, rxs, tx, margin=margin, tile=tile) * R
+            self.capture(R, caps[tile], tx, views, rxs, targets, tile=tile)
+            self.step(views, rxs, targets)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(steps):
+                self.step(views, rxs, targets)
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            self.plan.check()
+            times[tile] = a.elapsed_time(b) / steps
+            with torch.no_grad():
+                for t, s in zip(state, saved):
+                    t.copy_(s)
+            self.activate()
+        best = min(times, key=times.get)
+        self.capture(R, caps[best], tx, views, rxs, targets, tile=best)
+        return times
 
     def step(self, views, rxs, targets):
         """Copy a batch of R receivers (device or pinned host tensors) into the

@@ -1,7 +1,7 @@
 """CPU restatement (numpy) of the shared emission MLP of
 gsparc_b200.shared_mlp / csrc/shared_mlp.cu, for one receiver.
 
-TEST / BASELINE INFRASTRUCTURE ONLY: used by the CPU training step that
+TEST / CPU-BASELINE INFRASTRUCTURE ONLY: used by the CPU training step that
 bench.py times; never used by the product.
 
 Features per Gaussian (receiver rx): centre mu, sin/cos(2^k pi mu_j) for
@@ -33,7 +33,9 @@ def unflatten(flat, layers, width, out=1):
     return res
 
 
-def features(means, rx, radii):
+def features(means, rx, radii, dtype=np.float32):
+    means = means.astype(dtype)
+    rx = np.asarray(rx).astype(dtype)
     v = means - rx[None, :]
     d2 = (v * v).sum(1, keepdims=True)
     d = np.sqrt(d2)
@@ -44,7 +46,7 @@ def features(means, rx, radii):
             pe += [np.sin(w * means[:, j]), np.cos(w * means[:, j])]
     with np.errstate(all="ignore"):
         x = np.concatenate([means, np.stack(pe, 1), v / d, 1.0 / d2, np.zeros_like(d)], 1)
-    return np.where((radii > 0)[:, None], x, 0.0).astype(np.float32)
+    return np.where((radii > 0)[:, None], x, 0.0).astype(dtype)
 
 
 def _act(act, z):
@@ -57,19 +59,20 @@ def _act_grad(act, z):
     return 0.5 * (1 + erf(z / math.sqrt(2))) + z * np.exp(-0.5 * z * z) / math.sqrt(2 * math.pi)
 
 
-def forward(params, layers, width, act, means, rx, radii):
-    """Returns (signal [P], cache)."""
-    lay = unflatten(params, layers, width)
-    x = features(means, rx, radii)
+def forward(params, layers, width, act, means, rx, radii, dtype=np.float32):
+    """Returns (signal [P], cache); computed in `dtype` (float64 for the FP64
+    oracle render)."""
+    lay = [(w.astype(dtype), b.astype(dtype)) for w, b in unflatten(params, layers, width)]
+    x = features(means, rx, radii, dtype)
     hs, zs = [x], []
     h = x
     for w, b in lay[:-1]:
         z = h @ w.T + b
         zs.append(z)
-        h = _act(act, z).astype(np.float32)
+        h = _act(act, z).astype(dtype)
         hs.append(h)
     w, b = lay[-1]
-    s = (1.0 / (1.0 + np.exp(-(h @ w.T + b)[:, 0]))).astype(np.float32)
+    s = (1.0 / (1.0 + np.exp(-(h @ w.T + b)[:, 0]))).astype(dtype)
     return s, (x, hs, zs, s)
 
 

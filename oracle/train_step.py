@@ -1,6 +1,6 @@
 """CPU restatement of one GSpaRC training step (numpy, FP32).
 
-TEST / BASELINE INFRASTRUCTURE ONLY: timed by bench.py's cpu_baseline and
+TEST / CPU-BASELINE INFRASTRUCTURE ONLY: timed by bench.py's cpu_baseline and
 ``--impl reference`` legs as the CPU implementation of the path; never used by
 the product.
 

@@ -184,3 +184,53 @@ def test_shared_mlp_bf16_tensor_cores_match_bf16_emulation(layers, act, R):
         for a, b in ((gw, rw), (gb, rb)):
             assert (a - b).abs().max().item() <= 2e-3 * b.abs().max().item() + 1e-6
     assert (dmeans - ref_dm).abs().max().item() <= 2e-3 * ref_dm.abs().max().item()
+
+
+def test_bf16_and_fp32_renders_against_fp64_oracle():
+    """Error of the rendered spectra against the FP64 oracle render (oracle/
+    raster + oracle/shared_mlp in float64) for the 3x128 GELU model, FP32 and
+    BF16 tensor-core MLPs.  On pixels whose contributor count agrees with the
+    oracle's: FP32 within 1e-4 of the peak, BF16 within 2e-2 of the peak; the
+    SSIM of either render against the FP64 one is within 1e-3 of 1, and the
+    two differ by at most 1e-3.  The measured figures are printed."""
+    from fused_ssim import fused_ssim
+    from oracle import raster as oraster
+    from oracle import shared_mlp as osm
+    P, R = 4096, 2
+    sc = _scene(P, R, seed=9)
+    mlp32 = SharedMLP(3, 128, "gelu")
+    params = mlp32.init_params(seed=21)
+    outs = {}
+    for prec in ("fp32", "bf16"):
+        mlp = SharedMLP(3, 128, "gelu", precision=prec)
+        out_r, _, radii, st = raster.forward(sc["means"], None, sc["opac"], sc["scales"], sc["rots"], 90, 360, 1.0,
+                                             sc["views"], sc["tx"], sc["rxs"], shared=mlp, shared_params=params)
+        K, err = raster.read_status(st)
+        assert err == 0
+        outs[prec] = (out_r.cpu().numpy(), raster.state_views(st)["n_contrib"].cpu().numpy())
+    c = lambda a: a.detach().cpu().numpy().astype(np.float64)
+    pnp = params.cpu().numpy()
+    for r in range(R):
+        rx = c(sc["rxs"][r])
+
+        def signal_fn(radii):
+            s, _ = osm.forward(pnp, 3, 128, "gelu", c(sc["means"]), rx, radii, dtype=np.float64)
+            return np.stack([s * (radii > 0), np.zeros_like(s)], 1)
+
+        ref = oraster.render(c(sc["means"]), c(sc["scales"]), c(sc["rots"]), c(sc["opac"]), None,
+                             c(sc["views"][r]), c(sc["tx"]), rx, 90, 360, dtype=np.float64, signal_fn=signal_fn)
+        o64, nc64 = ref["out"][0], ref["n_contrib"]
+        peak = np.abs(o64).max()
+        errs = {}
+        for prec, (o, nc) in outs.items():
+            same = nc[r] == nc64
+            assert same.mean() >= 0.99
+            errs[prec] = np.abs(o[r] - o64)[same].max() / peak
+        s32, s16 = [float(fused_ssim(torch.tensor(outs[p][0][r])[None, None].cuda(),
+                                     torch.tensor(o64, dtype=torch.float32)[None, None].cuda()))
+                    for p in ("fp32", "bf16")]
+        print(f"receiver {r}: max-abs error / peak vs FP64 oracle: fp32 {errs['fp32']:.3e}, bf16 {errs['bf16']:.3e}; "
+              f"SSIM vs FP64 render: fp32 {s32:.6f}, bf16 {s16:.6f}")
+        assert errs["fp32"] <= 1e-4
+        assert errs["bf16"] <= 2e-2
+        assert 1.0 - s32 <= 1e-3 and 1.0 - s16 <= 1e-3 and abs(s32 - s16) <= 1e-3

@@ -128,3 +128,28 @@ def test_fused_trainer_with_shared_mlp_graph_matches_eager_and_learns():
         losses.append(la)
     assert np.isfinite(losses).all() and losses[4] < losses[0] and losses[7] < losses[3]
     torch.testing.assert_close(a.params, b.params, rtol=1e-3, atol=1e-5)
+
+
+def test_tile_autotuner_times_every_shape_and_keeps_the_fastest():
+    """FusedTrainer.autotune_tile: one timing per tile shape, the fastest left
+    captured, parameters and optimizer state as before the trials; each
+    shape's graphed step reproduces its own eager step."""
+    from gsparc_b200.fused import FusedTrainer
+    from gsparc_b200.shared_mlp import SharedMLP
+    sc, views, rxs, tx, targets = _setup(P=3000, R=3)
+    tr = FusedTrainer(sc, shared=SharedMLP())
+    before = tr.params.clone()
+    times = tr.autotune_tile(tx, views, rxs, targets, steps=2)
+    assert set(times) == {(16, 16), (8, 32), (32, 8)}
+    assert all(t > 0 for t in times.values())
+    assert tr.tile == min(times, key=times.get) and tr.plan.tile == tr.tile
+    assert torch.equal(tr.params, before)
+    loss = float(tr.step(views, rxs, targets))
+    torch.cuda.synchronize()
+    tr.plan.check()
+    # the graph's first step equals the same eager step from the same state
+    ref = FusedTrainer(sc, shared=SharedMLP())
+    from gsparc_b200.autograd import RasterPlan
+    ref.plan = RasterPlan(ref.P, 3, 90, 360, tr.plan.capacity, torch.device("cuda"), tile=tr.tile)
+    eager = float(ref.step_eager(views, rxs, tx, targets))
+    assert abs(loss - eager) <= 1e-6 * abs(eager)
