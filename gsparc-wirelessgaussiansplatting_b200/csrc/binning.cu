@@ -284,7 +284,7 @@ scatter_kernel(int P, TileGrid grid, GeomView geo, uint32_t* __restrict__ cursor
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   for (int t = threadIdx.x; t < grid.T; t += blockDim.x) cnt[t] = 0;
   __syncthreads();
-  int x0 = 0, y0 = 0, x1 = 0, y1 = 0;
+  TileSpan span{0, 0, 0, 0, grid.gx, 0};
   bool vis = false;
   uint32_t rk = 0;
   if (g < P) {
@@ -293,10 +293,9 @@ scatter_kernel(int P, TileGrid grid, GeomView geo, uint32_t* __restrict__ cursor
     if (rad > 0) {
       vis = true;
       const float2 xy = geo.means2D[rg];
-      tile_rect(xy.x, xy.y, rad, grid, x0, y0, x1, y1);
+      span = tile_span(xy.x, xy.y, rad, grid);
       rk = geo.rank[rg];
-      for (int ty = y0; ty < y1; ++ty)
-        for (int tx = x0; tx < x1; ++tx) atomicAdd(&cnt[ty * grid.gx + tx], 1u);
+      for_each_tile(span, grid.gx, [&](int tile) { atomicAdd(&cnt[tile], 1u); });
     }
   }
   __syncthreads();
@@ -306,11 +305,10 @@ scatter_kernel(int P, TileGrid grid, GeomView geo, uint32_t* __restrict__ cursor
   }
   __syncthreads();
   if (vis) {
-    for (int ty = y0; ty < y1; ++ty)
-      for (int tx = x0; tx < x1; ++tx) {
-        const uint32_t pos = atomicAdd(&base[ty * grid.gx + tx], 1u);
-        seg_rank[pos] = rk;
-      }
+    for_each_tile(span, grid.gx, [&](int tile) {
+      const uint32_t pos = atomicAdd(&base[tile], 1u);
+      seg_rank[pos] = rk;
+    });
   }
 }
 

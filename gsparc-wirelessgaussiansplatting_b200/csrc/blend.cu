@@ -116,6 +116,10 @@ blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict
         pf_co[k] = geo.conic_opacity[roff + id];
         pf_sg[k] = geo.signal[roff + id];
         pf_bb[k] = geo.box[roff + id];
+        const float sh = wrap_shift(pf_xy[k].x, tile_x, grid);   // the copy across the seam, if nearer
+        pf_xy[k].x += sh;
+        pf_bb[k].x += sh;
+        pf_bb[k].y += sh;
       }
     }
   };
@@ -348,6 +352,10 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, int RT, unsigned grad_
         pf_co[q] = geo.conic_opacity[roff + id];
         pf_sg[q] = geo.signal[roff + id];
         pf_bb[q] = geo.box[roff + id];
+        const float sh = wrap_shift(pf_xy[q].x, tile_x, grid);   // as the forward: the nearer copy
+        pf_xy[q].x += sh;
+        pf_bb[q].x += sh;
+        pf_bb[q].y += sh;
       }
     }
   };

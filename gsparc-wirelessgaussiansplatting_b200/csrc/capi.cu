@@ -108,7 +108,7 @@ int report_cuda(cudaError_t e, const char* where) { return cuda_fail(e, where); 
 
 extern "C" {
 
-int gsparc_abi_version(void) { return 3; }
+int gsparc_abi_version(void) { return 4; }
 
 const char* gsparc_status_string(int status) {
   switch (status) {
@@ -169,7 +169,8 @@ int gsparc_binning_state_layout(long long capacity, size_t* o) {
   return GSPARC_OK;
 }
 
-int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w, float scale_modifier,
+int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w, unsigned int flags,
+                             float scale_modifier,
                              const float* means3D, const float* emission_mlps, const float* opacities,
                              const float* scales, const float* rotations, const float* viewmatrices,
                              const float* tx_pos, const float* rx_pos, int* radii_out, void* geom_state,
@@ -182,7 +183,8 @@ int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w,
   if (P > 0 && (!geom_state || !means3D || !opacities || !scales || !rotations))
     return invalid("null Gaussian pointer");
   cudaStream_t s = (cudaStream_t)stream;
-  TileGrid grid(H, W, tile_h, tile_w);
+  if (flags & ~GSPARC_FLAG_WRAP_AZIMUTH) return invalid("unknown flags");
+  TileGrid grid(H, W, tile_h, tile_w, (flags & GSPARC_FLAG_WRAP_AZIMUTH) ? 1 : 0);
   GeomView geo{};
   if (geom_state) carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
   ImageView img;
@@ -211,7 +213,8 @@ int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w,
   return GSPARC_OK;
 }
 
-int gsparc_rasterize_render(int P, int R, int H, int W, int tile_h, int tile_w, const void* geom_state,
+int gsparc_rasterize_render(int P, int R, int H, int W, int tile_h, int tile_w, unsigned int flags,
+                            const void* geom_state,
                             void* image_state, void* binning_state, long long capacity, float* out_real,
                             float* out_imag, void* stream) {
   if (P < 0 || R < 1 || H <= 0 || W <= 0 || capacity < 0) return invalid("sizes");
@@ -220,7 +223,8 @@ int gsparc_rasterize_render(int P, int R, int H, int W, int tile_h, int tile_w, 
   if (capacity > 0 && !binning_state) return invalid("null binning state");
   if (P > 0 && !geom_state) return invalid("null geometry state");
   cudaStream_t s = (cudaStream_t)stream;
-  TileGrid grid(H, W, tile_h, tile_w);
+  if (flags & ~GSPARC_FLAG_WRAP_AZIMUTH) return invalid("unknown flags");
+  TileGrid grid(H, W, tile_h, tile_w, (flags & GSPARC_FLAG_WRAP_AZIMUTH) ? 1 : 0);
   GeomView geo{};
   if (geom_state) carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
   ImageView img;
@@ -262,7 +266,8 @@ int gsparc_read_status(const void* image_state, long long* num_rendered, unsigne
   return GSPARC_OK;
 }
 
-int gsparc_rasterize_backward(int P, int R, int H, int W, int tile_h, int tile_w, float scale_modifier,
+int gsparc_rasterize_backward(int P, int R, int H, int W, int tile_h, int tile_w, unsigned int flags,
+                              float scale_modifier,
                               unsigned int grad_mode, const float* means3D, const float* emission_mlps,
                               const float* scales, const float* rotations, const float* viewmatrices,
                               const float* tx_pos, const float* rx_pos, const void* geom_state,
@@ -284,7 +289,8 @@ int gsparc_rasterize_backward(int P, int R, int H, int W, int tile_h, int tile_w
     return invalid("emission_mlps and dL_demission_mlps: give both (per-Gaussian MLP) or neither (shared MLP)");
   if (binning_capacity > 0 && !binning_state) return invalid("null binning state");
   cudaStream_t s = (cudaStream_t)stream;
-  TileGrid grid(H, W, tile_h, tile_w);
+  if (flags & ~GSPARC_FLAG_WRAP_AZIMUTH) return invalid("unknown flags");
+  TileGrid grid(H, W, tile_h, tile_w, (flags & GSPARC_FLAG_WRAP_AZIMUTH) ? 1 : 0);
   GeomView geo;
   carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
   ImageView img;

@@ -48,10 +48,14 @@ static_assert(sizeof(ImageHeader) == 256, "header is one 256-byte block");
 
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Tile grid of an H x W spectrum.  `wrap` (GSPARC_FLAG_WRAP_AZIMUTH): pixel
+// columns x and x +- W are the same azimuth, so footprints continue across the
+// 0/2pi seam; off, footprints are clamped at the image edges as the reference
+// does (auxiliary.h:14-24).
 struct TileGrid {
-  int tile_h, tile_w, gx, gy, T;
-  __host__ __device__ TileGrid(int H, int W, int th, int tw)
-      : tile_h(th), tile_w(tw), gx((W + tw - 1) / tw), gy((H + th - 1) / th), T(gx * gy) {}
+  int tile_h, tile_w, gx, gy, T, W, wrap;
+  __host__ __device__ TileGrid(int H, int W_, int th, int tw, int wrap_ = 0)
+      : tile_h(th), tile_w(tw), gx((W_ + tw - 1) / tw), gy((H + th - 1) / th), T(gx * gy), W(W_), wrap(wrap_) {}
 };
 
 // Per-receiver depth order (binning.cu): an LSD radix sort of one 32-bit key
@@ -316,6 +320,51 @@ __device__ __forceinline__ void tile_rect(float px, float py, int radius, const 
   y0 = min(g.gy, max(0, (int)((py - radius) / by)));
   x1 = min(g.gx, max(0, (int)((px + radius + bx - 1) / bx)));
   y1 = min(g.gy, max(0, (int)((py + radius + by - 1) / by)));
+}
+
+// Tile columns a footprint covers: the clamped rectangle [x0, x1) x [y0, y1)
+// above and, with the azimuth wrap, the columns of the part beyond the left
+// edge, [xl, gx), and beyond the right edge, [0, xr) (xl = gx / xr = 0 when
+// there is none; they never overlap [x0, x1)).  The wrapped edges use the
+// rectangle's own rounding: xl = (int)(((px - r) + W) / bx),
+// xr = (int)((((px + r) - W) + bx) - 1) / bx).
+struct TileSpan {
+  int x0, y0, x1, y1, xl, xr;
+};
+__device__ __forceinline__ TileSpan tile_span(float px, float py, int radius, const TileGrid& g) {
+  TileSpan s;
+  tile_rect(px, py, radius, g, s.x0, s.y0, s.x1, s.y1);
+  s.xl = g.gx;
+  s.xr = 0;
+  if (g.wrap) {
+    const float bx = (float)g.tile_w, Wf = (float)g.W, rf = (float)radius;
+    const float ql = (px - rf) + Wf;
+    if (px - rf < 0.0f) s.xl = max(s.x1, min(g.gx, max(0, (int)(ql / bx))));
+    const float qr = (px + rf) - Wf;
+    if (qr > 0.0f) s.xr = min(s.x0, max(0, (int)(((qr + bx) - 1.0f) / bx)));
+  }
+  return s;
+}
+__device__ __forceinline__ int span_tiles(const TileSpan& s, int gx) {
+  return ((s.x1 - s.x0) + (gx - s.xl) + s.xr) * (s.y1 - s.y0);
+}
+template <class F>
+__device__ __forceinline__ void for_each_tile(const TileSpan& s, int gx, F&& f) {
+  for (int ty = s.y0; ty < s.y1; ++ty) {
+    for (int tx = s.x0; tx < s.x1; ++tx) f(ty * gx + tx);
+    for (int tx = s.xl; tx < gx; ++tx) f(ty * gx + tx);
+    for (int tx = 0; tx < s.xr; ++tx) f(ty * gx + tx);
+  }
+}
+// With the azimuth wrap, the copy of a Gaussian (x of its mean) nearest to
+// tile column tx: shifted by -W or +W when it lies more than W/2 from the
+// tile's centre; 0 otherwise (and always 0 without the wrap).
+__device__ __forceinline__ float wrap_shift(float x, int tx, const TileGrid& g) {
+  if (!g.wrap) return 0.0f;
+  const float half = 0.5f * (float)g.W;
+  const float cx = (float)(tx * g.tile_w) + 0.5f * (float)g.tile_w;
+  const float d = x - cx;
+  return d > half ? -(float)g.W : (d < -half ? (float)g.W : 0.0f);
 }
 
 // small column-major 3x3 matrix with GLM's element convention: c[col][row]

@@ -127,6 +127,7 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
 
   bool vis = false;
   int x0 = 0, y0 = 0, x1 = 0, y1 = 0;
+  TileSpan span{0, 0, 0, 0, grid.gx, 0};
   const size_t rg = (size_t)r * P + g;
   float3 p = make_float3(0.f, 0.f, 0.f);
   if (g < P) {
@@ -183,7 +184,8 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
         const float px = ndc_to_pixel(ndc_x, W);
         const float py = ndc_to_pixel(ndc_y, H);
         radius_i = (int)my_radius;
-        tile_rect(px, py, radius_i, grid, x0, y0, x1, y1);
+        span = tile_span(px, py, radius_i, grid);
+        x0 = span.x0; y0 = span.y0; x1 = span.x1; y1 = span.y1;
         // radius_i > 0 keeps the histogram consistent with the scatter, which
         // keys on radii > 0, even for non-finite inputs (ceil(NaN) -> 0)
         if (radius_i > 0 && (x1 - x0) * (y1 - y0) != 0) {
@@ -217,12 +219,10 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
   }
 
   if (vis) {
-    for (int ty = y0; ty < y1; ++ty)
-      for (int tx = x0; tx < x1; ++tx) {
-        const int tile = ty * grid.gx + tx;
-        if (kSharedHist) atomicAdd(&hist[tile], 1u);
-        else atomicAdd(&counts[(size_t)r * grid.T + tile], 1u);
-      }
+    for_each_tile(span, grid.gx, [&](int tile) {
+      if (kSharedHist) atomicAdd(&hist[tile], 1u);
+      else atomicAdd(&counts[(size_t)r * grid.T + tile], 1u);
+    });
   }
   __syncthreads();
   if (kSharedHist) {

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libgsparc_b200.so")
 
 GRAD_REFERENCE = 0
 GRAD_EXACT = 1
+FLAG_WRAP_AZIMUTH = 1   # GSPARC_FLAG_WRAP_AZIMUTH
 
 _c_int, _c_ll, _c_size, _c_float, _c_uint = ctypes.c_int, ctypes.c_longlong, ctypes.c_size_t, ctypes.c_float, ctypes.c_uint
 _vp = ctypes.c_void_p
@@ -39,13 +40,14 @@ _SIGS = {
     "gsparc_geom_state_layout": (_c_int, [_c_int, _c_int, ctypes.POINTER(_c_size)]),
     "gsparc_image_state_layout": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, ctypes.POINTER(_c_size)]),
     "gsparc_binning_state_layout": (_c_int, [_c_ll, ctypes.POINTER(_c_size)]),
-    "gsparc_rasterize_prepare": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_float,
+    "gsparc_rasterize_prepare": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_uint, _c_float,
                                           _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                           ctypes.POINTER(_c_ll), _vp]),
-    "gsparc_rasterize_render": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
+    "gsparc_rasterize_render": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_uint,
                                          _vp, _vp, _vp, _c_ll, _vp, _vp, _vp]),
     "gsparc_read_status": (_c_int, [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_uint), _vp]),
-    "gsparc_rasterize_backward": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_float, _c_uint,
+    "gsparc_rasterize_backward": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_uint, _c_float,
+                                           _c_uint,
                                            _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_ll,
                                            _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gsparc_mark_visible": (_c_int, [_c_int, _vp, _vp, _vp, _vp]),

@@ -18,11 +18,13 @@ from . import _lib, raster
 
 class RasterPlan:
     """Static buffers of a fixed-shape render: P Gaussians, R receivers,
-    H x W spectra, tile shape, binning capacity and gradient mode."""
+    H x W spectra, tile shape, binning capacity, gradient mode and the
+    azimuth seam wrap."""
 
-    def __init__(self, P, R, H, W, capacity, device, tile=(16, 16), grad_mode="reference"):
+    def __init__(self, P, R, H, W, capacity, device, tile=(16, 16), grad_mode="reference", wrap=False):
         self.P, self.R, self.H, self.W = int(P), int(R), int(H), int(W)
         self.tile = tuple(tile)
+        self.wrap = bool(wrap)   # azimuth seam wrap (GSPARC_FLAG_WRAP_AZIMUTH)
         self.capacity = int(capacity)
         self.grad_mode = grad_mode
         dev = torch.device(device)
@@ -60,7 +62,7 @@ class RasterizeFunction(torch.autograd.Function):
     def forward(ctx, means3D, mlp, opacities, scales, rotations, views, rxs, tx, plan):
         out_r, out_i, radii, st = raster.forward(
             means3D, mlp, opacities, scales, rotations, plan.H, plan.W, 1.0, views, tx, rxs, tile=plan.tile,
-            capacity=plan.capacity, binning=plan.binning, geom=plan.geom, image=plan.image)
+            capacity=plan.capacity, binning=plan.binning, geom=plan.geom, image=plan.image, wrap=plan.wrap)
         plan.record_status()
         ctx.plan, ctx.st = plan, st
         ctx.save_for_backward(means3D, mlp, scales, rotations, views, rxs, tx)

@@ -57,12 +57,15 @@ class FusedTrainer:
 
     def __init__(self, scene: scenes.Scene, H=scenes.H, W=scenes.W, device="cuda", group=None, seed=0,
                  grad_mode="reference", lr=LR, betas=(0.9, 0.999), eps=1e-15, conf_hidden=CONF_HIDDEN,
-                 shared=None):
+                 shared=None, wrap=False):
         """``shared``: a ``SharedMLP`` to use the benchmark's shared emission
         MLP (initialised from ``seed``) instead of the scene's per-Gaussian
-        3-32-2 MLPs."""
+        3-32-2 MLPs.  ``wrap``: continue footprints across the 0/2pi azimuth
+        seam (the reference clamps them at the image edges)."""
         self.H, self.W, self.device, self.group = H, W, torch.device(device), group
         self.grad_mode = grad_mode
+        self.wrap = bool(wrap)
+        self.tile = (16, 16)
         self.betas, self.eps = betas, eps
         self.conf_hidden = int(conf_hidden)
         self.n_conf = conf_floats(self.conf_hidden)
@@ -146,6 +149,7 @@ class FusedTrainer:
         out_r, _, _, st = raster.forward(
             self.centre, self._mlp_arg(), self.act_opac, self.act_scales, self.act_rots, self.H, self.W, 1.0, views, tx,
             rxs, tile=plan.tile, capacity=plan.capacity, binning=plan.binning, geom=plan.geom, image=plan.image,
+            wrap=plan.wrap,
             out_real=self._out_r, out_imag=self._out_i, radii=self._radii, **self._shared_kw())
         plan.record_status()
         loss, dpred = self._lossfn(out_r, targets, rxs, self.conf_params, self.conf_grads)
@@ -188,7 +192,7 @@ class FusedTrainer:
             for r in range(views.shape[0]):
                 _, _, _, st = raster.forward(self.centre, self._mlp_arg(), self.act_opac, self.act_scales,
                                              self.act_rots, self.H, self.W, 1.0, views[r], tx, rxs[r], tile=tile,
-                                             **self._shared_kw())
+                                             wrap=self.wrap, **self._shared_kw())
                 kmax = max(kmax, st.num_rendered)
         return int(kmax * margin) + slack
 
@@ -203,7 +207,8 @@ class FusedTrainer:
         dev = self.device
         self.graph = None
         self.tile = tuple(tile)
-        self.plan = RasterPlan(self.P, R, self.H, self.W, capacity, dev, tile=tile, grad_mode=self.grad_mode)
+        self.plan = RasterPlan(self.P, R, self.H, self.W, capacity, dev, tile=tile, grad_mode=self.grad_mode,
+                               wrap=self.wrap)
         self._buffers(R)
         self._s_views = torch.eye(4, device=dev).repeat(R, 1, 1).contiguous()
         self._s_rxs = torch.zeros((R, 3), device=dev)

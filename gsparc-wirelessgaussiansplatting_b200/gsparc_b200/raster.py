@@ -73,6 +73,7 @@ class ForwardState:
     geom: torch.Tensor
     image: torch.Tensor
     binning: torch.Tensor
+    flags: int = 0
 
 
 def _receivers(viewmatrices, rx_pos, device):
@@ -91,7 +92,8 @@ def _receivers(viewmatrices, rx_pos, device):
 
 def forward(means3D, emission_mlps, opacities, scales, rotations, H, W, scale_modifier,
             viewmatrices, tx_pos, rx_pos, tile=None, capacity=None, binning=None,
-            out_real=None, out_imag=None, radii=None, geom=None, image=None, shared=None, shared_params=None):
+            out_real=None, out_imag=None, radii=None, geom=None, image=None, shared=None, shared_params=None,
+            wrap=False):
     """Render R spectra.  Returns (out_real [R,H,W], out_imag [R,H,W], radii [R,P] int32, ForwardState).
 
     With ``capacity=None`` the instance count K is read back (one host sync,
@@ -100,7 +102,9 @@ def forward(means3D, emission_mlps, opacities, scales, rotations, H, W, scale_mo
     reported by ``read_status``.  Preallocated arenas/outputs may be passed.
     With ``shared`` (a ``SharedMLP``) and its flat ``shared_params`` the
     signals come from the shared emission MLP and ``emission_mlps`` must be
-    None."""
+    None.  ``wrap=True`` continues footprints across the 0/2pi azimuth seam
+    (GSPARC_FLAG_WRAP_AZIMUTH); the default clamps them at the image edges as
+    the reference does."""
     if means3D.dim() != 2 or means3D.shape[1] != 3:
         raise RuntimeError("means3D must have dimensions (num_points, 3)")
     device = means3D.device
@@ -146,8 +150,9 @@ def forward(means3D, emission_mlps, opacities, scales, rotations, H, W, scale_mo
         image = torch.empty(_lib.image_state_bytes(R, H, W, *tile), dtype=torch.uint8, device=device)
     stream = stream_of(device)
     K = ctypes.c_longlong(0)
+    flags = _lib.FLAG_WRAP_AZIMUTH if wrap else 0
     check("rasterize_prepare", L.gsparc_rasterize_prepare(
-        P, R, H, W, tile[0], tile[1], float(scale_modifier), ptr(m), ptr(mlp), ptr(op), ptr(sc), ptr(rot),
+        P, R, H, W, tile[0], tile[1], flags, float(scale_modifier), ptr(m), ptr(mlp), ptr(op), ptr(sc), ptr(rot),
         ptr(v), ptr(tx), ptr(rx), ptr(radii), ptr(geom), ptr(image),
         ctypes.byref(K) if capacity is None else None, stream))
     if shared is not None:
@@ -160,9 +165,9 @@ def forward(means3D, emission_mlps, opacities, scales, rotations, H, W, scale_mo
     if binning is None:
         binning = torch.empty(max(_lib.binning_state_bytes(capacity), 1), dtype=torch.uint8, device=device)
     check("rasterize_render", L.gsparc_rasterize_render(
-        P, R, H, W, tile[0], tile[1], ptr(geom), ptr(image), ptr(binning), int(capacity),
+        P, R, H, W, tile[0], tile[1], flags, ptr(geom), ptr(image), ptr(binning), int(capacity),
         ptr(out_real), ptr(out_imag), stream))
-    st = ForwardState(P, R, H, W, tile, int(capacity), num_rendered, geom, image, binning)
+    st = ForwardState(P, R, H, W, tile, int(capacity), num_rendered, geom, image, binning, flags)
     return out_real, out_imag, radii, st
 
 
@@ -208,7 +213,7 @@ def backward(st: ForwardState, means3D, emission_mlps, scales, rotations, scale_
     rot = _dev_f32(rotations, "rotations", device).reshape(P, 4)
     L = _lib.lib()
     check("rasterize_backward", L.gsparc_rasterize_backward(
-        P, R, H, W, st.tile[0], st.tile[1], float(scale_modifier), int(mode),
+        P, R, H, W, st.tile[0], st.tile[1], st.flags, float(scale_modifier), int(mode),
         ptr(m), ptr(mlp), ptr(sc), ptr(rot), ptr(v), ptr(tx), ptr(rx),
         ptr(st.geom), ptr(st.image), ptr(st.binning), int(st.capacity), ptr(g_r), ptr(g_i),
         ptr(out["dmeans2D"]), ptr(out["dconic"]), ptr(out["dsignal"]), ptr(out["dopacity"]),

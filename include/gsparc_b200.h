@@ -46,6 +46,18 @@ typedef enum gsparc_status {
                                     gradient (backward.cu:577,587) */
 #define GSPARC_GRAD_EXACT 1u     /* true derivative of the forward */
 
+/* `flags` of gsparc_rasterize_prepare / _render / _backward (pass the same
+ * value to all three for one forward).  0: footprints are clamped at the
+ * image's left and right edges, as the reference's getRect does
+ * (auxiliary.h:14-24) -- bit-exact parity.  GSPARC_FLAG_WRAP_AZIMUTH: pixel
+ * columns x and x +- W are the same azimuth, so a footprint that crosses the
+ * 0/2pi seam also covers the tiles on the other side (the columns beyond the
+ * left edge: [(int)(((px - r) + W) / tile_w), gx); beyond the right edge:
+ * [0, (int)((((px + r) - W) + tile_w) - 1) / tile_w)), and every tile blends
+ * the copy of a Gaussian (mean x or x -+ W) nearest to its centre column.
+ * Footprints that do not cross the seam give the same result either way. */
+#define GSPARC_FLAG_WRAP_AZIMUTH 1u
+
 /* Version of this ABI (bumped on any signature change). */
 GSPARC_API int gsparc_abi_version(void);
 
@@ -101,7 +113,7 @@ GSPARC_API int gsparc_binning_state_layout(long long capacity, size_t* offsets3)
  * synchronised (the reference's blocking readback, rasterizer_impl.cu:274);
  * pass NULL to stay asynchronous (CUDA-graph capture). */
 GSPARC_API int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w,
-                             float scale_modifier, const float* means3D,
+                             unsigned int flags, float scale_modifier, const float* means3D,
                              const float* emission_mlps, const float* opacities,
                              const float* scales, const float* rotations,
                              const float* viewmatrices, const float* tx_pos,
@@ -118,7 +130,7 @@ GSPARC_API int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, 
  * If K exceeds `capacity` the device error word gets the capacity bit and the
  * outputs are left unwritten; gsparc_read_status reports it. */
 GSPARC_API int gsparc_rasterize_render(int P, int R, int H, int W, int tile_h, int tile_w,
-                            const void* geom_state, void* image_state, void* binning_state,
+                            unsigned int flags, const void* geom_state, void* image_state, void* binning_state,
                             long long capacity, float* out_real, float* out_imag,
                             void* stream);
 
@@ -145,7 +157,7 @@ GSPARC_API int gsparc_read_status(const void* image_state, long long* num_render
  *   dL_demission_mlps [194*P].
  * grad_mode is GSPARC_GRAD_REFERENCE or GSPARC_GRAD_EXACT. */
 GSPARC_API int gsparc_rasterize_backward(int P, int R, int H, int W, int tile_h, int tile_w,
-                              float scale_modifier, unsigned int grad_mode,
+                              unsigned int flags, float scale_modifier, unsigned int grad_mode,
                               const float* means3D, const float* emission_mlps,
                               const float* scales, const float* rotations,
                               const float* viewmatrices, const float* tx_pos,

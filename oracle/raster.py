@@ -185,6 +185,41 @@ def get_rect(px, py, radius, grid_x, grid_y, tile_h, tile_w, dt):
     return clampi(x0, grid_x), clampi(y0, grid_y), clampi(x1, grid_x), clampi(y1, grid_y)
 
 
+def get_span(px, py, radius, grid_x, grid_y, tile_h, tile_w, W, dt, wrap):
+    """Tile columns of a footprint: get_rect's clamped rectangle plus, with the
+    azimuth seam wrap (this implementation's GSPARC_FLAG_WRAP_AZIMUTH; the
+    reference has none), the columns beyond the left edge [xl, gx) and beyond
+    the right edge [0, xr), with the rectangle's own rounding:
+    xl = trunc(((px - r) + W) / bx), xr = trunc((((px + r) - W) + bx - 1) / bx),
+    clamped so they never overlap [x0, x1)."""
+    x0, y0, x1, y1 = get_rect(px, py, radius, grid_x, grid_y, tile_h, tile_w, dt)
+    xl = np.full_like(x0, grid_x)
+    xr = np.zeros_like(x0)
+    if wrap:
+        rad = radius.astype(dt)
+        bx, Wf, one = _c(dt, tile_w), _c(dt, W), _c(dt, 1)
+        with np.errstate(invalid="ignore"):
+            left = (px - rad) < 0
+            ql = np.trunc(((px - rad) + Wf) / bx)
+            qr = (px + rad) - Wf
+            right = qr > 0
+            qrt = np.trunc(((qr + bx) - one) / bx)
+        ql = np.clip(np.where(np.isfinite(ql), ql, 0.0), 0, grid_x).astype(np.int64)
+        qrt = np.clip(np.where(np.isfinite(qrt), qrt, 0.0), 0, grid_x).astype(np.int64)
+        xl = np.where(left, np.maximum(x1, ql), grid_x)
+        xr = np.where(right, np.minimum(x0, qrt), 0)
+    return x0, y0, x1, y1, xl, xr
+
+
+def wrap_shift(x, tx, tile_w, W, dt):
+    """With the seam wrap, the shift (-W, +W or 0) that moves a mean's x to its
+    copy nearest tile column tx's centre (more than W/2 away: the other copy)."""
+    half = _c(dt, 0.5) * _c(dt, W)
+    cx = _c(dt, tx * tile_w) + _c(dt, 0.5) * _c(dt, tile_w)
+    d = x - cx
+    return np.where(d > half, -_c(dt, W), np.where(d < -half, _c(dt, W), _c(dt, 0)))
+
+
 def preprocess(means, scales, rots, opac, mlp, view, tx, rx, H, W,
                mod=1.0, tile_h=16, tile_w=16, dtype=np.float32):
     """preprocessCUDA (forward.cu:252-327) for one receiver.
@@ -272,7 +307,7 @@ def emission_forward(means, mlp, tx, rx, dt):
     return _c(dt, 1) / (_c(dt, 1) + np.exp(-att))
 
 
-def bin_and_sort(means2D, depth, radii, H, W, tile_h=16, tile_w=16):
+def bin_and_sort(means2D, depth, radii, H, W, tile_h=16, tile_w=16, wrap=False):
     """duplicateWithKeys + stable radix sort + identifyTileRanges
     (rasterizer_impl.cu:102-171, :270-310).
 
@@ -288,13 +323,14 @@ def bin_and_sort(means2D, depth, radii, H, W, tile_h=16, tile_w=16):
     gy = (H + tile_h - 1) // tile_h
     ntiles = gx * gy
     P = radii.shape[0]
-    x0, y0, x1, y1 = get_rect(means2D[:, 0], means2D[:, 1], radii.astype(np.int64), gx, gy,
-                              tile_h, tile_w, np.dtype(np.float32))
+    x0, y0, x1, y1, xl, xr = get_span(means2D[:, 0], means2D[:, 1], radii.astype(np.int64), gx, gy,
+                                      tile_h, tile_w, W, np.dtype(np.float32), wrap)
     dbits = depth.view(np.uint32).astype(np.uint64)
     keys, vals = [], []
     for g in np.nonzero(radii > 0)[0]:
+        cols = list(range(x0[g], x1[g])) + list(range(xl[g], gx)) + list(range(0, xr[g]))
         for ty in range(y0[g], y1[g]):
-            for tx in range(x0[g], x1[g]):
+            for tx in cols:
                 keys.append((np.uint64(ty * gx + tx) << np.uint64(32)) | dbits[g])
                 vals.append(g)
     keys = np.array(keys, dtype=np.uint64)
@@ -321,7 +357,7 @@ def _tile_pixels(tile, gx, H, W, tile_h, tile_w):
 
 
 def blend_forward(ranges, point_list, means2D, conic_opacity, signal, H, W,
-                  tile_h=16, tile_w=16, dtype=np.float32, record=False):
+                  tile_h=16, tile_w=16, dtype=np.float32, record=False, wrap=False):
     """renderCUDA forward (forward.cu:151-249): per pixel, walk the tile's
     sorted list front to back; skip power>0 and alpha<1/255; stop before the
     first Gaussian that would take T below 1e-4.
@@ -346,6 +382,7 @@ def blend_forward(ranges, point_list, means2D, conic_opacity, signal, H, W,
         if yy.size == 0:
             continue
         pxf, pyf = xx.astype(dt), yy.astype(dt)
+        tcol = tile % gx
         T = np.ones(yy.size, dtype=dt)
         Cr = np.zeros(yy.size, dtype=dt)
         Ci = np.zeros(yy.size, dtype=dt)
@@ -358,7 +395,8 @@ def blend_forward(ranges, point_list, means2D, conic_opacity, signal, H, W,
                 if done.all():
                     break
                 g = int(point_list[j])
-                dx = xy[g, 0] - pxf
+                xg = xy[g, 0] + wrap_shift(xy[g, 0], tcol, tile_w, W, dt) if wrap else xy[g, 0]
+                dx = xg - pxf
                 dy = xy[g, 1] - pyf
                 c = co[g]
                 power = _c(dt, -0.5) * (c[0] * dx * dx + c[2] * dy * dy) - c[1] * dx * dy
@@ -389,7 +427,7 @@ def blend_forward(ranges, point_list, means2D, conic_opacity, signal, H, W,
 
 
 def blend_backward(ranges, point_list, means2D, conic_opacity, signal, final_T, n_contrib,
-                   dL_dout, H, W, tile_h=16, tile_w=16, dtype=np.float32, ref_compat=True):
+                   dL_dout, H, W, tile_h=16, tile_w=16, dtype=np.float32, ref_compat=True, wrap=False):
     """renderCUDA backward (backward.cu:442-616): reverse walk recomputing T
     from the saved final T by division.
 
@@ -420,6 +458,7 @@ def blend_backward(ranges, point_list, means2D, conic_opacity, signal, final_T, 
         if yy.size == 0 or e <= s:
             continue
         pxf, pyf = xx.astype(dt), yy.astype(dt)
+        tcol = tile % gx
         T = final_T[yy, xx].astype(dt)
         last_c = n_contrib[yy, xx].astype(np.int64)
         gr = dL_dout[0, yy, xx].astype(dt)
@@ -436,7 +475,8 @@ def blend_backward(ranges, point_list, means2D, conic_opacity, signal, final_T, 
                 if not act.any():
                     continue
                 g = int(point_list[j])
-                dx = xy[g, 0] - pxf
+                xg = xy[g, 0] + wrap_shift(xy[g, 0], tcol, tile_w, W, dt) if wrap else xy[g, 0]
+                dx = xg - pxf
                 dy = xy[g, 1] - pyf
                 c = co[g]
                 power = _c(dt, -0.5) * (c[0] * dx * dx + c[2] * dy * dy) - c[1] * dx * dy
@@ -655,20 +695,21 @@ def mark_visible(means, view):
 
 
 def render(means, scales, rots, opac, mlp, view, tx, rx, H, W, mod=1.0,
-           tile_h=16, tile_w=16, dtype=np.float32, signal_fn=None):
+           tile_h=16, tile_w=16, dtype=np.float32, signal_fn=None, wrap=False):
     """Whole forward for one receiver: preprocess -> bin/sort -> blend.
     ``signal_fn(radii) -> [P,2]`` replaces the per-Gaussian MLP's signals
-    (the shared emission MLP); ``mlp`` may then be None."""
+    (the shared emission MLP); ``mlp`` may then be None.  ``wrap``: the
+    azimuth seam wrap (get_span / wrap_shift)."""
     if mlp is None:
         mlp = np.zeros(194 * means.shape[0], np.float32)
     pre = preprocess(means, scales, rots, opac, mlp, view, tx, rx, H, W, mod, tile_h, tile_w, dtype)
     if signal_fn is not None:
         pre["signal"] = signal_fn(pre["radii"]).astype(pre["signal"].dtype)
     keys, vals, ranges = bin_and_sort(pre["means2D"].astype(np.float32), pre["depth"].astype(np.float32),
-                                      pre["radii"], H, W, tile_h, tile_w)
+                                      pre["radii"], H, W, tile_h, tile_w, wrap)
     out, fT, nc = blend_forward(ranges, vals, pre["means2D"], pre["conic_opacity"], pre["signal"],
-                                H, W, tile_h, tile_w, dtype)
-    return dict(pre=pre, keys=keys, values=vals, ranges=ranges, out=out, final_T=fT, n_contrib=nc)
+                                H, W, tile_h, tile_w, dtype, wrap=wrap)
+    return dict(pre=pre, keys=keys, values=vals, ranges=ranges, out=out, final_T=fT, n_contrib=nc, wrap=wrap)
 
 
 def render_backward(fwd, means, scales, rots, opac, mlp, view, tx, rx, dL_dout, H, W, mod=1.0,
@@ -679,7 +720,8 @@ def render_backward(fwd, means, scales, rots, opac, mlp, view, tx, rx, dL_dout, 
     pre = fwd["pre"]
     dmean2, dconic, dopac, dsig = blend_backward(
         fwd["ranges"], fwd["values"], pre["means2D"], pre["conic_opacity"], pre["signal"],
-        fwd["final_T"], fwd["n_contrib"], dL_dout, H, W, tile_h, tile_w, dtype, ref_compat)
+        fwd["final_T"], fwd["n_contrib"], dL_dout, H, W, tile_h, tile_w, dtype, ref_compat,
+        wrap=fwd.get("wrap", False))
     dmean3_geo, dcov, dscale, drot = geometry_backward(
         means, scales, rots, view, pre["radii"], pre["cov3D"], dmean2, dconic, H, W, mod, dtype, ref_compat)
     if mlp is None:   # shared emission MLP: its adjoint is the caller's (dL_dsignal)

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     L = _lib.lib()
-    assert L.gsparc_abi_version() == 3
+    assert L.gsparc_abi_version() == 4
     for code, text in [(0, b"ok"), (1, b"invalid argument"), (2, b"CUDA error"), (3, b"binning capacity exceeded")]:
         assert L.gsparc_status_string(code) == text
 
@@ -53,14 +53,15 @@ def test_arena_sizes_and_layouts():
 
 
 def _call_prepare(**kw):
-    a = dict(P=10, R=1, H=90, W=360, th=16, tw=16, mod=1.0)
+    a = dict(P=10, R=1, H=90, W=360, th=16, tw=16, flags=0, mod=1.0)
     a.update(kw)
     dummy = ctypes.c_void_p(16)   # never dereferenced: validation fails first
-    return _lib.lib().gsparc_rasterize_prepare(a["P"], a["R"], a["H"], a["W"], a["th"], a["tw"], a["mod"],
-                                               *([dummy] * 11), None, None)
+    return _lib.lib().gsparc_rasterize_prepare(a["P"], a["R"], a["H"], a["W"], a["th"], a["tw"], a["flags"],
+                                               a["mod"], *([dummy] * 11), None, None)
 
 
-@pytest.mark.parametrize("kw", [dict(th=16, tw=8), dict(th=4, tw=64), dict(R=0), dict(H=0), dict(P=-1)])
+@pytest.mark.parametrize("kw", [dict(th=16, tw=8), dict(th=4, tw=64), dict(R=0), dict(H=0), dict(P=-1),
+                                dict(flags=2), dict(flags=0x101)])
 def test_prepare_rejects_bad_arguments_without_cuda(kw):
     assert _call_prepare(**kw) == 1
     assert b"invalid argument" in _lib.lib().gsparc_last_error_detail()
@@ -69,14 +70,15 @@ def test_prepare_rejects_bad_arguments_without_cuda(kw):
 def test_prepare_rejects_null_state():
     L = _lib.lib()
     d = ctypes.c_void_p(16)
-    st = L.gsparc_rasterize_prepare(10, 1, 90, 360, 16, 16, 1.0, d, d, d, d, d, d, d, d, None, None, d, None, None)
+    st = L.gsparc_rasterize_prepare(10, 1, 90, 360, 16, 16, 0, 1.0, d, d, d, d, d, d, d, d, None, None, d, None,
+                                    None)
     assert st == 1
 
 
 def test_backward_rejects_bad_grad_mode():
     L = _lib.lib()
     d = ctypes.c_void_p(16)
-    st = L.gsparc_rasterize_backward(10, 1, 90, 360, 16, 16, 1.0, 7, *([d] * 10), 10, *([d] * 11), None)
+    st = L.gsparc_rasterize_backward(10, 1, 90, 360, 16, 16, 0, 1.0, 7, *([d] * 10), 10, *([d] * 11), None)
     assert st == 1
     assert b"grad_mode" in L.gsparc_last_error_detail()
 

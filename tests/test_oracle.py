@@ -241,3 +241,73 @@ def test_gelu_cdf_rational_approximation_error_bound():
     d = z * f(0.39894228040143268) * ez + ph
     assert np.max(np.abs(a - gelu) / np.maximum(1.0, np.abs(zd))) <= 4e-7
     assert np.max(np.abs(d - dgelu)) <= 4e-7
+
+
+def _seam_scene(P=240, seed=3):
+    """Gaussians around a receiver at the origin, many of them near the 0/2pi
+    azimuth seam (direction -z), with per-Gaussian signals independent of
+    position."""
+    rng = np.random.default_rng(seed)
+    d = rng.uniform(0.6, 2.5, P)
+    lon = np.where(rng.random(P) < 0.6, np.pi + rng.normal(0, 0.08, P), rng.uniform(-np.pi, np.pi, P))
+    lat = rng.uniform(-0.6, 0.6, P)
+    means = np.stack([d * np.cos(lat) * np.sin(lon), d * np.sin(lat), d * np.cos(lat) * np.cos(lon)], 1)
+    scales = np.exp(rng.normal(-2.6, 0.3, (P, 3)))
+    q = rng.normal(size=(P, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    opac = rng.uniform(0.5, 0.95, P)
+    sig = np.stack([rng.uniform(0.2, 1.0, P), np.zeros(P)], 1)
+    return means, scales, q, opac, sig
+
+
+def _quat_mul(a, b):
+    w1, x1, y1, z1 = a.T
+    w2, x2, y2, z2 = b.T
+    return np.stack([w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2, w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2,
+                     w1 * y2 - x1 * z2 + y1 * w2 + z1 * x2, w1 * z2 + x1 * y2 - y1 * x2 + z1 * w2], 1)
+
+
+def test_seam_wrap_makes_the_render_invariant_to_a_half_turn_in_azimuth():
+    """With the azimuth wrap the spectrum of a scene turned by pi about the
+    receiver's vertical axis is the original rolled by W/2 columns (W/2 a
+    whole number of tiles), in FP64; the clamped render (the reference's) is
+    not, because footprints stop at the seam.  Also: scenes whose footprints
+    all stay off the seam render identically with and without the wrap."""
+    from oracle import raster as R
+    H, W = 48, 352
+    means, scales, q, opac, sig = _seam_scene()
+    view = np.eye(4)
+    tx = np.array([0.0, 0.5, 3.0])
+    rx = np.zeros(3)
+    ry = np.array([[-1.0, 0, 0], [0, 1.0, 0], [0, 0, -1.0]])
+    means_t = means @ ry.T
+    q_y = np.tile(np.array([0.0, 0.0, 1.0, 0.0]), (len(q), 1))
+    q_t = _quat_mul(q_y, q)
+    cov, _, _, _ = R.cov3d(scales, q, 1.0, np.dtype(np.float64))
+    cov_t, _, _, _ = R.cov3d(scales, q_t, 1.0, np.dtype(np.float64))
+    m = lambda c: np.array([[c[0], c[1], c[2]], [c[1], c[3], c[4]], [c[2], c[4], c[5]]])
+    for i in range(5):   # the turned quaternion turns the covariance
+        assert np.allclose(m(cov_t[i]), ry @ m(cov[i]) @ ry.T, atol=1e-12)
+    fn = lambda radii: sig
+    outs = {}
+    for wrap in (False, True):
+        a = R.render(means, scales, q, opac, None, view, tx, rx, H, W, dtype=np.float64, signal_fn=fn, wrap=wrap)
+        b = R.render(means_t, scales, q_t, opac, None, view, tx, rx, H, W, dtype=np.float64, signal_fn=fn,
+                     wrap=wrap)
+        outs[wrap] = (a, b)
+    a, b = outs[True]
+    peak = np.abs(a["out"]).max()
+    assert peak > 0.1
+    assert np.abs(np.roll(a["out"][0], W // 2, axis=1) - b["out"][0]).max() <= 1e-9 * peak
+    assert np.array_equal(np.roll(a["n_contrib"], W // 2, axis=1), b["n_contrib"])
+    a0, b0 = outs[False]
+    assert np.abs(np.roll(a0["out"][0], W // 2, axis=1) - b0["out"][0]).max() > 1e-3 * peak
+    assert len(a["keys"]) > len(a0["keys"])   # the seam-crossing footprints gained tiles
+    # footprints away from the seam: identical
+    far = np.abs(np.arctan2(means[:, 0], means[:, 2])) < 2.0
+    fn2 = lambda radii: sig[far]
+    c0 = R.render(means[far], scales[far], q[far], opac[far], None, view, tx, rx, H, W, dtype=np.float32,
+                  signal_fn=fn2, wrap=False)
+    c1 = R.render(means[far], scales[far], q[far], opac[far], None, view, tx, rx, H, W, dtype=np.float32,
+                  signal_fn=fn2, wrap=True)
+    assert np.array_equal(c0["keys"], c1["keys"]) and np.array_equal(c0["out"], c1["out"])
