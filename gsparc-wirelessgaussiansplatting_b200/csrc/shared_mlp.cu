@@ -275,21 +275,71 @@ struct FusedParams {
   static constexpr int kPadded = (kCount + 3) / 4 * 4;   // keeps what follows 16-byte aligned
 };
 
-// acc[j] = sum_i v[i] * W[j][i] over i ascending, for one output j (W row-major)
 template <int N>
-__device__ __forceinline__ float dot_row(const float* __restrict__ v, const float* __restrict__ wrow) {
-  const float4* w = reinterpret_cast<const float4*>(wrow);
-  float acc = 0.0f;
+__device__ __forceinline__ void store_row(float* dst, const float* v) {
 #pragma unroll
-  for (int q = 0; q < N / 4; ++q) {
-    const float4 w4 = w[q];
-    acc = fmaf(v[4 * q], w4.x, acc);
-    acc = fmaf(v[4 * q + 1], w4.y, acc);
-    acc = fmaf(v[4 * q + 2], w4.z, acc);
-    acc = fmaf(v[4 * q + 3], w4.w, acc);
-  }
-  return acc;
+  for (int q = 0; q < N / 4; ++q)
+    reinterpret_cast<float4*>(dst)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
 }
+
+// W [64][K] (row-major, global) -> W^T [K][64] in shared memory.  Each thread
+// takes four consecutive inputs of one output row, consecutive threads
+// consecutive outputs, so the shared-memory writes of a warp are contiguous;
+// every load is independent (all of them in flight at once).  blockDim.x must
+// be kFusedRows.
+template <int K>
+__device__ __forceinline__ void stage_transposed(float* __restrict__ dst, const float* __restrict__ W) {
+  constexpr int kItems = kW64 * (K / 4);
+#pragma unroll
+  for (int it = 0; it < (kItems + kFusedRows - 1) / kFusedRows; ++it) {
+    const int i = it * kFusedRows + (int)threadIdx.x;
+    if (i < kItems) {
+      const int j = i % kW64, k = 4 * (i / kW64);
+      const float w0 = W[j * K + k], w1 = W[j * K + k + 1], w2 = W[j * K + k + 2], w3 = W[j * K + k + 3];
+      dst[k * kW64 + j] = w0;
+      dst[(k + 1) * kW64 + j] = w1;
+      dst[(k + 2) * kW64 + j] = w2;
+      dst[(k + 3) * kW64 + j] = w3;
+    }
+  }
+}
+
+// Row strides of the per-thread shared-memory rows: float4-aligned, and eight
+// consecutive rows' float4s fall on distinct banks.
+constexpr int kXs = kFeat + 4, kHs = kW64 + 4;
+
+// C[8 rows][8 cols] += sum_k AT[k][rows] * BT[k][cols], k ascending from zero:
+// a register-blocked SIMT GEMM step over operands in shared memory (AT rows
+// contiguous, BT columns contiguous).  The thread's rows are r0..r0+3 and
+// r0+64..r0+67, its columns c0..c0+3 and c0+32..c0+35.
+template <int K>
+__device__ __forceinline__ void gemm_8x8(const float* __restrict__ AT, int lda, const float* __restrict__ BT,
+                                         int ldb, int r0, int c0, float (&acc)[8][8]) {
+#pragma unroll 2
+  for (int k = 0; k < K; ++k) {
+    const float4 a0 = *reinterpret_cast<const float4*>(AT + k * lda + r0);
+    const float4 a1 = *reinterpret_cast<const float4*>(AT + k * lda + r0 + 64);
+    const float4 b0 = *reinterpret_cast<const float4*>(BT + k * ldb + c0);
+    const float4 b1 = *reinterpret_cast<const float4*>(BT + k * ldb + c0 + 32);
+    const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+    const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+  }
+}
+
+// forward: W0^T [32][64], W1^T [64][64] (two layers), b0, b1, wo, bo; then the
+// transposed tiles X^T [32][128] and H^T [64][128] (hidden activations, then the
+// last layer's)
+template <int kL>
+struct FusedFwdSmem {
+  static constexpr int kWt0 = 0, kWt1 = kWt0 + kFeat * kW64;
+  static constexpr int kB0 = kWt1 + (kL == 2 ? kW64 * kW64 : 0), kB1 = kB0 + kW64, kWo = kB1 + kW64;
+  static constexpr int kBo = kWo + kW64, kXT = kBo + 4, kHT = kXT + kFeat * kFusedRows;
+  static constexpr int kTotal = kHT + kW64 * kFusedRows;
+};
 
 template <int kL, int kAct>
 __global__ void __launch_bounds__(kFusedRows)
@@ -297,80 +347,121 @@ mlp64_forward_kernel(int P, size_t rows, const float* __restrict__ means3D, cons
                      const float* __restrict__ params, const int* __restrict__ radii, float* __restrict__ S,
                      float2* __restrict__ signal) {
   using FP = FusedParams<kL>;
-  // W0 transposed ([32][64]: the first layer runs input-outer over 64 accumulators), then the rest as given
-  constexpr int kWt0 = 0, kRest = kW64 * kFeat;
-  __shared__ __align__(16) float sp[FP::kPadded];
-  for (int i = threadIdx.x; i < kW64 * kFeat; i += blockDim.x) {
-    const int k = i / kW64, j = i % kW64;
-    sp[kWt0 + i] = params[FP::kW0 + j * kFeat + k];
+  using SM = FusedFwdSmem<kL>;
+  extern __shared__ __align__(16) float sm[];
+  const int t = threadIdx.x;
+  stage_transposed<kFeat>(sm + SM::kWt0, params + FP::kW0);
+  if (kL == 2) stage_transposed<kW64>(sm + SM::kWt1, params + FP::kW1);
+  for (int i = t; i < kW64; i += blockDim.x) {
+    sm[SM::kB0 + i] = params[FP::kB0 + i];
+    if (kL == 2) sm[SM::kB1 + i] = params[FP::kB1 + i];
+    sm[SM::kWo + i] = params[FP::kWo + i];
   }
-  for (int i = kRest + threadIdx.x; i < FP::kCount; i += blockDim.x) sp[i] = params[i];
-  __syncthreads();
-  for (size_t row = blockIdx.x * (size_t)blockDim.x + threadIdx.x; row < rows; row += (size_t)gridDim.x * blockDim.x) {
-    if (radii[row] <= 0) continue;
-    float x[kFeat];
-    pair_features_fp32(means3D, rx_pos, (int)(row % P), (int)(row / P), x);
-    float a0[kW64];
+  if (t == 0) sm[SM::kBo] = params[FP::kBo];
+  float* XT = sm + SM::kXT;
+  float* HT = sm + SM::kHT;
+  // GEMM blocks: 16 row groups x 8 column groups; eight consecutive lanes share
+  // a column group, so the transposed stores of a lane octet are contiguous
+  const int r0 = (t & 15) * 4, c0 = (t >> 4) * 4;
+  const size_t ntiles = (rows + kFusedRows - 1) / kFusedRows;
+  for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const size_t row = tile * kFusedRows + t;
+    const bool vis = row < rows && radii[row] > 0;
+    __syncthreads();   // the previous tile's reads of XT / HT are done
+    {
+      float x[kFeat];
+      if (vis) pair_features_fp32(means3D, rx_pos, (int)(row % P), (int)(row / P), x);
+      else
 #pragma unroll
-    for (int j = 0; j < kW64; ++j) a0[j] = 0.0f;
+        for (int f = 0; f < kFeat; ++f) x[f] = 0.0f;
 #pragma unroll
-    for (int k = 0; k < kFeat; ++k) {
-      const float4* w = reinterpret_cast<const float4*>(sp + kWt0 + k * kW64);
+      for (int f = 0; f < kFeat; ++f) XT[f * kFusedRows + t] = x[f];
+    }
+    __syncthreads();
+    float acc[8][8];
 #pragma unroll
-      for (int q = 0; q < kW64 / 4; ++q) {
-        const float4 w4 = w[q];
-        a0[4 * q] = fmaf(x[k], w4.x, a0[4 * q]);
-        a0[4 * q + 1] = fmaf(x[k], w4.y, a0[4 * q + 1]);
-        a0[4 * q + 2] = fmaf(x[k], w4.z, a0[4 * q + 2]);
-        a0[4 * q + 3] = fmaf(x[k], w4.w, a0[4 * q + 3]);
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+    gemm_8x8<kFeat>(XT, kFusedRows, sm + SM::kWt0, kW64, r0, c0, acc);
+    if (kL == 2) {
+      // H^T = act(Z0 + b0), then the second layer over it
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int c = c0 + (j & 3) + (j >> 2) * 32;
+        const float b = sm[SM::kB0 + c];
+        float h[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) h[i] = act_fwd(kAct, acc[i][j] + b);
+        *reinterpret_cast<float4*>(HT + c * kFusedRows + r0) = make_float4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<float4*>(HT + c * kFusedRows + r0 + 64) = make_float4(h[4], h[5], h[6], h[7]);
       }
-    }
+      __syncthreads();
 #pragma unroll
-    for (int j = 0; j < kW64; ++j) a0[j] = act_fwd(kAct, a0[j] + sp[FP::kB0 + j]);
-    float o = 0.0f;
-    if (kL == 1) {
+      for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int j = 0; j < kW64; ++j) o = fmaf(a0[j], sp[FP::kWo + j], o);
-    } else {
-#pragma unroll 4
-      for (int j = 0; j < kW64; ++j)
-        o = fmaf(act_fwd(kAct, dot_row<kW64>(a0, sp + FP::kW1 + j * kW64) + sp[FP::kB1 + j]), sp[FP::kWo + j], o);
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+      gemm_8x8<kW64>(HT, kFusedRows, sm + SM::kWt1, kW64, r0, c0, acc);
+      __syncthreads();   // every thread has read HT before it is overwritten
     }
-    const float sg = 1.0f / (1.0f + expf(-(o + sp[FP::kBo])));
-    S[row] = sg;
-    signal[row] = make_float2(sg, 0.0f);
+    // the last hidden layer's activations -> H^T, then the output per row in the
+    // GEMMs' order (hidden units ascending)
+    const float* bl = sm + (kL == 2 ? SM::kB1 : SM::kB0);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int c = c0 + (j & 3) + (j >> 2) * 32;
+      const float b = bl[c];
+      float h[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) h[i] = act_fwd(kAct, acc[i][j] + b);
+      *reinterpret_cast<float4*>(HT + c * kFusedRows + r0) = make_float4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<float4*>(HT + c * kFusedRows + r0 + 64) = make_float4(h[4], h[5], h[6], h[7]);
+    }
+    __syncthreads();
+    if (vis) {
+      float o = 0.0f;
+#pragma unroll 8
+      for (int j = 0; j < kW64; ++j) o = fmaf(HT[j * kFusedRows + t], sm[SM::kWo + j], o);
+      const float sg = 1.0f / (1.0f + expf(-(o + sm[SM::kBo])));
+      S[row] = sg;
+      signal[row] = make_float2(sg, 0.0f);
+    }
   }
 }
 
-// Sum of v[i] over the warp, returned in lane i (v is overwritten).
-__device__ __forceinline__ float warp_sum_transpose32(float* v, int lane) {
+// C[8 rows][4 cols] += sum_k AT[k][rows] * B[k][cols] (rows r0..r0+3, r0+64..r0+67;
+// columns c0..c0+3), k ascending
+template <int K>
+__device__ __forceinline__ void gemm_8x4(const float* __restrict__ AT, int lda, const float* __restrict__ B, int ldb,
+                                         int r0, int c0, float (&acc)[8][4]) {
+#pragma unroll 2
+  for (int k = 0; k < K; ++k) {
+    const float4 a0 = *reinterpret_cast<const float4*>(AT + k * lda + r0);
+    const float4 a1 = *reinterpret_cast<const float4*>(AT + k * lda + r0 + 64);
+    const float4 b0 = *reinterpret_cast<const float4*>(B + k * ldb + c0);
+    const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+    const float b[4] = {b0.x, b0.y, b0.z, b0.w};
 #pragma unroll
-  for (int half = 16; half >= 1; half >>= 1) {
-    const bool upper = lane & half;
+    for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int i = 0; i < half; ++i) {
-      const float send = upper ? v[i] : v[i + half];
-      const float keep = upper ? v[i + half] : v[i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, half);
-    }
+      for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
   }
-  return v[0];
 }
 
-// Shared-memory tiles of the adjoint (floats; row strides keep float4 rows
-// aligned and 8 consecutive rows on distinct banks).
-constexpr int kXs = kFeat + 4, kHs = kW64 + 4;
-
+// adjoint shared memory (floats): weights W0 [64][32], W0^T, W1 [64][64], W1^T (two
+// layers), b0, b1, wo, bo; tiles X^T [32][128] (forward operand), X [128][36]
+// (rows, for dW0), HT [64][128] (H0^T, then H1^T, then dZ1^T, then dZ0^T), A0 [128][68]
+// (rows, for dW1), G0^T [64][128] (act'(Z0)), D [128][68] (dZ1, then dZ0, rows),
+// dO [128], dwo [64 + 4]
 template <int kL>
 struct FusedTiles {
-  using FP = FusedParams<kL>;
-  static constexpr int kX = FP::kPadded;
-  static constexpr int kA0 = kX + kFusedRows * kXs;        // act(Z0) rows (two layers)
-  static constexpr int kZ0 = kA0 + (kL == 2 ? kFusedRows * kHs : 0);
-  static constexpr int kD1 = kZ0 + (kL == 2 ? kFusedRows * kHs : 0);   // Z1, then dZ1, rows (two layers)
-  static constexpr int kD0 = kD1 + (kL == 2 ? kFusedRows * kHs : 0);   // Z0 then dZ0 (one layer); dZ0
-  static constexpr int kDwo = kD0 + kFusedRows * kHs;      // output-layer weight gradient, then its bias
-  static constexpr int kTotal = kDwo + kW64 + 4;
+  static constexpr int kW0 = 0, kWt0 = kW0 + kW64 * kFeat, kW1 = kWt0 + kFeat * kW64;
+  static constexpr int kWt1 = kW1 + (kL == 2 ? kW64 * kW64 : 0), kB0 = kWt1 + (kL == 2 ? kW64 * kW64 : 0);
+  static constexpr int kB1 = kB0 + kW64, kWo = kB1 + kW64, kBo = kWo + kW64;
+  static constexpr int kXT = kBo + 4, kX = kXT + kFeat * kFusedRows, kHT = kX + kFusedRows * kXs;
+  static constexpr int kA0 = kHT + kW64 * kFusedRows, kG0T = kA0 + (kL == 2 ? kFusedRows * kHs : 0);
+  static constexpr int kD = kG0T + (kL == 2 ? kW64 * kFusedRows : 0), kDO = kD + kFusedRows * kHs;
+  static constexpr int kDwo = kDO + kFusedRows, kTotal = kDwo + kW64 + 4;
 };
 
 // acc[4][NI] += sum over the tile's rows of D[r][j0..j0+3] (x) A[r][i0..i0+NI-1];
@@ -378,7 +469,7 @@ struct FusedTiles {
 template <int NI, int kAs>
 __device__ __forceinline__ void tile_outer(const float* __restrict__ D, const float* __restrict__ A, int j0, int i0,
                                            bool bias, float (&acc)[4][NI], float (&bsum)[4]) {
-#pragma unroll 4
+#pragma unroll 2
   for (int r = 0; r < kFusedRows; ++r) {
     const float4 d = *reinterpret_cast<const float4*>(D + r * kHs + j0);
     float a[NI];
@@ -397,35 +488,26 @@ __device__ __forceinline__ void tile_outer(const float* __restrict__ D, const fl
   }
 }
 
-template <int N>
-__device__ __forceinline__ void load_row(const float* __restrict__ src, float* v) {
+// the thread's 8x8 GEMM block column c (j = 0..7) and row (i = 0..7) indices
+__device__ __forceinline__ int blk_col(int c0, int j) { return c0 + (j & 3) + (j >> 2) * 32; }
+__device__ __forceinline__ int blk_row(int r0, int i) { return r0 + (i & 3) + (i >> 2) * 64; }
+
+// v[8][8] of the thread's block -> T [col][row] (transposed tile, 128 rows)
+__device__ __forceinline__ void store_block_T(float* T, int r0, int c0, const float (&v)[8][8]) {
 #pragma unroll
-  for (int q = 0; q < N / 4; ++q) {
-    const float4 a = reinterpret_cast<const float4*>(src)[q];
-    v[4 * q] = a.x; v[4 * q + 1] = a.y; v[4 * q + 2] = a.z; v[4 * q + 3] = a.w;
+  for (int j = 0; j < 8; ++j) {
+    const int c = blk_col(c0, j);
+    *reinterpret_cast<float4*>(T + c * kFusedRows + r0) = make_float4(v[0][j], v[1][j], v[2][j], v[3][j]);
+    *reinterpret_cast<float4*>(T + c * kFusedRows + r0 + 64) = make_float4(v[4][j], v[5][j], v[6][j], v[7][j]);
   }
 }
-template <int N>
-__device__ __forceinline__ void store_row(float* dst, const float* v) {
+// v[8][8] -> D [row][col] (row tiles, stride kHs)
+__device__ __forceinline__ void store_block_rows(float* D, int r0, int c0, const float (&v)[8][8]) {
 #pragma unroll
-  for (int q = 0; q < N / 4; ++q)
-    reinterpret_cast<float4*>(dst)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-}
-
-// One layer of the forward in dot form for this thread's row: z[j] (and
-// act(z)) for j in 0..63, written four at a time to the row's tile slots.
-template <int N, int kAct>
-__device__ __forceinline__ void layer_rows(const float* v, const float* __restrict__ W, const float* __restrict__ b,
-                                           float* zrow, float* arow) {
-#pragma unroll 2
-  for (int j = 0; j < kW64; j += 4) {
-    float z[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) z[u] = dot_row<N>(v, W + (j + u) * N) + b[j + u];
-    reinterpret_cast<float4*>(zrow)[j / 4] = make_float4(z[0], z[1], z[2], z[3]);
-    if (arow)
-      reinterpret_cast<float4*>(arow)[j / 4] =
-          make_float4(act_fwd(kAct, z[0]), act_fwd(kAct, z[1]), act_fwd(kAct, z[2]), act_fwd(kAct, z[3]));
+  for (int i = 0; i < 8; ++i) {
+    const int r = blk_row(r0, i);
+    *reinterpret_cast<float4*>(D + r * kHs + c0) = make_float4(v[i][0], v[i][1], v[i][2], v[i][3]);
+    *reinterpret_cast<float4*>(D + r * kHs + c0 + 32) = make_float4(v[i][4], v[i][5], v[i][6], v[i][7]);
   }
 }
 
@@ -438,139 +520,182 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
   using TL = FusedTiles<kL>;
   extern __shared__ __align__(16) float sm[];
   const int t = threadIdx.x, lane = t & 31;
-  for (int i = t; i < FP::kCount; i += blockDim.x) sm[i] = params[i];
-  for (int i = t; i < kW64 + 4; i += blockDim.x) sm[TL::kDwo + i] = 0.0f;
-  __syncthreads();
-  const float* W0 = sm + FP::kW0;
-  const float* W1 = sm + FP::kW1;
-  const float* wo = sm + FP::kWo;
-  float* Xs = sm + TL::kX;
+#pragma unroll 4
+  for (int i = t; i < kW64 * kFeat; i += kFusedRows) sm[TL::kW0 + i] = params[FP::kW0 + i];
+  stage_transposed<kFeat>(sm + TL::kWt0, params + FP::kW0);
+  if (kL == 2) {
+#pragma unroll 4
+    for (int i = t; i < kW64 * kW64; i += kFusedRows) sm[TL::kW1 + i] = params[FP::kW1 + i];
+    stage_transposed<kW64>(sm + TL::kWt1, params + FP::kW1);
+  }
+  for (int i = t; i < kW64; i += kFusedRows) {
+    sm[TL::kB0 + i] = params[FP::kB0 + i];
+    if (kL == 2) sm[TL::kB1 + i] = params[FP::kB1 + i];
+    sm[TL::kWo + i] = params[FP::kWo + i];
+  }
+  if (t == 0) sm[TL::kBo] = params[FP::kBo];
+  for (int i = t; i < kW64 + 4; i += kFusedRows) sm[TL::kDwo + i] = 0.0f;
+  float* XT = sm + TL::kXT;
+  float* Xr = sm + TL::kX;
+  float* HT = sm + TL::kHT;
   float* A0 = sm + TL::kA0;
-  float* Z0 = sm + TL::kZ0;
-  float* D1 = sm + TL::kD1;
-  float* D0 = sm + TL::kD0;
+  float* G0T = sm + TL::kG0T;
+  float* D = sm + TL::kD;
+  float* sdO = sm + TL::kDO;
   float* dwo = sm + TL::kDwo;
-  // the last hidden layer's pre-activation / dZ rows
-  float* DL = kL == 2 ? D1 : D0;
-
-  // this thread's blocks of the weight gradients, accumulated over all tiles
-  const int j0 = (t >> 3) * 4;
+  const float* wo = sm + TL::kWo;
+  const int r0 = (t & 15) * 4, c0 = (t >> 4) * 4;   // GEMM block of this thread (as the forward)
+  const int j0 = (t >> 3) * 4;                      // weight-gradient blocks
   const bool bias_owner = (t & 7) == 0;
-  float g1[4][8] = {}, gb1[4] = {};   // second layer: outputs j0..j0+3 x inputs (t & 7) * 8 ..+7
-  float g0[4][4] = {}, gb0[4] = {};   // first layer: outputs j0..j0+3 x features (t & 7) * 4 ..+3
+  float g1[4][8] = {}, gb1[4] = {};   // dW1: outputs j0..j0+3 x inputs (t & 7) * 8 ..+7, accumulated over tiles
+  float g0[4][4] = {}, gb0[4] = {};   // dW0: outputs j0..j0+3 x features (t & 7) * 4 ..+3
   const size_t ntiles = (rows + kFusedRows - 1) / kFusedRows;
   for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const size_t row = tile * kFusedRows + t;
     const bool vis = row < rows && radii[row] > 0;
-    float* xr = Xs + t * kXs;
-    float* dl = DL + t * kHs;
-    float red[kW64];   // dO * act(z) of the last hidden layer: this row's output-layer gradient
-    float dO = 0.0f;
-    if (!vis) {   // zero rows: they add nothing to the reductions
-#pragma unroll
-      for (int j = 0; j < kW64; ++j) red[j] = 0.0f;
-      store_row<kFeat>(xr, red);
-      store_row<kW64>(dl, red);
-      if (kL == 2) {
-        store_row<kW64>(A0 + t * kHs, red);
-        store_row<kW64>(Z0 + t * kHs, red);
-      }
-    } else {
-      // ---- forward recompute (same sums as mlp64_forward_kernel), Z of the
-      // last hidden layer into its dZ slots
-      {
-        float x[kFeat];
-        pair_features_fp32(means3D, rx_pos, (int)(row % P), (int)(row / P), x);
-        store_row<kFeat>(xr, x);
-        if (kL == 1) layer_rows<kFeat, kAct>(x, W0, sm + FP::kB0, dl, nullptr);
-        else layer_rows<kFeat, kAct>(x, W0, sm + FP::kB0, Z0 + t * kHs, A0 + t * kHs);
-      }
-      if (kL == 2) {
-        float a0[kW64];
-        load_row<kW64>(A0 + t * kHs, a0);
-        layer_rows<kW64, kAct>(a0, W1, sm + FP::kB1, dl, nullptr);
-      }
-      float zl[kW64];
-      load_row<kW64>(dl, zl);
-      float o = 0.0f;
-#pragma unroll
-      for (int j = 0; j < kW64; ++j) o = fmaf(act_fwd(kAct, zl[j]), wo[j], o);
-      const float sg = 1.0f / (1.0f + expf(-(o + sm[FP::kBo])));
-      dO = dL_dsignal[2 * row] * sg * (1.0f - sg);
-      // zl becomes dZ of the last hidden layer in place
-#pragma unroll
-      for (int j = 0; j < kW64; ++j) {
-        float a, d;
-        act_both(kAct, zl[j], a, d);
-        red[j] = dO * a;
-        zl[j] = dO * wo[j] * d;
-      }
-      store_row<kW64>(dl, zl);
-    }
+    __syncthreads();   // weights staged / the previous tile's reads done
     {
-      const float s0 = warp_sum_transpose32(red, lane);
-      const float s1 = warp_sum_transpose32(red + 32, lane);
-      atomicAdd(&dwo[lane], s0);
-      atomicAdd(&dwo[32 + lane], s1);
+      float x[kFeat];
+      if (vis) pair_features_fp32(means3D, rx_pos, (int)(row % P), (int)(row / P), x);
+      else
+#pragma unroll
+        for (int f = 0; f < kFeat; ++f) x[f] = 0.0f;
+#pragma unroll
+      for (int f = 0; f < kFeat; ++f) XT[f * kFusedRows + t] = x[f];
+      store_row<kFeat>(Xr + t * kXs, x);
+    }
+    __syncthreads();
+    // ---- forward recompute (the sums of mlp64_forward_kernel)
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+    gemm_8x8<kFeat>(XT, kFusedRows, sm + TL::kWt0, kW64, r0, c0, acc);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const float b = sm[TL::kB0 + blk_col(c0, j)];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) acc[i][j] += b;
+    }
+    if (kL == 2) {
+      float h[8][8], gd[8][8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) act_both(kAct, acc[i][j], h[i][j], gd[i][j]);
+      store_block_T(HT, r0, c0, h);
+      store_block_rows(A0, r0, c0, h);
+      store_block_T(G0T, r0, c0, gd);
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+      gemm_8x8<kW64>(HT, kFusedRows, sm + TL::kWt1, kW64, r0, c0, acc);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const float b = sm[TL::kB1 + blk_col(c0, j)];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i][j] += b;
+      }
+      __syncthreads();   // HT (H0^T) fully read
+    }
+    // acc = Z of the last hidden layer.  Its activations -> HT, output per row
+    {
+      float h[8][8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) h[i][j] = act_fwd(kAct, acc[i][j]);
+      store_block_T(HT, r0, c0, h);
+    }
+    __syncthreads();
+    {
+      float o = 0.0f;
+#pragma unroll 8
+      for (int j = 0; j < kW64; ++j) o = fmaf(HT[j * kFusedRows + t], wo[j], o);
+      const float sg = 1.0f / (1.0f + expf(-(o + sm[TL::kBo])));
+      const float dO = vis ? dL_dsignal[2 * row] * sg * (1.0f - sg) : 0.0f;
+      sdO[t] = dO;
       float ds = dO;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) ds += __shfl_xor_sync(0xffffffffu, ds, o);
+      for (int q = 16; q > 0; q >>= 1) ds += __shfl_xor_sync(0xffffffffu, ds, q);
       if (lane == 0) atomicAdd(&dwo[kW64], ds);
+    }
+    __syncthreads();   // dO ready; HT (H^T) fully read
+    {
+      // output-layer weight gradient: this block's rows, then over the 16 row groups (lanes)
+      float dOr[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) dOr[i] = sdO[blk_row(r0, i)];
+      float part[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        float p = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) p = fmaf(dOr[i], act_fwd(kAct, acc[i][j]), p);
+        part[j] = p;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int q = 8; q > 0; q >>= 1) part[j] += __shfl_xor_sync(0xffffffffu, part[j], q);
+      if ((t & 15) == 0)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) atomicAdd(&dwo[blk_col(c0, j)], part[j]);
+      // dZ of the last hidden layer -> rows (D) and transposed (HT)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const float w = wo[blk_col(c0, j)];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i][j] = dOr[i] * w * act_grad(kAct, acc[i][j]);
+      }
+      store_block_rows(D, r0, c0, acc);
+      store_block_T(HT, r0, c0, acc);
     }
     __syncthreads();
     if (kL == 2) {
-      // second layer: dW1 += D1^T A0, db1 += column sums of D1
-      tile_outer<8, kHs>(D1, A0, j0, (t & 7) * 8, bias_owner, g1, gb1);
-      // dZ0 = (W1^T dZ1) * act'(Z0) for this row: dZ1-outer over 64 accumulators
-      float da[kW64];
+      // second layer: dW1 += dZ1^T A0, db1 += column sums of dZ1
+      tile_outer<8, kHs>(D, A0, j0, (t & 7) * 8, bias_owner, g1, gb1);
+      // dZ0 = (dZ1 W1) * act'(Z0)
 #pragma unroll
-      for (int k = 0; k < kW64; ++k) da[k] = 0.0f;
-      if (vis) {
-#pragma unroll 2
-        for (int j = 0; j < kW64; ++j) {
-          const float dj = D1[t * kHs + j];
-          const float4* w = reinterpret_cast<const float4*>(W1 + j * kW64);
+      for (int i = 0; i < 8; ++i)
 #pragma unroll
-          for (int q = 0; q < kW64 / 4; ++q) {
-            const float4 w4 = w[q];
-            da[4 * q] = fmaf(dj, w4.x, da[4 * q]);
-            da[4 * q + 1] = fmaf(dj, w4.y, da[4 * q + 1]);
-            da[4 * q + 2] = fmaf(dj, w4.z, da[4 * q + 2]);
-            da[4 * q + 3] = fmaf(dj, w4.w, da[4 * q + 3]);
-          }
-        }
-        float z0[kW64];
-        load_row<kW64>(Z0 + t * kHs, z0);
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+      gemm_8x8<kW64>(HT, kFusedRows, sm + TL::kW1, kW64, r0, c0, acc);
 #pragma unroll
-        for (int k = 0; k < kW64; ++k) da[k] *= act_grad(kAct, z0[k]);
+      for (int j = 0; j < 8; ++j) {
+        const int c = blk_col(c0, j);
+        const float4 ga = *reinterpret_cast<const float4*>(G0T + c * kFusedRows + r0);
+        const float4 gb = *reinterpret_cast<const float4*>(G0T + c * kFusedRows + r0 + 64);
+        acc[0][j] *= ga.x; acc[1][j] *= ga.y; acc[2][j] *= ga.z; acc[3][j] *= ga.w;
+        acc[4][j] *= gb.x; acc[5][j] *= gb.y; acc[6][j] *= gb.z; acc[7][j] *= gb.w;
       }
-      store_row<kW64>(D0 + t * kHs, da);
+      __syncthreads();   // D (dZ1) and HT (dZ1^T) fully read
+      store_block_rows(D, r0, c0, acc);
+      store_block_T(HT, r0, c0, acc);
+      __syncthreads();
     }
-    // dX = W0^T dZ0 for this row (feature gradient, to HBM): dZ0-outer over 32 accumulators
-    if (row < rows) {
-      float dx[kFeat];
+    // first layer: dW0 += dZ0^T X, db0 += column sums of dZ0
+    tile_outer<4, kXs>(D, Xr, j0, (t & 7) * 4, bias_owner, g0, gb0);
+    // dX = dZ0 W0 (feature gradient, to HBM)
+    {
+      float dx[8][4];
 #pragma unroll
-      for (int k = 0; k < kFeat; ++k) dx[k] = 0.0f;
-#pragma unroll 2
-      for (int j = 0; j < kW64; ++j) {
-        const float dj = D0[t * kHs + j];
-        const float4* w = reinterpret_cast<const float4*>(W0 + j * kFeat);
+      for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int q = 0; q < kFeat / 4; ++q) {
-          const float4 w4 = w[q];
-          dx[4 * q] = fmaf(dj, w4.x, dx[4 * q]);
-          dx[4 * q + 1] = fmaf(dj, w4.y, dx[4 * q + 1]);
-          dx[4 * q + 2] = fmaf(dj, w4.z, dx[4 * q + 2]);
-          dx[4 * q + 3] = fmaf(dj, w4.w, dx[4 * q + 3]);
-        }
+        for (int j = 0; j < 4; ++j) dx[i][j] = 0.0f;
+      gemm_8x4<kW64>(HT, kFusedRows, sm + TL::kW0, kFeat, r0, c0, dx);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const size_t rr = tile * kFusedRows + blk_row(r0, i);
+        if (rr < rows)
+          *reinterpret_cast<float4*>(dX + rr * kFeat + c0) = make_float4(dx[i][0], dx[i][1], dx[i][2], dx[i][3]);
       }
-      store_row<kFeat>(dX + row * kFeat, dx);
     }
-    __syncthreads();
-    // first layer: dW0 += D0^T X, db0 += column sums of D0
-    tile_outer<4, kXs>(D0, Xs, j0, (t & 7) * 4, bias_owner, g0, gb0);
-    __syncthreads();
   }
+  __syncthreads();
   // this CTA's share -> global
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
@@ -583,21 +708,15 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
       if (bias_owner) atomicAdd(&dparams[FP::kB1 + j0 + u], gb1[u]);
     }
   }
-  for (int j = t; j <= kW64; j += blockDim.x) atomicAdd(&dparams[FP::kWo + j], dwo[j]);   // kWo + 64 = kBo
+  for (int j = t; j <= kW64; j += kFusedRows) atomicAdd(&dparams[FP::kWo + j], dwo[j]);   // kWo + 64 = kBo
 }
 
 template <int kL, int kAct>
 static cudaError_t launch_fused(bool fwd, int P, size_t rows, const float* means3D, const float* rx_pos,
                                 const float* params, const GeomView& geo, const SharedMlpLayout& L, float* work,
                                 const float* dL_dsignal, float* dparams, cudaStream_t s) {
-  if (fwd) {
-    const size_t blocks = (rows + kFusedRows - 1) / kFusedRows;
-    mlp64_forward_kernel<kL, kAct><<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), kFusedRows, 0, s>>>(
-        P, rows, means3D, rx_pos, params, geo.radii, work + L.s, geo.signal);
-    return cudaGetLastError();
-  }
-  const size_t smem = (size_t)FusedTiles<kL>::kTotal * sizeof(float);
-  static bool attr_done[64] = {};
+  const size_t smem = (size_t)(fwd ? FusedFwdSmem<kL>::kTotal : FusedTiles<kL>::kTotal) * sizeof(float);
+  static bool attr_done[2][64] = {};
   static int sm_count[64] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -607,12 +726,21 @@ static cudaError_t launch_fused(bool fwd, int P, size_t rows, const float* means
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     if (dev >= 0 && dev < 64) sm_count[dev] = sms;
   }
-  if (dev < 0 || dev >= 64 || !attr_done[dev]) {
-    e = cudaFuncSetAttribute(mlp64_backward_kernel<kL, kAct>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (dev < 0 || dev >= 64 || !attr_done[fwd][dev]) {
+    e = fwd ? cudaFuncSetAttribute(mlp64_forward_kernel<kL, kAct>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem)
+            : cudaFuncSetAttribute(mlp64_backward_kernel<kL, kAct>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem);
     if (e != cudaSuccess) return e;
-    if (dev >= 0 && dev < 64) attr_done[dev] = true;
+    if (dev >= 0 && dev < 64) attr_done[fwd][dev] = true;
   }
   const size_t ntiles = (rows + kFusedRows - 1) / kFusedRows;
+  if (fwd) {
+    const size_t cap = (size_t)sms * 2;   // persistent, two CTAs per SM (74 KB of shared memory each)
+    mlp64_forward_kernel<kL, kAct><<<(unsigned)(ntiles < cap ? ntiles : cap), kFusedRows, smem, s>>>(
+        P, rows, means3D, rx_pos, params, geo.radii, work + L.s, geo.signal);
+    return cudaGetLastError();
+  }
   const unsigned grid = (unsigned)(ntiles < (size_t)sms ? ntiles : (size_t)sms);
   mlp64_backward_kernel<kL, kAct><<<grid, kFusedRows, smem, s>>>(P, rows, means3D, rx_pos, params, geo.radii,
                                                                  dL_dsignal, work + L.d0, dparams);
