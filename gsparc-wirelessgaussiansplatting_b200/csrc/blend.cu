@@ -221,35 +221,6 @@ blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict
   }
 }
 
-// Sum eight per-lane values over the warp.  Returns the full sum of value
-// `vidx` in lanes with (lane & 3) == 0, where vidx = bits 4,3,2 of the lane.
-__device__ __forceinline__ float warp_reduce8(const float v[8], int lane) {
-  const bool b16 = lane & 16, b8 = lane & 8, b4 = lane & 4;
-  float u[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const float send = b16 ? v[k] : v[k + 4];
-    const float keep = b16 ? v[k + 4] : v[k];
-    u[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-  }
-  float w[2];
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const float send = b8 ? u[k] : u[k + 2];
-    const float keep = b8 ? u[k + 2] : u[k];
-    w[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-  }
-  float z;
-  {
-    const float send = b4 ? w[0] : w[1];
-    const float keep = b4 ? w[1] : w[0];
-    z = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-  }
-  z += __shfl_xor_sync(0xffffffffu, z, 2);
-  z += __shfl_xor_sync(0xffffffffu, z, 1);
-  return z;
-}
-
 template <int kThreads>
 __global__ void __launch_bounds__(kThreads)
 blend_backward_kernel(int P, int H, int W, TileGrid grid, int RT, unsigned grad_mode,

@@ -47,6 +47,7 @@ bool valid_tile(int th, int tw) {
 enum KernelId {
   KID_PREPROCESS, KID_CHECK, KID_SCATTER, KID_DEPTH_SORT, KID_PLACE, KID_BLEND_FWD, KID_BLEND_BWD,
   KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_ADAM, KID_LOSS, KID_ACTIVATE, KID_SHARED_MLP, KID_SHARED_MLP_BWD,
+  KID_BLEND_MC_FWD, KID_BLEND_MC_BWD,
   KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
@@ -54,7 +55,7 @@ const char* const kKernelNames[KID_COUNT] = {
     "depth_sort_kernels", "segment_place_kernel", "blend_forward_kernel", "blend_backward_kernel", "geometry_backward_kernel",
     "emission_backward_kernel", "ssim_forward_kernel", "ssim_backward_kernel", "mark_visible_kernel",
     "gaussian_adam_kernels", "splat_loss_kernels", "gaussian_activate_kernel", "shared_mlp_forward_kernels",
-    "shared_mlp_backward_kernels"};
+    "shared_mlp_backward_kernels", "blend_channels_forward_kernel", "blend_channels_backward_kernel"};
 
 struct PendingTiming {
   int id;
@@ -108,7 +109,7 @@ int report_cuda(cudaError_t e, const char* where) { return cuda_fail(e, where); 
 
 extern "C" {
 
-int gsparc_abi_version(void) { return 4; }
+int gsparc_abi_version(void) { return 5; }
 
 const char* gsparc_status_string(int status) {
   switch (status) {
@@ -213,6 +214,30 @@ int gsparc_rasterize_prepare(int P, int R, int H, int W, int tile_h, int tile_w,
   return GSPARC_OK;
 }
 
+namespace {
+// The binning stages shared by the single- and multi-channel renders: depth
+// order, instance scatter, segment placement.
+int render_binning(int P, int R, const TileGrid& grid, GeomView& geo, ImageView& img, BinningView& bin,
+                   long long capacity, cudaStream_t s) {
+  if (P == 0) {
+    Timed t(KID_CHECK, s);
+    GS_CHECK(launch_check_capacity(img, (unsigned long long)capacity, s), "capacity check");
+  } else {
+    Timed t(KID_DEPTH_SORT, s);   // also records the capacity and flags K > capacity
+    GS_CHECK(launch_depth_sort(P, R, geo, img, (unsigned long long)capacity, s), "depth sort");
+  }
+  {
+    Timed t(KID_SCATTER, s);
+    GS_CHECK(launch_scatter(P, R, grid, geo, img, bin, s), "scatter");
+  }
+  {
+    Timed t(KID_PLACE, s);
+    GS_CHECK(launch_segment_place(P, R, grid, geo, img, bin, s), "segment place");
+  }
+  return GSPARC_OK;
+}
+}  // namespace
+
 int gsparc_rasterize_render(int P, int R, int H, int W, int tile_h, int tile_w, unsigned int flags,
                             const void* geom_state,
                             void* image_state, void* binning_state, long long capacity, float* out_real,
@@ -231,24 +256,39 @@ int gsparc_rasterize_render(int P, int R, int H, int W, int tile_h, int tile_w, 
   carve_image((char*)image_state, (size_t)R, (size_t)grid.T, (size_t)H * W, &img);
   BinningView bin{};
   carve_binning((char*)binning_state, (size_t)capacity, &bin);
-  if (P == 0) {
-    Timed t(KID_CHECK, s);
-    GS_CHECK(launch_check_capacity(img, (unsigned long long)capacity, s), "capacity check");
-  } else {
-    Timed t(KID_DEPTH_SORT, s);   // also records the capacity and flags K > capacity
-    GS_CHECK(launch_depth_sort(P, R, geo, img, (unsigned long long)capacity, s), "depth sort");
-  }
-  {
-    Timed t(KID_SCATTER, s);
-    GS_CHECK(launch_scatter(P, R, grid, geo, img, bin, s), "scatter");
-  }
-  {
-    Timed t(KID_PLACE, s);
-    GS_CHECK(launch_segment_place(P, R, grid, geo, img, bin, s), "segment place");
-  }
+  int st = render_binning(P, R, grid, geo, img, bin, capacity, s);
+  if (st != GSPARC_OK) return st;
   {
     Timed t(KID_BLEND_FWD, s);
     GS_CHECK(launch_blend_forward(P, R, H, W, grid, geo, img, bin, out_real, out_imag, s), "blend forward");
+  }
+  return GSPARC_OK;
+}
+
+int gsparc_rasterize_render_channels(int P, int R, int H, int W, int tile_h, int tile_w, unsigned int flags, int C,
+                                     const void* geom_state, void* image_state, void* binning_state,
+                                     long long capacity, const float* features, float* out, void* stream) {
+  if (P < 0 || R < 1 || H <= 0 || W <= 0 || capacity < 0) return invalid("sizes");
+  if (C < 1 || C > kMaxChannels) return invalid("channels must be in [1, 64]");
+  if (!valid_tile(tile_h, tile_w)) return invalid("tile shape must be 16x16, 8x32 or 32x8");
+  if (!image_state || !out) return invalid("null image state or output");
+  if (capacity > 0 && !binning_state) return invalid("null binning state");
+  if (P > 0 && (!geom_state || !features)) return invalid("null geometry state or features");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (flags & ~GSPARC_FLAG_WRAP_AZIMUTH) return invalid("unknown flags");
+  TileGrid grid(H, W, tile_h, tile_w, (flags & GSPARC_FLAG_WRAP_AZIMUTH) ? 1 : 0);
+  GeomView geo{};
+  if (geom_state) carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
+  ImageView img;
+  carve_image((char*)image_state, (size_t)R, (size_t)grid.T, (size_t)H * W, &img);
+  BinningView bin{};
+  carve_binning((char*)binning_state, (size_t)capacity, &bin);
+  int st = render_binning(P, R, grid, geo, img, bin, capacity, s);
+  if (st != GSPARC_OK) return st;
+  {
+    Timed t(KID_BLEND_MC_FWD, s);
+    GS_CHECK(launch_blend_channels_forward(P, R, H, W, C, grid, geo, img, bin, features, out, s),
+             "blend forward (channels)");
   }
   return GSPARC_OK;
 }
@@ -324,6 +364,53 @@ int gsparc_rasterize_backward(int P, int R, int H, int W, int tile_h, int tile_w
   return GSPARC_OK;
 }
 
+int gsparc_rasterize_backward_channels(int P, int R, int H, int W, int tile_h, int tile_w, unsigned int flags,
+                                       int C, float scale_modifier, const float* means3D, const float* scales,
+                                       const float* rotations, const float* viewmatrices, const void* geom_state,
+                                       const void* image_state, const void* binning_state,
+                                       long long binning_capacity, const float* features, const float* dL_dout,
+                                       float* dL_dfeatures, float* dL_dmeans2D, float* dL_dconic,
+                                       float* dL_dopacity, float* dL_dmeans3D, float* dL_dcov3D, float* dL_dscales,
+                                       float* dL_drotations, void* stream) {
+  if (P < 0 || R < 1 || H <= 0 || W <= 0 || binning_capacity < 0) return invalid("sizes");
+  if (C < 1 || C > kMaxChannels) return invalid("channels must be in [1, 64]");
+  if (!valid_tile(tile_h, tile_w)) return invalid("tile shape must be 16x16, 8x32 or 32x8");
+  if (!image_state || !dL_dout || !viewmatrices) return invalid("null image state, upstream gradient or view");
+  if (P == 0) return GSPARC_OK;
+  if (!geom_state || !means3D || !scales || !rotations || !features || !dL_dfeatures || !dL_dmeans2D ||
+      !dL_dconic || !dL_dopacity || !dL_dmeans3D || !dL_dcov3D || !dL_dscales || !dL_drotations)
+    return invalid("null Gaussian input or gradient output");
+  if (binning_capacity > 0 && !binning_state) return invalid("null binning state");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (flags & ~GSPARC_FLAG_WRAP_AZIMUTH) return invalid("unknown flags");
+  TileGrid grid(H, W, tile_h, tile_w, (flags & GSPARC_FLAG_WRAP_AZIMUTH) ? 1 : 0);
+  GeomView geo;
+  carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
+  ImageView img;
+  carve_image((char*)image_state, (size_t)R, (size_t)grid.T, (size_t)H * W, &img);
+  BinningView bin{};
+  carve_binning((char*)binning_state, (size_t)binning_capacity, &bin);
+  const size_t rp = (size_t)R * P;
+  GS_CHECK(cudaMemsetAsync(dL_dmeans2D, 0, rp * 3 * sizeof(float), s), "memset dmeans2D");
+  GS_CHECK(cudaMemsetAsync(dL_dconic, 0, rp * 4 * sizeof(float), s), "memset dconic");
+  GS_CHECK(cudaMemsetAsync(dL_dfeatures, 0, rp * (size_t)C * sizeof(float), s), "memset dfeatures");
+  GS_CHECK(cudaMemsetAsync(dL_dopacity, 0, (size_t)P * sizeof(float), s), "memset dopacity");
+  {
+    Timed t(KID_BLEND_MC_BWD, s);
+    GS_CHECK(launch_blend_channels_backward(P, R, H, W, C, grid, geo, img, bin, features, dL_dout, dL_dfeatures,
+                                            dL_dmeans2D, dL_dconic, dL_dopacity, s),
+             "blend backward (channels)");
+  }
+  {
+    Timed t(KID_GEOM_BWD, s);
+    GS_CHECK(launch_geometry_backward(P, R, H, W, scale_modifier, GSPARC_GRAD_EXACT, means3D, scales, rotations,
+                                      viewmatrices, geo, dL_dmeans2D, dL_dconic, dL_dmeans3D, dL_dcov3D, dL_dscales,
+                                      dL_drotations, s),
+             "geometry backward");
+  }
+  return GSPARC_OK;
+}
+
 // ---- shared emission MLP -------------------------------------------------------
 
 namespace {
@@ -331,10 +418,10 @@ int check_mlp_spec(int layers, int width, int act, int out, int precision) {
   if (layers < 1 || layers > kMaxMlpLayers) return invalid("layers must be in [1, 6]");
   if (width < 8 || width > 256) return invalid("width must be in [8, 256]");
   if (act != GSPARC_ACT_RELU && act != GSPARC_ACT_GELU) return invalid("act must be GSPARC_ACT_RELU or _GELU");
-  if (out != 1) return invalid("out must be 1 (one amplitude per pair)");
+  if (out < 1 || out > kMaxChannels) return invalid("out must be in [1, 64]");
   if (precision != GSPARC_MLP_FP32 && precision != GSPARC_MLP_BF16) return invalid("precision");
-  if (precision == GSPARC_MLP_BF16 && (width != 128 || layers > 3))
-    return invalid("the BF16 tensor-core path needs width 128 and at most 3 hidden layers");
+  if (precision == GSPARC_MLP_BF16 && (width != 128 || layers > 3 || out != 1))
+    return invalid("the BF16 tensor-core path needs width 128, at most 3 hidden layers and one output");
   return GSPARC_OK;
 }
 }  // namespace

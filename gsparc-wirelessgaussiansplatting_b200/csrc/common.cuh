@@ -62,6 +62,8 @@ struct TileGrid {
 // per (receiver, Gaussian) -- the depth bits of visible Gaussians, ~0 for the
 // rest -- in tiles of kSortTileKeys keys with decoupled look-back.
 constexpr int kSortTileKeys = 2048;   // 256 threads x 8 keys
+// Multi-channel blend (blend_channels.cu): at most this many amplitude channels.
+constexpr int kMaxChannels = 64;
 __host__ __device__ inline size_t sort_tiles(size_t P) { return (P + kSortTileKeys - 1) / kSortTileKeys; }
 // words of the sort state: digit histograms [R][4][256], tile tickets [R][4],
 // look-back words [R][4][tiles][256]; zeroed before every preprocess
@@ -499,6 +501,35 @@ __device__ __forceinline__ bool box_outside(const float4 b, float x0, float x1, 
 
 __device__ __forceinline__ void atomic_or_error(ImageHeader* hdr, uint32_t bits) {
   atomicOr(&hdr->error, bits);
+}
+
+// Sum eight per-lane values over the warp.  Returns the full sum of value
+// `vidx` in lanes with (lane & 3) == 0, where vidx = bits 4,3,2 of the lane.
+__device__ __forceinline__ float warp_reduce8(const float v[8], int lane) {
+  const bool b16 = lane & 16, b8 = lane & 8, b4 = lane & 4;
+  float u[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float send = b16 ? v[k] : v[k + 4];
+    const float keep = b16 ? v[k + 4] : v[k];
+    u[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+  float w[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float send = b8 ? u[k] : u[k + 2];
+    const float keep = b8 ? u[k + 2] : u[k];
+    w[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  float z;
+  {
+    const float send = b4 ? w[0] : w[1];
+    const float keep = b4 ? w[1] : w[0];
+    z = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  z += __shfl_xor_sync(0xffffffffu, z, 2);
+  z += __shfl_xor_sync(0xffffffffu, z, 1);
+  return z;
 }
 
 // Gaussian id read from a point list, clamped into [0, P) so a mismatched or

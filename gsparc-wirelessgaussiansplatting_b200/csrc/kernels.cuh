@@ -90,6 +90,15 @@ struct SharedMlpLayout {
 };
 SharedMlpLayout shared_mlp_layout(int layers, int width, int out, size_t rows);
 
+// Multi-channel blend (blend_channels.cu): features [R][P][C], out [R][C][H][W].
+cudaError_t launch_blend_channels_forward(int P, int R, int H, int W, int C, const TileGrid& grid,
+                                          const GeomView& geo, const ImageView& img, const BinningView& bin,
+                                          const float* features, float* out, cudaStream_t s);
+cudaError_t launch_blend_channels_backward(int P, int R, int H, int W, int C, const TileGrid& grid,
+                                           const GeomView& geo, const ImageView& img, const BinningView& bin,
+                                           const float* features, const float* dL_dout, float* dL_dfeatures,
+                                           float* dmean2D, float* dconic, float* dopacity, cudaStream_t s);
+
 // BF16 / tcgen05 path (shared_mlp_tc.cu): width 128, one output, 1-3 layers;
 // workspace: BF16 pre-activations [layers][rows][128] at z[1], signal at s,
 // feature gradient [rows][32] at d0.

@@ -231,15 +231,16 @@ mlp_colsum_kernel(int M, int N, const float* __restrict__ A, float* __restrict__
   }
 }
 
-// signal = sigmoid(o_0) for visible pairs; dO = dL/dsignal_real * s (1 - s)
+// S = sigmoid(O) per output; with one output the signal of visible pairs is
+// (S, 0).  Backward: dO = dL/dS * S (1 - S), where dL/dS is the real part of
+// dL/dsignal (stride 2) for one output and dL/dfeatures (stride Cout) otherwise.
 __global__ void __launch_bounds__(256)
 mlp_signal_kernel(size_t rows, int Cout, const float* __restrict__ O, const int* __restrict__ radii,
                   float* __restrict__ S, float2* __restrict__ signal) {
   const size_t row = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (row >= rows) return;
-  const float s = 1.0f / (1.0f + expf(-O[row * Cout]));
-  S[row] = s;
-  if (radii[row] > 0) signal[row] = make_float2(s, 0.0f);
+  for (int c = 0; c < Cout; ++c) S[row * Cout + c] = 1.0f / (1.0f + expf(-O[row * Cout + c]));
+  if (Cout == 1 && radii[row] > 0) signal[row] = make_float2(S[row], 0.0f);
 }
 
 __global__ void __launch_bounds__(256)
@@ -247,9 +248,12 @@ mlp_signal_backward_kernel(size_t rows, int Cout, const float* __restrict__ S, c
                            const float* __restrict__ dL_dsignal, float* __restrict__ dO) {
   const size_t row = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (row >= rows) return;
-  const float s = S[row];
-  const float g = radii[row] > 0 ? dL_dsignal[2 * row] * s * (1.0f - s) : 0.0f;
-  for (int c = 0; c < Cout; ++c) dO[row * Cout + c] = c == 0 ? g : 0.0f;
+  const bool vis = radii[row] > 0;
+  const int ld = Cout == 1 ? 2 : Cout;
+  for (int c = 0; c < Cout; ++c) {
+    const float s = S[row * Cout + c];
+    dO[row * Cout + c] = vis ? dL_dsignal[row * ld + c] * s * (1.0f - s) : 0.0f;
+  }
 }
 
 // ---- fused path: width 64, one output, one or two hidden layers --------------
@@ -784,6 +788,8 @@ SharedMlpLayout shared_mlp_layout(int layers, int width, int out, size_t rows) {
     L.work = w;
     return L;
   }
+  L.s = w;   // first: the sigmoid outputs [rows][out] (the amplitudes for out > 1)
+  w += al(rows * out);
   L.x0 = w;
   w += al(rows * kFeat);
   for (int l = 1; l <= layers; ++l) {
@@ -794,8 +800,6 @@ SharedMlpLayout shared_mlp_layout(int layers, int width, int out, size_t rows) {
   }
   L.o = w;
   w += al(rows * out);
-  L.s = w;
-  w += al(rows);
   size_t dw = width > kFeat ? width : kFeat;
   if ((size_t)out > dw) dw = out;
   L.d0 = w;

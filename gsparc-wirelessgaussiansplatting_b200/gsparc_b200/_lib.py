@@ -50,6 +50,11 @@ _SIGS = {
                                            _c_uint,
                                            _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_ll,
                                            _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gsparc_rasterize_render_channels": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_uint, _c_int,
+                                                  _vp, _vp, _vp, _c_ll, _vp, _vp, _vp]),
+    "gsparc_rasterize_backward_channels": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_uint, _c_int,
+                                                    _c_float, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_ll, _vp, _vp,
+                                                    _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gsparc_mark_visible": (_c_int, [_c_int, _vp, _vp, _vp, _vp]),
     "gsparc_ssim_forward": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_float, _c_float,
                                      _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

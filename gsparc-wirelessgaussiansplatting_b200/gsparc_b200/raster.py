@@ -225,6 +225,96 @@ def backward(st: ForwardState, means3D, emission_mlps, scales, rotations, scale_
     return out
 
 
+def forward_channels(means3D, opacities, scales, rotations, H, W, scale_modifier, viewmatrices, tx_pos, rx_pos,
+                     shared, shared_params, tile=None, capacity=None, binning=None, out=None, radii=None, geom=None,
+                     image=None, wrap=False):
+    """Render R x C spectra: the shared emission MLP with ``shared.out = C``
+    outputs gives every (receiver, Gaussian) pair C amplitudes (one per
+    frequency bin), blended with one set of transmittance decisions
+    (gsparc_rasterize_render_channels).  Returns (out [R,C,H,W], radii [R,P],
+    ForwardState); the amplitudes are ``shared.features(P, R)``."""
+    if means3D.dim() != 2 or means3D.shape[1] != 3:
+        raise RuntimeError("means3D must have dimensions (num_points, 3)")
+    if shared is None or shared.precision != "fp32":
+        raise ValueError("forward_channels needs an FP32 SharedMLP (out = channels)")
+    device = means3D.device
+    tile = tuple(_tile if tile is None else tile)
+    P = means3D.shape[0]
+    v, rx = _receivers(viewmatrices, rx_pos, device)
+    R, C = v.shape[0], shared.out
+    m = _dev_f32(means3D, "means3D")
+    tx = _dev_f32(tx_pos, "tx_pos", device).reshape(-1)
+    op = _dev_f32(opacities, "opacities", device).reshape(-1)
+    sc = _dev_f32(scales, "scales", device).reshape(P, 3)
+    rot = _dev_f32(rotations, "rotations", device).reshape(P, 4)
+    sp = _dev_f32(shared_params, "shared_params", device).reshape(-1)
+    if sp.numel() != shared.n_params:
+        raise ValueError(f"shared_params must hold {shared.n_params} floats")
+    L = _lib.lib()
+    if out is None:
+        out = torch.zeros((R, C, H, W), dtype=torch.float32, device=device)
+    if radii is None:
+        radii = torch.zeros((R, P), dtype=torch.int32, device=device)
+    if geom is None:
+        geom = torch.empty(_lib.geom_state_bytes(P, R), dtype=torch.uint8, device=device)
+    if image is None:
+        image = torch.empty(_lib.image_state_bytes(R, H, W, *tile), dtype=torch.uint8, device=device)
+    stream = stream_of(device)
+    flags = _lib.FLAG_WRAP_AZIMUTH if wrap else 0
+    K = ctypes.c_longlong(0)
+    check("rasterize_prepare", L.gsparc_rasterize_prepare(
+        P, R, H, W, tile[0], tile[1], flags, float(scale_modifier), ptr(m), None, ptr(op), ptr(sc), ptr(rot),
+        ptr(v), ptr(tx), ptr(rx), ptr(radii), ptr(geom), ptr(image),
+        ctypes.byref(K) if capacity is None else None, stream))
+    shared.forward(P, R, m, rx, sp, geom, image)
+    feats = shared.features(P, R)
+    if capacity is None:
+        capacity = int(K.value)
+        num_rendered = capacity
+    else:
+        num_rendered = -1
+    if binning is None:
+        binning = torch.empty(max(_lib.binning_state_bytes(capacity), 1), dtype=torch.uint8, device=device)
+    check("rasterize_render_channels", L.gsparc_rasterize_render_channels(
+        P, R, H, W, tile[0], tile[1], flags, C, ptr(geom), ptr(image), ptr(binning), int(capacity), ptr(feats),
+        ptr(out), stream))
+    st = ForwardState(P, R, H, W, tile, int(capacity), num_rendered, geom, image, binning, flags)
+    return out, radii, st
+
+
+def backward_channels(st: ForwardState, means3D, scales, rotations, scale_modifier, viewmatrices, tx_pos, rx_pos,
+                      dL_dout, shared, shared_params, out=None):
+    """Adjoint of ``forward_channels`` (true derivative).  Returns a dict:
+    dmeans2D [R,P,3], dconic [R,P,4], dfeatures [R,P,C], dopacity [P],
+    dmeans3D [P,3], dcov3D [P,6], dscales [P,3], drotations [P,4],
+    dshared [n_params]."""
+    device = means3D.device
+    P, R, H, W = st.P, st.R, st.H, st.W
+    C = shared.out
+    m = _dev_f32(means3D, "means3D")
+    v, rx = _receivers(viewmatrices, rx_pos, device)
+    g = _dev_f32(dL_dout, "dL_dout", device).reshape(R, C, H, W)
+    if out is None:
+        z = lambda *s: torch.empty(s, dtype=torch.float32, device=device)
+        out = dict(dmeans2D=z(R, P, 3), dconic=z(R, P, 4), dfeatures=z(R, P, C), dopacity=z(P), dmeans3D=z(P, 3),
+                   dcov3D=z(P, 6), dscales=z(P, 3), drotations=z(P, 4), dshared=z(shared.n_params))
+    if P == 0:
+        for t in out.values():
+            t.zero_()
+        return out
+    sc = _dev_f32(scales, "scales", device).reshape(P, 3)
+    rot = _dev_f32(rotations, "rotations", device).reshape(P, 4)
+    sp = _dev_f32(shared_params, "shared_params", device).reshape(-1)
+    feats = shared.features(P, R)
+    check("rasterize_backward_channels", _lib.lib().gsparc_rasterize_backward_channels(
+        P, R, H, W, st.tile[0], st.tile[1], st.flags, C, float(scale_modifier), ptr(m), ptr(sc), ptr(rot), ptr(v),
+        ptr(st.geom), ptr(st.image), ptr(st.binning), int(st.capacity), ptr(feats), ptr(g), ptr(out["dfeatures"]),
+        ptr(out["dmeans2D"]), ptr(out["dconic"]), ptr(out["dopacity"]), ptr(out["dmeans3D"]), ptr(out["dcov3D"]),
+        ptr(out["dscales"]), ptr(out["drotations"]), stream_of(device)))
+    shared.backward(P, R, m, rx, sp, st.geom, out["dfeatures"], out["dshared"], out["dmeans3D"], st.image)
+    return out
+
+
 def mark_visible(means3D, viewmatrix):
     m = _dev_f32(means3D, "means3D")
     v = _dev_f32(viewmatrix, "viewmatrix", m.device).reshape(16)

@@ -90,6 +90,11 @@ class SharedMLP:
             self._work_key = key
         return self._work
 
+    def features(self, P, R):
+        """[R, P, out] amplitudes (sigmoid outputs) of the last forward: the
+        first R*P*out floats of the workspace (out > 1, FP32)."""
+        return self._work[:int(R) * int(P) * self.out].view(int(R), int(P), self.out)
+
     def _spec(self):
         return (self.layers, self.width, ACTS[self.act], self.out, PRECISIONS[self.precision])
 

@@ -169,6 +169,37 @@ GSPARC_API int gsparc_rasterize_backward(int P, int R, int H, int W, int tile_h,
                               float* dL_dscales, float* dL_drotations,
                               float* dL_demission_mlps, void* stream);
 
+/* ---- multi-channel render (C amplitude channels per Gaussian) ------------ */
+
+/* Stage 2 of the forward for C channels (1 <= C <= 64, e.g. one per frequency
+ * bin): the binning of gsparc_rasterize_render, then one blend of all C
+ * channels with the same transmittance and contributor decisions (final T and
+ * contributor counts equal a single-channel render of the same geometry).
+ * The reference blends NUM_CHANNELS = 1 (config.h:15, forward.cu:151-249).
+ * features [R,P,C] are per-(receiver, Gaussian) amplitudes (from
+ * gsparc_shared_mlp_forward with out = C); out [R,C,H,W] is overwritten:
+ * out[r,c] = sum_i features[r,i,c] * alpha_i * T_i. */
+GSPARC_API int gsparc_rasterize_render_channels(int P, int R, int H, int W, int tile_h, int tile_w,
+                                     unsigned int flags, int C, const void* geom_state, void* image_state,
+                                     void* binning_state, long long capacity, const float* features,
+                                     float* out, void* stream);
+
+/* Adjoint of gsparc_rasterize_render_channels (the true derivative; the 0.99
+ * alpha clamp blocks the gradient) followed by the conic / projection / cov3D
+ * adjoint of gsparc_rasterize_backward in GSPARC_GRAD_EXACT mode.  dL_dout
+ * [R,C,H,W].  Outputs (all overwritten): dL_dfeatures [R,P,C], dL_dmeans2D
+ * [R,P,3], dL_dconic [R,P,4], dL_dopacity [P], dL_dmeans3D [P,3] (geometry
+ * part), dL_dcov3D [P,6], dL_dscales [P,3], dL_drotations [P,4]. */
+GSPARC_API int gsparc_rasterize_backward_channels(int P, int R, int H, int W, int tile_h, int tile_w,
+                                       unsigned int flags, int C, float scale_modifier,
+                                       const float* means3D, const float* scales, const float* rotations,
+                                       const float* viewmatrices, const void* geom_state,
+                                       const void* image_state, const void* binning_state,
+                                       long long binning_capacity, const float* features,
+                                       const float* dL_dout, float* dL_dfeatures, float* dL_dmeans2D,
+                                       float* dL_dconic, float* dL_dopacity, float* dL_dmeans3D,
+                                       float* dL_dcov3D, float* dL_dscales, float* dL_drotations, void* stream);
+
 /* Range cull only: present[i] = |view * means3D[i]|^2 > 0.04.  Replaces
  * markVisible / checkFrustum (rasterize_points.cu:203-221,
  * rasterizer_impl.cu:173-202).  present is [P] bytes (0/1). */
@@ -209,11 +240,16 @@ GSPARC_API int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float
  * gsparc_rasterize_backward with gsparc_shared_mlp_backward.
  * params: flat fp32, per layer W [out, in] row-major then b [out].
  * workspace: gsparc_shared_mlp_workspace_floats floats; the forward keeps
- * what the backward needs there.  out must be 1.
+ * what the backward needs there.
+ * out: 1 (the signal of gsparc_rasterize_render), or up to 64 amplitude
+ * channels for gsparc_rasterize_render_channels: then the first R*P*out floats
+ * of the workspace hold features [R,P,out] = sigmoid(outputs) after the forward
+ * and the geometry arena's signal is not written (FP32 only).
  * precision GSPARC_MLP_FP32: SIMT FP32 layers (any width 8..256, 1-6
- * layers).  GSPARC_MLP_BF16: BF16 operands on the tcgen05 tensor cores with
- * FP32 accumulation (width 128, 1-3 layers); the forward and the backward
- * are one fused kernel each.  image_state (optional) receives the error bit
+ * layers; width 64 with one output and 1-2 layers runs fused kernels).
+ * GSPARC_MLP_BF16: BF16 operands on the tcgen05 tensor cores with FP32
+ * accumulation (width 128, 1-3 layers, one output); the forward and the
+ * backward are one fused kernel each.  image_state (optional) receives the error bit
  * of a bounded tensor-core wait that gave up. */
 #define GSPARC_ACT_RELU 1
 #define GSPARC_ACT_GELU 2
@@ -228,8 +264,10 @@ GSPARC_API int gsparc_shared_mlp_forward(int P, int R, int layers, int width, in
                                          int precision, const float* means3D, const float* rx_pos,
                                          const float* params, void* geom_state, void* image_state,
                                          float* workspace, void* stream);
-/* dL_dsignal [R,P,2] as gsparc_rasterize_backward returns it; dL_dparams is
- * overwritten; dL/dmeans3D through the features is ADDED to dL_dmeans3D. */
+/* dL_dsignal [R,P,2] as gsparc_rasterize_backward returns it (out = 1), or
+ * dL_dfeatures [R,P,out] from gsparc_rasterize_backward_channels (out > 1);
+ * dL_dparams is overwritten; dL/dmeans3D through the features is ADDED to
+ * dL_dmeans3D. */
 GSPARC_API int gsparc_shared_mlp_backward(int P, int R, int layers, int width, int act, int out,
                                           int precision, const float* means3D, const float* rx_pos,
                                           const float* params, const void* geom_state, void* image_state,

@@ -731,3 +731,134 @@ def render_backward(fwd, means, scales, rots, opac, mlp, view, tx, rx, dL_dout, 
     return dict(dL_dmeans2D=dmean2, dL_dmeans3D=dmean3_geo + dmean3_mlp, dL_dmlp=dmlp,
                 dL_dopacity=dopac.reshape(-1, 1), dL_dcov3D=dcov, dL_dscales=dscale,
                 dL_drotations=drot, dL_dconic=dconic, dL_dsignal=dsig)
+
+
+# ---- multi-channel blend (this implementation's C-channel extension; the
+# reference renders one channel, NUM_CHANNELS 1 in config.h) ----------------
+def blend_forward_channels(ranges, point_list, means2D, conic_opacity, features, H, W,
+                           tile_h=16, tile_w=16, dtype=np.float32, wrap=False):
+    """renderCUDA's front-to-back walk (forward.cu:151-249) with C amplitude
+    channels per Gaussian (features [P,C]): the same skip / termination
+    decisions as blend_forward, and out[c] += features[g,c] * (alpha * T).
+
+    Returns out [C,H,W], final_T [H,W], n_contrib [H,W] (uint32)."""
+    dt = np.dtype(dtype)
+    gx = (W + tile_w - 1) // tile_w
+    C = features.shape[1]
+    out = np.zeros((C, H, W), dtype=dt)
+    final_T = np.ones((H, W), dtype=dt)
+    n_contrib = np.zeros((H, W), dtype=np.uint32)
+    xy = means2D.astype(dt)
+    co = conic_opacity.astype(dt)
+    ft = features.astype(dt)
+    thr = _c(dt, 1.0) / _c(dt, 255.0)
+    for tile in range(ranges.shape[0]):
+        s, e = int(ranges[tile, 0]), int(ranges[tile, 1])
+        yy, xx = _tile_pixels(tile, gx, H, W, tile_h, tile_w)
+        if yy.size == 0:
+            continue
+        pxf, pyf = xx.astype(dt), yy.astype(dt)
+        tcol = tile % gx
+        T = np.ones(yy.size, dtype=dt)
+        acc = np.zeros((C, yy.size), dtype=dt)
+        last = np.zeros(yy.size, dtype=np.int64)
+        done = np.zeros(yy.size, dtype=bool)
+        with np.errstate(all="ignore"):
+            for j in range(s, e):
+                if done.all():
+                    break
+                g = int(point_list[j])
+                xg = xy[g, 0] + wrap_shift(xy[g, 0], tcol, tile_w, W, dt) if wrap else xy[g, 0]
+                dx = xg - pxf
+                dy = xy[g, 1] - pyf
+                c = co[g]
+                power = _c(dt, -0.5) * (c[0] * dx * dx + c[2] * dy * dy) - c[1] * dx * dy
+                alpha = np.minimum(_c(dt, 0.99), c[3] * np.exp(power))
+                ok = (~done) & (power <= 0) & (alpha >= thr)
+                test_T = T * (_c(dt, 1) - alpha)
+                stop = ok & (test_T < _c(dt, 1e-4))
+                done |= stop
+                ok &= ~stop
+                w = alpha * T
+                acc = np.where(ok[None], acc + ft[g][:, None] * w[None], acc)
+                T = np.where(ok, test_T, T)
+                last = np.where(ok, j - s + 1, last)
+        out[:, yy, xx] = acc
+        final_T[yy, xx] = T
+        n_contrib[yy, xx] = last
+    return out, final_T, n_contrib
+
+
+def blend_backward_channels(ranges, point_list, means2D, conic_opacity, features, final_T, n_contrib,
+                            dL_dout, H, W, tile_h=16, tile_w=16, dtype=np.float32, wrap=False):
+    """Adjoint of blend_forward_channels (the true derivative: the 0.99 alpha
+    clamp blocks the gradient).  Back to front from each pixel's contributor
+    count, recomputing T by division from the saved final T.  The colour
+    behind entry j, sum_{k>j} f_k alpha_k T_k / T_{j+1}, enters only through
+    its dot product with dL/dout, so one scalar per pixel carries it:
+    B += alpha_j T_j (f_j . g), and dL/dalpha_j = T_j (f_j . g - B / T_{j+1}).
+
+    dL_dout [C,H,W].  Returns (dL_dmeans2D [P,3], dL_dconic [P,4] (slots x, y,
+    -, w), dL_dopacity [P], dL_dfeatures [P,C])."""
+    dt = np.dtype(dtype)
+    P, C = features.shape
+    gx = (W + tile_w - 1) // tile_w
+    xy = means2D.astype(dt)
+    co = conic_opacity.astype(dt)
+    ft = features.astype(dt)
+    dmean = np.zeros((P, 3), dtype=dt)
+    dconic = np.zeros((P, 4), dtype=dt)
+    dopac = np.zeros(P, dtype=dt)
+    dfeat = np.zeros((P, C), dtype=dt)
+    thr = _c(dt, 1.0) / _c(dt, 255.0)
+    hw, hh = _c(dt, 0.5 * W), _c(dt, 0.5 * H)
+    one = _c(dt, 1)
+    for tile in range(ranges.shape[0]):
+        s, e = int(ranges[tile, 0]), int(ranges[tile, 1])
+        yy, xx = _tile_pixels(tile, gx, H, W, tile_h, tile_w)
+        if yy.size == 0 or e <= s:
+            continue
+        pxf, pyf = xx.astype(dt), yy.astype(dt)
+        tcol = tile % gx
+        T = final_T[yy, xx].astype(dt)
+        last_c = n_contrib[yy, xx].astype(np.int64)
+        g = dL_dout[:, yy, xx].astype(dt)            # [C, px]
+        B = np.zeros(yy.size, dtype=dt)
+        with np.errstate(all="ignore"):
+            for j in range(e - 1, s - 1, -1):
+                pos = j - s
+                act = pos < last_c
+                if not act.any():
+                    continue
+                gi = int(point_list[j])
+                xg = xy[gi, 0] + wrap_shift(xy[gi, 0], tcol, tile_w, W, dt) if wrap else xy[gi, 0]
+                dx = xg - pxf
+                dy = xy[gi, 1] - pyf
+                c = co[gi]
+                power = _c(dt, -0.5) * (c[0] * dx * dx + c[2] * dy * dy) - c[1] * dx * dy
+                G = np.exp(power)
+                a_raw = c[3] * G
+                alpha = np.minimum(_c(dt, 0.99), a_raw)
+                ok = act & (power <= 0) & (alpha >= thr)
+                if not ok.any():
+                    continue
+                Tn = np.where(ok, T / (one - alpha), T)
+                fg = (ft[gi][:, None] * g).sum(0, dtype=dt)
+                da = (fg - B / T) * Tn
+                da = np.where(a_raw > _c(dt, 0.99), _c(dt, 0), da)
+                w = np.where(ok, alpha * Tn, _c(dt, 0))
+                dfeat[gi] += (g * w[None]).sum(1, dtype=dt)
+                dG = c[3] * da
+                gdx = G * dx
+                gdy = G * dy
+                dGdx = -gdx * c[0] - gdy * c[1]
+                dGdy = -gdy * c[2] - gdx * c[1]
+                dmean[gi, 0] += np.sum(np.where(ok, dG * dGdx * hw, 0), dtype=dt)
+                dmean[gi, 1] += np.sum(np.where(ok, dG * dGdy * hh, 0), dtype=dt)
+                dconic[gi, 0] += np.sum(np.where(ok, _c(dt, -0.5) * gdx * dx * dG, 0), dtype=dt)
+                dconic[gi, 1] += np.sum(np.where(ok, _c(dt, -0.5) * gdx * dy * dG, 0), dtype=dt)
+                dconic[gi, 3] += np.sum(np.where(ok, _c(dt, -0.5) * gdy * dy * dG, 0), dtype=dt)
+                dopac[gi] += np.sum(np.where(ok, G * da, 0), dtype=dt)
+                B = np.where(ok, B + w * fg, B)
+                T = Tn
+    return dmean, dconic, dopac, dfeat

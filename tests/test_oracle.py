@@ -311,3 +311,48 @@ def test_seam_wrap_makes_the_render_invariant_to_a_half_turn_in_azimuth():
     c1 = R.render(means[far], scales[far], q[far], opac[far], None, view, tx, rx, H, W, dtype=np.float32,
                   signal_fn=fn2, wrap=True)
     assert np.array_equal(c0["keys"], c1["keys"]) and np.array_equal(c0["out"], c1["out"])
+
+
+def test_multichannel_blend_adjoint_matches_fd_and_single_channel():
+    """oracle/raster.blend_*_channels: with one channel (dL/dout zero on the
+    others) it equals the exact single-channel forward and adjoint; its
+    feature and opacity gradients match FP64 central differences (h = 1e-6)
+    to 1e-6 relative."""
+    from oracle import raster as R
+    rng = np.random.default_rng(0)
+    H, W, P, C = 32, 64, 60, 3
+    m2 = np.stack([rng.uniform(0, W, P), rng.uniform(0, H, P)], 1)
+    a, c = rng.uniform(0.02, 0.2, P), rng.uniform(0.02, 0.2, P)
+    b = rng.uniform(-0.5, 0.5, P) * np.sqrt(a * c)
+    co = np.stack([a, b, c, rng.uniform(0.3, 0.9, P)], 1)
+    depth = rng.uniform(1, 5, P).astype(np.float32)
+    _, vals, ranges = R.bin_and_sort(m2.astype(np.float32), depth, np.full(P, 12, np.int32), H, W)
+    f = rng.uniform(0, 1, (P, C))
+    out, fT, nc = R.blend_forward_channels(ranges, vals, m2, co, f, H, W, dtype=np.float64)
+    sig = np.stack([f[:, 0], np.zeros(P)], 1)
+    o1, fT1, nc1 = R.blend_forward(ranges, vals, m2, co, sig, H, W, dtype=np.float64)
+    assert np.abs(o1[0] - out[0]).max() <= 1e-12 and np.array_equal(nc1, nc) and np.array_equal(fT1, fT)
+    g = rng.normal(size=(C, H, W))
+    g0 = g.copy()
+    g0[1:] = 0
+    dm0, dc0, do0, df0 = R.blend_backward_channels(ranges, vals, m2, co, f, fT, nc, g0, H, W, dtype=np.float64)
+    dm1, dc1, do1, ds1 = R.blend_backward(ranges, vals, m2, co, sig, fT1, nc1, np.stack([g[0], np.zeros((H, W))]),
+                                          H, W, dtype=np.float64, ref_compat=False)
+    assert np.abs(dm0 - dm1).max() <= 1e-10 and np.abs(do0 - do1).max() <= 1e-10
+    assert np.abs(df0[:, 0] - ds1[:, 0]).max() <= 1e-10
+    dm, dc, do, df = R.blend_backward_channels(ranges, vals, m2, co, f, fT, nc, g, H, W, dtype=np.float64)
+    L = lambda o: (o * g).sum()
+    h = 1e-6
+    for k, ch in [(3, 1), (10, 2), (25, 0)]:
+        fp, fm = f.copy(), f.copy()
+        fp[k, ch] += h
+        fm[k, ch] -= h
+        fd = (L(R.blend_forward_channels(ranges, vals, m2, co, fp, H, W, dtype=np.float64)[0]) -
+              L(R.blend_forward_channels(ranges, vals, m2, co, fm, H, W, dtype=np.float64)[0])) / (2 * h)
+        assert abs(fd - df[k, ch]) <= 1e-6 * max(1.0, abs(fd))
+        cp, cm = co.copy(), co.copy()
+        cp[k, 3] += h
+        cm[k, 3] -= h
+        fd = (L(R.blend_forward_channels(ranges, vals, m2, cp, f, H, W, dtype=np.float64)[0]) -
+              L(R.blend_forward_channels(ranges, vals, m2, cm, f, H, W, dtype=np.float64)[0])) / (2 * h)
+        assert abs(fd - do[k]) <= 1e-6 * max(1.0, abs(fd))
