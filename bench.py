@@ -33,6 +33,9 @@ and per-kernel device times (eager runs of the same step; graph replays
 bypass the library's event hooks).
 N > 1: one process per GPU (torchrun), receivers sharded, Gaussians
 replicated, gradients all-reduced over NCCL every step (weak scaling).
+cfg4_multichannel: 100,000 Gaussians, 16 receivers x 64 frequency channels per
+step: the shared MLP's 64 outputs are the amplitudes of a 64-channel blend,
+the loss runs over the 1,024 spectra; spectra/s of the graph-captured step.
 --impl reference: the CPU restatement of the same step (oracle/) on the
 host, rank 0 only.
 """
@@ -60,6 +63,8 @@ SHARED_CFG1 = dict(layers=2, width=64, act="relu")    # emission MLP of configs 
 SHARED_CFG3 = dict(layers=3, width=128, act="gelu")   # emission MLP of config 3
 P_CFG2, R_CFG2 = 50000, 64
 P_CFG3, R_CFG3 = 200000, 32
+P_CFG4, R_CFG4, C_CFG4 = 100000, 16, 64
+SHARED_CFG4 = dict(layers=3, width=128, act="gelu", out=C_CFG4)   # 64 amplitudes, one per frequency bin
 WORKLOAD = ("cfg1_train_20k: per-receiver training step (forward + L1/SSIM/confidence loss + hand-written adjoint "
             "+ Adam), P=20000 Gaussians uniform in a 10x8x3 m room, one 90x360 spectrum per step, 16x16 tiles, "
             "shared emission MLP 2x64 ReLU from [position PE, rx-relative direction, 1/d^2] to 1 amplitude, FP32")
@@ -429,6 +434,36 @@ def run_ours(args):
             "speedup_spectra_per_s": bf_sps / plain_sps,
             "delta_ssim_bf16_vs_fp32": dssim}
 
+    # ---- 100,000 Gaussians, 16 receivers x 64 frequency bins per step (multi-channel render)
+    del d3, sc3
+    torch.cuda.empty_cache()
+    sc4 = scenes.make_scene(P_CFG4, scenes.SEED_SCENE)
+    tg4 = scenes.make_scene(P_CFG4, scenes.SEED_TARGET)
+    rx4 = scenes.make_receivers(R_CFG4 * world)[rank * R_CFG4:(rank + 1) * R_CFG4]
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
+    v4, r4 = t(scenes.view_matrices(rx4)), t(rx4)
+    with torch.no_grad():   # targets: the second scene rendered through a seeded 64-output MLP
+        tm, ts, tq, to = tg4.activated()
+        tmlp = SharedMLP(**SHARED_CFG4)
+        t4, _, _ = raster.forward_channels(t(tm), t(to.reshape(-1)), t(ts), t(tq), 90, 360, 1.0, v4, tx, r4, tmlp,
+                                           tmlp.init_params(seed=7, device=dev))
+        t4 = t4.clone()
+        del tmlp
+    tr4 = FusedTrainer(sc4, device=dev, group=group, shared=SharedMLP(**SHARED_CFG4))
+    cap4 = tr4.probe_capacity(v4, r4, tx) * R_CFG4
+    tr4.capture(R_CFG4, cap4, tx, v4, r4, t4)
+    n4 = max(3, args.steps // 40)
+    sec4 = timed(lambda i: tr4.step(v4, r4, t4), n4)
+    K4, _ = tr4.plan.host_status()
+    tr4.plan.check()
+    cfg4 = {"workload": f"cfg4: P={P_CFG4}, {R_CFG4} receivers x {C_CFG4} frequency channels per step, shared "
+                        "emission MLP 3x128 GELU -> 64 amplitudes (FP32), multi-channel FP32 blend, loss over "
+                        "R*C spectra, training step with adjoint, CUDA graph",
+            "instances_K": K4, "steps_per_s": n4 * world / sec4,
+            "spectra_per_s": n4 * R_CFG4 * C_CFG4 * world / sec4}
+    del tr4
+    torch.cuda.empty_cache()
+
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle.train_step import OracleTrainer
@@ -456,6 +491,7 @@ def run_ours(args):
                 "kernel_ms_per_step": {k: v[0] / n_eager for k, v in sorted(ktimes.items())},
                 "cfg2_batched_clustered_autotuned": cfg2,
                 "cfg3_batched_bf16_vs_plain_fp32": cfg3,
+                "cfg4_multichannel": cfg4,
                 "reference_mlp_steps_per_s": n_ref * world / ref_sec,
                 "dropin_eager_steps_per_s": dropin,
                 "batched": batched16,

@@ -117,6 +117,8 @@ class FusedTrainer:
         self.lr6 = torch.tensor(lr, dtype=torch.float32, device=dev)
         self.lo3 = torch.tensor(scenes.ROOM_LO, dtype=torch.float32, device=dev)
         self.hi3 = torch.tensor(scenes.ROOM_HI, dtype=torch.float32, device=dev)
+        # amplitude channels per spectrum: the shared MLP's outputs (one = the signal path)
+        self.channels = 1 if shared is None else int(shared.out)
         self.graph = None
         self.plan = None
         self._R = None
@@ -140,12 +142,39 @@ class FusedTrainer:
         self._radii = torch.empty((R, P), dtype=torch.int32, device=dev)
         self._zero_imag = torch.zeros((R, self.H, self.W), dtype=torch.float32, device=dev)
         self._scratch = dict(dmeans2D=z(R, P, 3), dconic=z(R, P, 4), dsignal=z(R, P, 2), dcov3D=z(P, 6))
-        self._lossfn = SplatLoss(R, self.H, self.W, self.conf_hidden, dev, self.lambda1, self.confidence_alpha)
+        C = self.channels
+        if C > 1:   # R x C spectra; the loss sees R*C spectra, each with its receiver's position
+            self._out_mc = z(R, C, self.H, self.W)
+            self._scratch = dict(dmeans2D=z(R, P, 3), dconic=z(R, P, 4), dfeatures=z(R, P, C), dcov3D=z(P, 6))
+            self._rep_idx = torch.arange(R, device=dev).repeat_interleave(C)
+            self._rx_rep = z(R * C, 3)
+        self._lossfn = SplatLoss(R * C, self.H, self.W, self.conf_hidden, dev, self.lambda1, self.confidence_alpha)
         self._R = R
+
+    def _body_channels(self, views, rxs, tx, targets):
+        plan = self.plan
+        R, C, H, W = plan.R, self.channels, self.H, self.W
+        out, _, st = raster.forward_channels(
+            self.centre, self.act_opac, self.act_scales, self.act_rots, H, W, 1.0, views, tx, rxs, self.shared,
+            self.mlp, tile=plan.tile, capacity=plan.capacity, binning=plan.binning, out=self._out_mc,
+            radii=self._radii, geom=plan.geom, image=plan.image, wrap=plan.wrap)
+        plan.record_status()
+        torch.index_select(rxs, 0, self._rep_idx, out=self._rx_rep)
+        loss, dpred = self._lossfn(out.view(R * C, H, W), targets.reshape(R * C, H, W), self._rx_rep,
+                                   self.conf_params, self.conf_grads)
+        bo = dict(self._scratch, dmeans3D=self.gout["dmeans3D"], dscales=self.gout["dscales"],
+                  drotations=self.gout["drotations"], dopacity=self.gout["dopacity"], dshared=self.gout["dmlp"])
+        raster.backward_channels(st, self.centre, self.act_scales, self.act_rots, 1.0, views, tx, rxs,
+                                 dpred.view(R, C, H, W), self.shared, self.mlp, out=bo)
+        return loss
 
     def _body(self, views, rxs, tx, targets):
         plan = self.plan
         self._buffers(plan.R)
+        if self.channels > 1:
+            loss = self._body_channels(views, rxs, tx, targets)
+            self._reduce_and_adam()
+            return loss
         out_r, _, _, st = raster.forward(
             self.centre, self._mlp_arg(), self.act_opac, self.act_scales, self.act_rots, self.H, self.W, 1.0, views, tx,
             rxs, tile=plan.tile, capacity=plan.capacity, binning=plan.binning, geom=plan.geom, image=plan.image,
@@ -156,6 +185,10 @@ class FusedTrainer:
         raster.backward(st, self.centre, self._mlp_arg(), self.act_scales, self.act_rots, 1.0, views, tx, rxs,
                         dpred, self._zero_imag, grad_mode=self.grad_mode, out=self._bwd_out(),
                         **self._shared_kw())
+        self._reduce_and_adam()
+        return loss
+
+    def _reduce_and_adam(self):
         if self.group is not None:
             import torch.distributed as dist
             dist.all_reduce(self.grads, op=dist.ReduceOp.SUM, group=self.group)
@@ -164,7 +197,6 @@ class FusedTrainer:
             self.P, self.n_mlp, self.n_conf, ptr(self.params), ptr(self.grads), ptr(self.exp_avg), ptr(self.exp_avg_sq),
             ptr(self.step_count), ptr(self.lr6), b1, b2, self.eps, ptr(self.lo3), ptr(self.hi3),
             ptr(self.act_scales), ptr(self.act_rots), ptr(self.act_opac), stream_of(self.device)))
-        return loss
 
     def _mlp_arg(self):
         return self.mlp if self.shared is None else None
@@ -190,6 +222,12 @@ class FusedTrainer:
         kmax = 0
         with torch.no_grad():
             for r in range(views.shape[0]):
+                if self.channels > 1:
+                    _, _, st = raster.forward_channels(self.centre, self.act_opac, self.act_scales, self.act_rots,
+                                                       self.H, self.W, 1.0, views[r], tx, rxs[r], self.shared,
+                                                       self.mlp, tile=tile, wrap=self.wrap)
+                    kmax = max(kmax, st.num_rendered)
+                    continue
                 _, _, _, st = raster.forward(self.centre, self._mlp_arg(), self.act_opac, self.act_scales,
                                              self.act_rots, self.H, self.W, 1.0, views[r], tx, rxs[r], tile=tile,
                                              wrap=self.wrap, **self._shared_kw())
@@ -213,7 +251,8 @@ class FusedTrainer:
         self._s_views = torch.eye(4, device=dev).repeat(R, 1, 1).contiguous()
         self._s_rxs = torch.zeros((R, 3), device=dev)
         self._s_tx = tx.detach().clone().reshape(3)
-        self._s_targets = torch.zeros((R, self.H, self.W), device=dev)
+        self._s_targets = torch.zeros((R, self.H, self.W) if self.channels == 1 else
+                                      (R, self.channels, self.H, self.W), device=dev)
         if views is not None:
             self._s_views.copy_(views.reshape(self._s_views.shape))
             self._s_rxs.copy_(rxs.reshape(self._s_rxs.shape))
