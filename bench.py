@@ -34,7 +34,8 @@ bypass the library's event hooks).
 N > 1: one process per GPU (torchrun), receivers sharded, Gaussians
 replicated, gradients all-reduced over NCCL every step (weak scaling).
 cfg4_multichannel: 100,000 Gaussians, 16 receivers x 64 frequency channels per
-step: the shared MLP's 64 outputs are the amplitudes of a 64-channel blend,
+step: the shared MLP's 64 outputs (BF16 on the tensor cores) are the
+amplitudes of a 64-channel FP32 blend,
 the loss runs over the 1,024 spectra; spectra/s of the graph-captured step.
 --impl reference: the CPU restatement of the same step (oracle/) on the
 host, rank 0 only.
@@ -64,7 +65,7 @@ SHARED_CFG3 = dict(layers=3, width=128, act="gelu")   # emission MLP of config 3
 P_CFG2, R_CFG2 = 50000, 64
 P_CFG3, R_CFG3 = 200000, 32
 P_CFG4, R_CFG4, C_CFG4 = 100000, 16, 64
-SHARED_CFG4 = dict(layers=3, width=128, act="gelu", out=C_CFG4)   # 64 amplitudes, one per frequency bin
+SHARED_CFG4 = dict(layers=3, width=128, act="gelu", out=C_CFG4, precision="bf16")   # 64 amplitudes, one per bin
 WORKLOAD = ("cfg1_train_20k: per-receiver training step (forward + L1/SSIM/confidence loss + hand-written adjoint "
             "+ Adam), P=20000 Gaussians uniform in a 10x8x3 m room, one 90x360 spectrum per step, 16x16 tiles, "
             "shared emission MLP 2x64 ReLU from [position PE, rx-relative direction, 1/d^2] to 1 amplitude, FP32")
@@ -457,7 +458,7 @@ def run_ours(args):
     K4, _ = tr4.plan.host_status()
     tr4.plan.check()
     cfg4 = {"workload": f"cfg4: P={P_CFG4}, {R_CFG4} receivers x {C_CFG4} frequency channels per step, shared "
-                        "emission MLP 3x128 GELU -> 64 amplitudes (FP32), multi-channel FP32 blend, loss over "
+                        "emission MLP 3x128 GELU -> 64 amplitudes (BF16 on tcgen05), multi-channel FP32 blend, loss over "
                         "R*C spectra, training step with adjoint, CUDA graph",
             "instances_K": K4, "steps_per_s": n4 * world / sec4,
             "spectra_per_s": n4 * R_CFG4 * C_CFG4 * world / sec4}

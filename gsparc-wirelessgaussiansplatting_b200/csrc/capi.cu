@@ -420,8 +420,8 @@ int check_mlp_spec(int layers, int width, int act, int out, int precision) {
   if (act != GSPARC_ACT_RELU && act != GSPARC_ACT_GELU) return invalid("act must be GSPARC_ACT_RELU or _GELU");
   if (out < 1 || out > kMaxChannels) return invalid("out must be in [1, 64]");
   if (precision != GSPARC_MLP_FP32 && precision != GSPARC_MLP_BF16) return invalid("precision");
-  if (precision == GSPARC_MLP_BF16 && (width != 128 || layers > 3 || out != 1))
-    return invalid("the BF16 tensor-core path needs width 128, at most 3 hidden layers and one output");
+  if (precision == GSPARC_MLP_BF16 && (width != 128 || layers > 3 || (out != 1 && out != 64)))
+    return invalid("the BF16 tensor-core path needs width 128, at most 3 hidden layers and 1 or 64 outputs");
   return GSPARC_OK;
 }
 }  // namespace
@@ -433,7 +433,7 @@ size_t gsparc_shared_mlp_param_floats(int layers, int width, int out) {
 
 size_t gsparc_shared_mlp_workspace_floats(int P, int R, int layers, int width, int out, int precision) {
   if (P < 0 || R < 0 || layers < 1 || layers > kMaxMlpLayers || width < 1 || out < 1) return 0;
-  if (precision == GSPARC_MLP_BF16) return shared_mlp_layout_bf16(layers, (size_t)P * R).work;
+  if (precision == GSPARC_MLP_BF16) return shared_mlp_layout_bf16(layers, (size_t)P * R, out).work;
   return shared_mlp_layout(layers, width, out, (size_t)P * R).work;
 }
 
@@ -450,7 +450,7 @@ int gsparc_shared_mlp_forward(int P, int R, int layers, int width, int act, int 
   carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
   Timed t(KID_SHARED_MLP, s);
   if (precision == GSPARC_MLP_BF16) {
-    GS_CHECK(launch_shared_mlp_bf16(true, P, R, layers, act, means3D, rx_pos, params, geo, workspace, nullptr,
+    GS_CHECK(launch_shared_mlp_bf16(true, P, R, layers, act, out, means3D, rx_pos, params, geo, workspace, nullptr,
                                     nullptr, nullptr, (ImageHeader*)image_state, s),
              "shared mlp forward (bf16)");
   } else {
@@ -480,7 +480,7 @@ int gsparc_shared_mlp_backward(int P, int R, int layers, int width, int act, int
   carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
   Timed t(KID_SHARED_MLP_BWD, s);
   if (precision == GSPARC_MLP_BF16) {
-    GS_CHECK(launch_shared_mlp_bf16(false, P, R, layers, act, means3D, rx_pos, params, geo, workspace, dL_dsignal,
+    GS_CHECK(launch_shared_mlp_bf16(false, P, R, layers, act, out, means3D, rx_pos, params, geo, workspace, dL_dsignal,
                                     dL_dparams, dL_dmeans3D, (ImageHeader*)image_state, s),
              "shared mlp backward (bf16)");
   } else {

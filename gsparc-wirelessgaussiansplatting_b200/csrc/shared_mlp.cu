@@ -810,14 +810,14 @@ SharedMlpLayout shared_mlp_layout(int layers, int width, int out, size_t rows) {
   return L;
 }
 
-SharedMlpLayout shared_mlp_layout_bf16(int layers, size_t rows) {
-  SharedMlpLayout L = shared_mlp_layout(layers, 128, 1, 0);   // parameter offsets as the FP32 path
-  auto a = [](size_t x) { return (x + 63) / 64 * 64; };         // 256-byte aligned segments (vector access)
+SharedMlpLayout shared_mlp_layout_bf16(int layers, size_t rows, int out) {
+  SharedMlpLayout L = shared_mlp_layout(layers, 128, out, 0);   // parameter offsets as the FP32 path
+  auto a = [](size_t x) { return (x + 63) / 64 * 64; };           // 256-byte aligned segments (vector access)
   size_t w = 0;
+  L.s = w;   // first: the sigmoid outputs [rows][out] (the amplitudes for out > 1)
+  w += a(rows * (size_t)out);
   L.z[1] = w;
   w += a((size_t)layers * rows * 128 / 2);   // BF16 pre-activations, two per float
-  L.s = w;
-  w += a(rows);
   L.d0 = w;
   w += a(rows * kFeat);
   L.work = w;

@@ -1,8 +1,8 @@
 // Shared emission MLP in BF16 on the 5th-generation tensor cores (tcgen05).
 //
 // Same network as shared_mlp.cu (features, hidden layers of width 128,
-// sigmoid of one output) with BF16 operands and FP32 accumulation in tensor
-// memory.  Two fused persistent kernels over tiles of 128 (receiver, Gaussian)
+// sigmoid of one output, or of 64 outputs whose layer is one more MMA) with
+// BF16 operands and FP32 accumulation in tensor memory.  Two fused persistent kernels over tiles of 128 (receiver, Gaussian)
 // rows, one row per thread of a 128-thread warpgroup:
 //
 //   forward:  four warpgroups per CTA, each with its own tile in flight and
@@ -185,7 +185,7 @@ __device__ __forceinline__ void group_publish(uint32_t bar_id) {
 // k = input), then per warpgroup an activation tile H [128 x 128] K-major bf16
 // whose first 8 KB also hold the feature tile X [128 x 32]; biases and the
 // output row in fp32.
-template <int kLayers, int act>
+template <int kLayers, int act, int kOut>
 __global__ void __launch_bounds__(128 * kFwdGroups, 1)
 mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                         const float* __restrict__ rx_pos, const float* __restrict__ params,
@@ -203,8 +203,11 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   }
   unsigned char* Hs = smem + off + (size_t)grp * kRows * kH * 2;
   off += (size_t)kFwdGroups * kRows * kH * 2;
-  float* bias = reinterpret_cast<float*>(smem + off);   // [kLayers][128], then w_out[128]
-  float* wout = bias + kLayers * kH;
+  float* bias = reinterpret_cast<float*>(smem + off);   // [kLayers][128], then w_out[128] + b_out (one
+  float* wout = bias + kLayers * kH;                    // output) or b_out[kOut] (kOut outputs)
+  off += (size_t)(kLayers * kH + kH + 4) * sizeof(float);
+  // kOut > 1: the output layer as an MMA, W_out K-major [kOut x 128] bf16
+  unsigned char* Wo = smem + (off + 127) / 128 * 128;
 
   size_t poff = 0;
   for (int l = 0; l < kLayers; ++l) {
@@ -222,8 +225,20 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
     for (int j = tid; j < kH; j += blockDim.x) bias[l * kH + j] = params[poff + j];
     poff += kH;
   }
-  for (int j = tid; j < kH; j += blockDim.x) wout[j] = params[poff + j];
-  const float bout = params[poff + kH];
+  float bout = 0.0f;
+  if constexpr (kOut == 1) {
+    for (int j = tid; j < kH; j += blockDim.x) wout[j] = params[poff + j];
+    bout = params[poff + kH];
+  } else {
+    for (int c = tid; c < kOut * (kH / 8); c += blockDim.x) {
+      const int n = c / (kH / 8), kc = c % (kH / 8);
+      float v[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = params[poff + (size_t)n * kH + kc * 8 + i];
+      *reinterpret_cast<uint4*>(Wo + tc::kmajor_off(n, kc * 8, kLbo, kSboH)) = pack8(v);
+    }
+    for (int j = tid; j < kOut; j += blockDim.x) wout[j] = params[poff + (size_t)kOut * kH + j];
+  }
   if (tid == 0)
     for (int q = 0; q < kFwdGroups; ++q) tc::mbar_init(&mbar[q], 1);
   if (warp == 0) tc::tmem_alloc(&tbase, kFwdGroups * kH);
@@ -287,7 +302,7 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
           unpack8(zp, zr);
 #pragma unroll
           for (int i = 0; i < 8; ++i) a[i] = actf(act, zr[i]);
-          if (l + 1 < kLayers) {
+          if (l + 1 < kLayers || kOut > 1) {
             *reinterpret_cast<uint4*>(Hs + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = pack8(a);
           } else {
 #pragma unroll
@@ -297,10 +312,42 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
       }
     }
     if (!ok) break;
-    if (valid) {
-      const float s = 1.0f / (1.0f + expf(-o));
-      S[row] = s;
-      if (vis) signal[row] = make_float2(s, 0.0f);
+    if constexpr (kOut == 1) {
+      if (valid) {
+        const float s = 1.0f / (1.0f + expf(-o));
+        S[row] = s;
+        if (vis) signal[row] = make_float2(s, 0.0f);
+      }
+    } else {
+      // output layer: [128 rows x kOut] = A_{L-1} W_out^T into the group's TMEM columns
+      group_publish(bar_id);
+      if (t == 0) {
+        const uint32_t a0 = tc::smem_u32(Hs), b0 = tc::smem_u32(Wo);
+        const uint32_t idesc = tc::idesc_bf16(kRows, kOut, false, false);
+        for (int kk = 0; kk < kH / 16; ++kk)
+          tc::mma_bf16(tmem, tc::smem_desc(a0 + kk * 2 * kLbo, kLbo, kSboH),
+                       tc::smem_desc(b0 + kk * 2 * kLbo, kLbo, kSboH), idesc, kk > 0 ? 1u : 0u);
+        tc::commit(&mbar[grp]);
+      }
+      const bool got = tc::mbar_wait(&mbar[grp], phase, kPolls);
+      phase ^= 1u;
+      tc::fence_after_sync();
+      if (!tc::named_all(bar_id, 128, got)) {
+        ok = false;
+        break;
+      }
+#pragma unroll 1
+      for (int c0 = 0; c0 < kOut; c0 += 32) {
+        float v[32];
+        tc::tmem_ld32(tmem + lane_base + c0, v);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = 1.0f / (1.0f + expf(-(v[i] + wout[c0 + i])));
+        if (valid)
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            *reinterpret_cast<float4*>(S + row * kOut + c0 + 4 * q) =
+                make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      }
     }
   }
   if (!ok && t == 0 && hdr) atomic_or_error(hdr, kErrMlpWait);
@@ -313,10 +360,16 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
 // dynamic smem: W_l as the MN-major B operand of dA = dZ W ([n = in_l] x
 // [k = 128 outputs]) for every layer; per compute warpgroup dZ [128 rows x 128]
 // and A [128 rows x 144] (activations, then a ones column and 15 zero columns),
-// both K-major by row; the output row in fp32.
+// both K-major by row; the output row in fp32 (one output) or W_out as the
+// MN-major B operand of dA = dO W_out ([n = 128] x [k = kOut]) (kOut outputs).
 // TMEM columns: dW_l accumulators of (in_l + 16) columns each (last layer
-// first), then one 128-column scratch accumulator for dA.
-template <int kLayers, int act>
+// first; with kOut outputs the first layer's bias is summed on the CUDA cores
+// and its accumulator is in_0 wide), then dW_out^T (kOut columns, lanes =
+// hidden units; kOut outputs only), then one 128-column scratch accumulator
+// for dA.  With kOut outputs every tile starts with an output step: dW_out^T +=
+// A_{L-1}^T dO and dA_{L-1} = dO W_out on the tensor cores, dO staged as a
+// K-major row tile in the dZ buffer.
+template <int kLayers, int act, int kOut>
 __global__ void __launch_bounds__(kBwdThreads, 1)
 mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                          const float* __restrict__ rx_pos, const float* __restrict__ params,
@@ -329,7 +382,11 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   __shared__ __align__(8) uint64_t bar_free;
   __shared__ uint32_t tbase;
   __shared__ int s_fail;
-  __shared__ float s_dwo[kH + 1];
+  // one output: dw_out[128], db_out; kOut outputs: db_out[kOut], db_0[128]
+  constexpr int kRed = kOut == 1 ? kH + 1 : kOut + kH;
+  __shared__ float s_red[kRed];
+  constexpr bool kMulti = kOut > 1;
+  constexpr uint32_t kSboO = (uint32_t)(kOut / 8) * 128u;   // [rows x kOut] K-major / W_out MN-major
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int grp = tid >> 7;   // compute warpgroup 0..kBwdGroups-1; kBwdGroups = the MMA warp
   const int t = tid & 127;
@@ -342,7 +399,9 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   }
   unsigned char* const groups = smem + off;
   off += kBwdGroups * kGroupBytes;
-  float* wout = reinterpret_cast<float*>(smem + off);
+  float* wout = reinterpret_cast<float*>(smem + off);   // one output: w_out[128]
+  off += (size_t)kH * sizeof(float);
+  unsigned char* const Wo = smem + off;                 // kOut outputs: W_out MN-major
 
   // W_l [out][in] -> MN-major B operand (n = in, k = out), once per CTA
   size_t poff = 0;
@@ -363,9 +422,19 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
     poff += kH;
   }
   woff[kLayers] = poff;
-  boff[kLayers] = poff + kH;
-  for (int j = tid; j < kH; j += blockDim.x) wout[j] = params[woff[kLayers] + j];
-  for (int j = tid; j <= kH; j += blockDim.x) s_dwo[j] = 0.0f;
+  boff[kLayers] = poff + (size_t)kOut * kH;
+  if constexpr (kMulti) {
+    for (int c = tid; c < kOut * (kH / 8); c += blockDim.x) {
+      const int k = c / (kH / 8), nc = c % (kH / 8);   // k = output row of W_out, nc = group of 8 hidden units
+      float v[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = params[poff + (size_t)k * kH + nc * 8 + i];
+      *reinterpret_cast<uint4*>(Wo + tc::mnmajor_off(nc * 8, k, kLbo, kSboO)) = pack8(v);
+    }
+  } else {
+    for (int j = tid; j < kH; j += blockDim.x) wout[j] = params[woff[kLayers] + j];
+  }
+  for (int j = tid; j < kRed; j += blockDim.x) s_red[j] = 0.0f;
   unsigned char* const dZ = groups + (size_t)(grp < kBwdGroups ? grp : 0) * kGroupBytes;
   unsigned char* const Ab = dZ + (size_t)kRows * kH * 2;
   if (grp < kBwdGroups) {   // the constant ones column (db) of the activation tile
@@ -387,28 +456,34 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = tbase;
+  // the first layer's accumulator has the ones columns unless kOut outputs need the room
+  auto dw_width = [](int l) { return (l == 0 ? kFin : kH) + ((l == 0 && kMulti) ? 0 : 16); };
   uint32_t dwcol[kLayers];
   uint32_t col = 0;
   for (int l = kLayers - 1; l >= 0; --l) {
     dwcol[l] = col;
-    col += (l == 0 ? kFin : kH) + 16;
+    col += dw_width(l);
   }
-  const uint32_t scratch = col;   // <= 144 + 144 + 48 = 336; the scratch needs 128 more
+  const uint32_t dwo_col = col;                       // kOut outputs: dW_out^T
+  const uint32_t scratch = col + (kMulti ? kOut : 0);  // 3 layers: 336 (+ 0) or 320 + 64 = 384; + 128 <= 512
   const size_t ntiles = (rows + kRows - 1) / kRows;
   const size_t tile_stride = (size_t)gridDim.x * kBwdGroups;
+  // steps per tile, from the top: the output step (kOut outputs), then hidden layers L-1 .. 0
+  constexpr int kTop = kMulti ? kLayers : kLayers - 1;
 
   if (grp == kBwdGroups) {
     // ---- MMA warp: one thread issues every MMA of the CTA, in the order
-    // (tile round, layer, group), so both groups' weight gradients accumulate
+    // (tile round, step, group), so both groups' weight gradients accumulate
     // into the same TMEM columns in issue order.
     if (lane == 0) {
       uint32_t ph_ready[kBwdGroups] = {};
-      bool first[kLayers];
-      for (int l = 0; l < kLayers; ++l) first[l] = true;
+      bool first[kLayers + 1];
+      for (int l = 0; l <= kLayers; ++l) first[l] = true;
       uint32_t n_da = 0;
       bool ok = true;
       for (size_t base = (size_t)blockIdx.x * kBwdGroups; base < ntiles && ok; base += tile_stride) {
-        for (int l = kLayers - 1; l >= 0 && ok; --l) {
+        for (int l = kTop; l >= 0 && ok; --l) {
+          const bool out_step = kMulti && l == kLayers;
           const int in = l == 0 ? kFin : kH;
           for (int q = 0; q < kBwdGroups; ++q) {
             if (base + q >= ntiles) break;
@@ -420,16 +495,27 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
             tc::fence_after_sync();
             const uint32_t zq = tc::smem_u32(groups + (size_t)q * kGroupBytes);
             const uint32_t aq = zq + (uint32_t)(kRows * kH * 2);
-            // dW_l | db_l += dZ^T [A | 1]: A operand dZ^T (M = outputs, K = rows) and
-            // B operand [A | 1]^T (N = in + 16, K = rows), both MN-major views of the
-            // row-major tiles (core-matrix stride 128 B along M/N, one row group along K)
-            const uint32_t id_w = tc::idesc_bf16(kH, in + 16, true, true);
-            for (int kk = 0; kk < kRows / 16; ++kk)
-              tc::mma_bf16(tmem + dwcol[l], tc::smem_desc(zq + kk * 2 * kSboH, kSboH, 128u),
-                           tc::smem_desc(aq + kk * 2 * kSboA, kSboA, 128u), id_w,
-                           (!first[l] || kk > 0) ? 1u : 0u);
-            first[l] = false;
-            // dA_{l-1} = dZ_l W_l into the scratch, once its previous reader has drained it
+            if (out_step) {
+              // dW_out^T += A_{L-1}^T dO: A operand A^T (M = hidden units, K = rows) and B operand
+              // dO^T (N = outputs, K = rows), MN-major views of the row tiles
+              const uint32_t id_o = tc::idesc_bf16(kH, kOut, true, true);
+              for (int kk = 0; kk < kRows / 16; ++kk)
+                tc::mma_bf16(tmem + dwo_col, tc::smem_desc(aq + kk * 2 * kSboA, kSboA, 128u),
+                             tc::smem_desc(zq + kk * 2 * kSboO, kSboO, 128u), id_o,
+                             (!first[kLayers] || kk > 0) ? 1u : 0u);
+              first[kLayers] = false;
+            } else {
+              // dW_l | db_l += dZ^T [A | 1]: A operand dZ^T (M = outputs, K = rows) and
+              // B operand [A | 1]^T (N = in (+ 16), K = rows), both MN-major views of the
+              // row-major tiles (core-matrix stride 128 B along M/N, one row group along K)
+              const uint32_t id_w = tc::idesc_bf16(kH, dw_width(l), true, true);
+              for (int kk = 0; kk < kRows / 16; ++kk)
+                tc::mma_bf16(tmem + dwcol[l], tc::smem_desc(zq + kk * 2 * kSboH, kSboH, 128u),
+                             tc::smem_desc(aq + kk * 2 * kSboA, kSboA, 128u), id_w,
+                             (!first[l] || kk > 0) ? 1u : 0u);
+              first[l] = false;
+            }
+            // dA = dZ_l W_l (or dO W_out) into the scratch, once its previous reader has drained it
             if (n_da > 0) {
               if (!tc::mbar_wait(&bar_free, (n_da - 1) & 1u, kPolls)) {
                 ok = false;
@@ -437,11 +523,19 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
               }
               tc::fence_after_sync();
             }
-            const uint32_t id_x = tc::idesc_bf16(kRows, in, false, true);
-            const uint32_t wb = tc::smem_u32(Wb[l]);
-            for (int kk = 0; kk < kH / 16; ++kk)
-              tc::mma_bf16(tmem + scratch, tc::smem_desc(zq + kk * 2 * kLbo, kLbo, kSboH),
-                           tc::smem_desc(wb + kk * 2 * kLbo, kLbo, kSboH), id_x, kk > 0 ? 1u : 0u);
+            if (out_step) {
+              const uint32_t id_x = tc::idesc_bf16(kRows, kH, false, true);
+              const uint32_t wo = tc::smem_u32(Wo);
+              for (int kk = 0; kk < kOut / 16; ++kk)
+                tc::mma_bf16(tmem + scratch, tc::smem_desc(zq + kk * 2 * kLbo, kLbo, kSboO),
+                             tc::smem_desc(wo + kk * 2 * kLbo, kLbo, kSboO), id_x, kk > 0 ? 1u : 0u);
+            } else {
+              const uint32_t id_x = tc::idesc_bf16(kRows, in, false, true);
+              const uint32_t wb = tc::smem_u32(Wb[l]);
+              for (int kk = 0; kk < kH / 16; ++kk)
+                tc::mma_bf16(tmem + scratch, tc::smem_desc(zq + kk * 2 * kLbo, kLbo, kSboH),
+                             tc::smem_desc(wb + kk * 2 * kLbo, kLbo, kSboH), id_x, kk > 0 ? 1u : 0u);
+            }
             ++n_da;
             tc::commit(&bar_done[q]);
           }
@@ -468,16 +562,39 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
           const size_t r1 = nt * kRows;
           const uint32_t n1 = (uint32_t)(rows - r1 < (size_t)kRows ? rows - r1 : (size_t)kRows);
           tc::prefetch_l2(zb + (size_t)(kLayers - 1) * rows * kH + r1 * kH, n1 * kH * 2);
-          tc::prefetch_l2(S + r1, n1 * 4);
+          tc::prefetch_l2(S + r1 * kOut, n1 * 4 * kOut);
           tc::prefetch_l2(radii + r1, n1 * 4);
-          tc::prefetch_l2(dL_dsignal + 2 * r1, n1 * 8);
+          tc::prefetch_l2(dL_dsignal + (kMulti ? r1 * kOut : 2 * r1), n1 * (kMulti ? 4 * kOut : 8));
         }
       }
       const bool vis = valid && radii[row] > 0;
-      // output layer: dO, its weight gradient (reduced over the warp's rows), dZ of the last hidden layer
-      const float s = valid ? S[row] : 0.0f;
-      const float dO = vis ? dL_dsignal[2 * row] * s * (1.0f - s) : 0.0f;
-      {
+      if constexpr (kMulti) {
+        // dO = dL/dfeatures * s (1 - s) -> the dO row tile (BF16) in the dZ buffer; db_out
+#pragma unroll 1
+        for (int c0 = 0; c0 < kOut; c0 += 32) {
+          float d[32];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            float4 sv = make_float4(0.f, 0.f, 0.f, 0.f), gv = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (vis) {
+              sv = *reinterpret_cast<const float4*>(S + row * kOut + c0 + 4 * q);
+              gv = *reinterpret_cast<const float4*>(dL_dsignal + row * kOut + c0 + 4 * q);
+            }
+            d[4 * q] = gv.x * sv.x * (1.0f - sv.x);
+            d[4 * q + 1] = gv.y * sv.y * (1.0f - sv.y);
+            d[4 * q + 2] = gv.z * sv.z * (1.0f - sv.z);
+            d[4 * q + 3] = gv.w * sv.w * (1.0f - sv.w);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboO)) = pack8(d + q * 8);
+          const float sum = warp_transpose_sum32(d, lane);
+          atomicAdd(&s_red[c0 + lane], sum);
+        }
+      } else {
+        // output layer: dO, its weight gradient (reduced over the warp's rows), dZ of the last hidden layer
+        const float s = valid ? S[row] : 0.0f;
+        const float dO = vis ? dL_dsignal[2 * row] * s * (1.0f - s) : 0.0f;
         const uint4* zl = reinterpret_cast<const uint4*>(zb + (size_t)(kLayers - 1) * rows * kH + row * kH);
 #pragma unroll 1
         for (int c0 = 0; c0 < kH; c0 += 32) {
@@ -499,14 +616,14 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
             *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = pack8(dz);
           }
           const float sum = warp_transpose_sum32(red, lane);
-          atomicAdd(&s_dwo[c0 + lane], sum);
+          atomicAdd(&s_red[c0 + lane], sum);
         }
         float dsum = dO;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
-        if (lane == 0) atomicAdd(&s_dwo[kH], dsum);
+        if (lane == 0) atomicAdd(&s_red[kH], dsum);
       }
-      for (int l = kLayers - 1; l >= 0; --l) {
+      for (int l = kTop; l >= 0; --l) {
         // act'(Z_{l-1}) of this row, kept for dZ_{l-1} after the MMAs as FP16 pairs
         // (nine warps leave 168 registers a thread; the FP16 rounding, 2^-11
         // relative, sits below the BF16 rounding of dZ that follows)
@@ -520,9 +637,11 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
 #pragma unroll
           for (int kc = 0; kc < kFin / 8; ++kc)
             *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kc * 8, kLbo, kSboA)) = pack8(x + kc * 8);
-          *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kFin, kLbo, kSboA)) =
-              make_uint4(pack2(1.0f, 0.0f), 0u, 0u, 0u);
-          *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kFin + 8, kLbo, kSboA)) = make_uint4(0u, 0u, 0u, 0u);
+          if constexpr (!kMulti) {
+            *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kFin, kLbo, kSboA)) =
+                make_uint4(pack2(1.0f, 0.0f), 0u, 0u, 0u);
+            *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kFin + 8, kLbo, kSboA)) = make_uint4(0u, 0u, 0u, 0u);
+          }
         } else {
           const __nv_bfloat16* zp = zb + (size_t)(l - 1) * rows * kH + row * kH;
 #pragma unroll
@@ -540,7 +659,7 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
             *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, c0, kLbo, kSboA)) = pack8(a);
           }
         }
-        // hand dZ_l and A_{l-1} to the MMA warp
+        // hand dZ_l (or dO) and A_{l-1} to the MMA warp
         tc::fence_async_smem();
         tc::mbar_arrive(&bar_ready[grp]);
         const bool got = tc::mbar_wait(&bar_done[grp], ph_done, kPolls);
@@ -561,7 +680,7 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
               *reinterpret_cast<float4*>(dX0 + row * kFin + q * 4) =
                   make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
         } else {
-          // dZ_{l-1} = dA_{l-1} * act'(Z_{l-1}); the MMAs that read dZ_l are done
+          // dZ_{l-1} = dA_{l-1} * act'(Z_{l-1}); the MMAs that read dZ_l (or dO) are done
 #pragma unroll
           for (int c0 = 0; c0 < kH; c0 += 32) {
             float v[32];
@@ -577,8 +696,15 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
               v[2 * i + 1] *= d.y;
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-              *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = pack8(v + q * 8);
+            for (int q = 0; q < 4; ++q) {
+              const uint4 p = pack8(v + q * 8);
+              *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = p;
+              if (kMulti && l == 1) unpack8(p, v + q * 8);   // db_0 sums the BF16 dZ_0 the MMAs see
+            }
+            if (kMulti && l == 1) {
+              const float sum = warp_transpose_sum32(v, lane);
+              atomicAdd(&s_red[kOut + c0 + lane], sum);
+            }
           }
         }
       }
@@ -594,8 +720,9 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
     int item = 0;
     for (int l = 0; l < kLayers; ++l) {
       const int in = l == 0 ? kFin : kH;
+      const int ncols = (l == 0 && kMulti) ? in : in + 1;   // weights, then the bias column
 #pragma unroll 1
-      for (int c0 = 0; c0 <= in; c0 += 32, ++item) {
+      for (int c0 = 0; c0 < ncols; c0 += 32, ++item) {
         if (item % kBwdGroups != grp) continue;
         float v[32];
         tc::tmem_ld32(tmem + lane_base + dwcol[l] + c0, v);
@@ -603,12 +730,28 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         for (int i = 0; i < 32; ++i) {
           const int n = c0 + i;
           if (n < in) atomicAdd(&dparams[woff[l] + (size_t)t * in + n], v[i]);
-          else if (n == in) atomicAdd(&dparams[boff[l] + t], v[i]);
+          else if (n == in && n < ncols) atomicAdd(&dparams[boff[l] + t], v[i]);
         }
       }
     }
-    if (grp == 0)
-      for (int j = t; j <= kH; j += 128) atomicAdd(&dparams[j < kH ? woff[kLayers] + j : boff[kLayers]], s_dwo[j]);
+    if constexpr (kMulti) {
+      // dW_out^T: lane = hidden unit t, column = output
+#pragma unroll 1
+      for (int c0 = 0; c0 < kOut; c0 += 32, ++item) {
+        if (item % kBwdGroups != grp) continue;
+        float v[32];
+        tc::tmem_ld32(tmem + lane_base + dwo_col + c0, v);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) atomicAdd(&dparams[woff[kLayers] + (size_t)(c0 + i) * kH + t], v[i]);
+      }
+      if (grp == 0) {
+        for (int j = t; j < kOut; j += 128) atomicAdd(&dparams[boff[kLayers] + j], s_red[j]);
+        for (int j = t; j < kH; j += 128) atomicAdd(&dparams[boff[0] + j], s_red[kOut + j]);
+      }
+    } else {
+      if (grp == 0)
+        for (int j = t; j <= kH; j += 128) atomicAdd(&dparams[j < kH ? woff[kLayers] + j : boff[kLayers]], s_red[j]);
+    }
   }
   if (s_fail && tid == 0 && hdr) atomic_or_error(hdr, kErrMlpWait);
   tc::fence_before_sync();
@@ -618,21 +761,23 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
 
 // ---- launchers ------------------------------------------------------------------
 
-size_t mlp_bf16_forward_smem(int layers) {
-  return (size_t)kH * kFin * 2 + (size_t)(layers - 1) * kH * kH * 2 + (size_t)kFwdGroups * kRows * kH * 2 +
-         (size_t)(layers * kH + kH + 4) * sizeof(float);
+size_t mlp_bf16_forward_smem(int layers, int out) {
+  const size_t base = (size_t)kH * kFin * 2 + (size_t)(layers - 1) * kH * kH * 2 +
+                      (size_t)kFwdGroups * kRows * kH * 2 + (size_t)(layers * kH + kH + 4) * sizeof(float);
+  return out > 1 ? (base + 127) / 128 * 128 + (size_t)out * kH * 2 : base;
 }
-size_t mlp_bf16_backward_smem(int layers) {
+size_t mlp_bf16_backward_smem(int layers, int out) {
   return (size_t)kFin * kH * 2 + (size_t)(layers - 1) * kH * kH * 2 +
-         (size_t)kBwdGroups * ((size_t)kRows * kH * 2 + (size_t)kRows * (kH + 16) * 2) + (size_t)kH * sizeof(float);
+         (size_t)kBwdGroups * ((size_t)kRows * kH * 2 + (size_t)kRows * (kH + 16) * 2) + (size_t)kH * sizeof(float) +
+         (out > 1 ? (size_t)out * kH * 2 : 0);
 }
 
-template <int L, int A>
+template <int L, int A, int O>
 static cudaError_t launch_bf16_layers(bool fwd, int P, size_t rows, const float* means3D, const float* rx_pos,
                                       const float* params, const GeomView& geo, const SharedMlpLayout& Lt,
                                       float* work, const float* dL_dsignal, float* dparams, ImageHeader* hdr,
                                       cudaStream_t s) {
-  const size_t smem = fwd ? mlp_bf16_forward_smem(L) : mlp_bf16_backward_smem(L);
+  const size_t smem = fwd ? mlp_bf16_forward_smem(L, O) : mlp_bf16_backward_smem(L, O);
   static bool attr_done[2][64] = {};   // per instantiation
   static int sm_count[64] = {};
   int dev = 0;
@@ -644,9 +789,9 @@ static cudaError_t launch_bf16_layers(bool fwd, int P, size_t rows, const float*
     if (dev >= 0 && dev < 64) sm_count[dev] = sms;
   }
   if (dev < 0 || dev >= 64 || !attr_done[fwd][dev]) {
-    e = fwd ? cudaFuncSetAttribute(mlp_bf16_forward_kernel<L, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = fwd ? cudaFuncSetAttribute(mlp_bf16_forward_kernel<L, A, O>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem)
-            : cudaFuncSetAttribute(mlp_bf16_backward_kernel<L, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            : cudaFuncSetAttribute(mlp_bf16_backward_kernel<L, A, O>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem);
     if (e != cudaSuccess) return e;
     if (dev >= 0 && dev < 64) attr_done[fwd][dev] = true;
@@ -658,40 +803,48 @@ static cudaError_t launch_bf16_layers(bool fwd, int P, size_t rows, const float*
   const unsigned grid = (unsigned)(want < (size_t)sms ? want : (size_t)sms);
   __nv_bfloat16* zb = reinterpret_cast<__nv_bfloat16*>(work + Lt.z[1]);
   if (fwd)
-    mlp_bf16_forward_kernel<L, A><<<grid, 128 * kFwdGroups, smem, s>>>(P, rows, means3D, rx_pos, params, geo.radii,
-                                                                       zb, work + Lt.s, geo.signal, hdr);
+    mlp_bf16_forward_kernel<L, A, O><<<grid, 128 * kFwdGroups, smem, s>>>(P, rows, means3D, rx_pos, params,
+                                                                          geo.radii, zb, work + Lt.s, geo.signal,
+                                                                          hdr);
   else
-    mlp_bf16_backward_kernel<L, A><<<grid, kBwdThreads, smem, s>>>(P, rows, means3D, rx_pos, params, geo.radii, zb,
-                                                                   work + Lt.s, dL_dsignal, work + Lt.d0, dparams,
-                                                                   hdr);
+    mlp_bf16_backward_kernel<L, A, O><<<grid, kBwdThreads, smem, s>>>(P, rows, means3D, rx_pos, params, geo.radii,
+                                                                      zb, work + Lt.s, dL_dsignal, work + Lt.d0,
+                                                                      dparams, hdr);
   return cudaGetLastError();
 }
 
 template <int L>
-static cudaError_t launch_bf16_act(bool fwd, int P, size_t rows, int act, const float* means3D, const float* rx_pos,
-                                   const float* params, const GeomView& geo, const SharedMlpLayout& Lt, float* work,
-                                   const float* dL_dsignal, float* dparams, ImageHeader* hdr, cudaStream_t s) {
-  return act == 1 ? launch_bf16_layers<L, 1>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work, dL_dsignal,
-                                             dparams, hdr, s)
-                  : launch_bf16_layers<L, 2>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work, dL_dsignal,
-                                             dparams, hdr, s);
+static cudaError_t launch_bf16_act(bool fwd, int P, size_t rows, int act, int out, const float* means3D,
+                                   const float* rx_pos, const float* params, const GeomView& geo,
+                                   const SharedMlpLayout& Lt, float* work, const float* dL_dsignal, float* dparams,
+                                   ImageHeader* hdr, cudaStream_t s) {
+  if (out == 64)
+    return act == 1 ? launch_bf16_layers<L, 1, 64>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work,
+                                                   dL_dsignal, dparams, hdr, s)
+                    : launch_bf16_layers<L, 2, 64>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work,
+                                                   dL_dsignal, dparams, hdr, s);
+  if (out != 1) return cudaErrorInvalidValue;
+  return act == 1 ? launch_bf16_layers<L, 1, 1>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work, dL_dsignal,
+                                                dparams, hdr, s)
+                  : launch_bf16_layers<L, 2, 1>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work, dL_dsignal,
+                                                dparams, hdr, s);
 }
 
-cudaError_t launch_shared_mlp_bf16(bool fwd, int P, int R, int layers, int act, const float* means3D,
+cudaError_t launch_shared_mlp_bf16(bool fwd, int P, int R, int layers, int act, int out, const float* means3D,
                                    const float* rx_pos, const float* params, const GeomView& geo, float* work,
                                    const float* dL_dsignal, float* dparams, float* dL_dmeans3D, ImageHeader* hdr,
                                    cudaStream_t s) {
   const size_t rows = (size_t)P * R;
-  const SharedMlpLayout Lt = shared_mlp_layout_bf16(layers, rows);
+  const SharedMlpLayout Lt = shared_mlp_layout_bf16(layers, rows, out);
   cudaError_t e = cudaSuccess;
   if (!fwd) {
     e = cudaMemsetAsync(dparams, 0, Lt.params * sizeof(float), s);
     if (e != cudaSuccess) return e;
   }
   switch (layers) {
-    case 1: e = launch_bf16_act<1>(fwd, P, rows, act, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
-    case 2: e = launch_bf16_act<2>(fwd, P, rows, act, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
-    case 3: e = launch_bf16_act<3>(fwd, P, rows, act, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
+    case 1: e = launch_bf16_act<1>(fwd, P, rows, act, out, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
+    case 2: e = launch_bf16_act<2>(fwd, P, rows, act, out, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
+    case 3: e = launch_bf16_act<3>(fwd, P, rows, act, out, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
     default: return cudaErrorInvalidValue;
   }
   if (e != cudaSuccess || fwd) return e;

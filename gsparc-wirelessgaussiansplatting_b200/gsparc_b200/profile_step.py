@@ -43,7 +43,7 @@ def main(argv=None):
     from .shared_mlp import SharedMLP
     shared = {"ref": None, "relu64": SharedMLP(2, 64, "relu", precision=a.precision),
               "gelu128": SharedMLP(3, 128, "gelu", precision=a.precision),
-              "ch64": SharedMLP(3, 128, "gelu", out=64)}[a.mlp]
+              "ch64": SharedMLP(3, 128, "gelu", out=64, precision=a.precision)}[a.mlp]
     C = 1 if shared is None else shared.out
     targets = torch.rand((a.R, scenes.H, scenes.W) if C == 1 else (a.R, C, scenes.H, scenes.W), generator=gen).to(dev)
     tr = FusedTrainer(sc, device=dev, shared=shared)

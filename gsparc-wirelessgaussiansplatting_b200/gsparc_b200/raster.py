@@ -235,8 +235,8 @@ def forward_channels(means3D, opacities, scales, rotations, H, W, scale_modifier
     ForwardState); the amplitudes are ``shared.features(P, R)``."""
     if means3D.dim() != 2 or means3D.shape[1] != 3:
         raise RuntimeError("means3D must have dimensions (num_points, 3)")
-    if shared is None or shared.precision != "fp32":
-        raise ValueError("forward_channels needs an FP32 SharedMLP (out = channels)")
+    if shared is None or not (shared.precision == "fp32" or shared.out == 64):
+        raise ValueError("forward_channels needs a SharedMLP with out = channels (BF16: out = 64)")
     device = means3D.device
     tile = tuple(_tile if tile is None else tile)
     P = means3D.shape[0]

@@ -92,7 +92,7 @@ class SharedMLP:
 
     def features(self, P, R):
         """[R, P, out] amplitudes (sigmoid outputs) of the last forward: the
-        first R*P*out floats of the workspace (out > 1, FP32)."""
+        first R*P*out floats of the workspace."""
         return self._work[:int(R) * int(P) * self.out].view(int(R), int(P), self.out)
 
     def _spec(self):
