@@ -61,7 +61,7 @@ __device__ __forceinline__ int2 tile_pixel(int li, int tile_w) {
   return make_int2((w % bx) * 8 + (ln & 7), (w / bx) * 4 + (ln >> 3));
 }
 
-template <int kThreads>
+template <int kThreads, bool kWrap>
 __global__ void __launch_bounds__(kThreads)
 blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict__ ranges,
                      const uint32_t* __restrict__ chunk_base, const uint32_t* __restrict__ point_list,
@@ -116,10 +116,12 @@ blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict
         pf_co[k] = geo.conic_opacity[roff + id];
         pf_sg[k] = geo.signal[roff + id];
         pf_bb[k] = geo.box[roff + id];
-        const float sh = wrap_shift(pf_xy[k].x, tile_x, grid);   // the copy across the seam, if nearer
-        pf_xy[k].x += sh;
-        pf_bb[k].x += sh;
-        pf_bb[k].y += sh;
+        if constexpr (kWrap) {   // the copy across the seam, if nearer
+          const float sh = wrap_shift(pf_xy[k].x, tile_x, grid);
+          pf_xy[k].x += sh;
+          pf_bb[k].x += sh;
+          pf_bb[k].y += sh;
+        }
       }
     }
   };
@@ -221,7 +223,7 @@ blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict
   }
 }
 
-template <int kThreads>
+template <int kThreads, bool kWrap>
 __global__ void __launch_bounds__(kThreads)
 blend_backward_kernel(int P, int H, int W, TileGrid grid, int RT, unsigned grad_mode,
                       const uint2* __restrict__ ranges, const uint32_t* __restrict__ chunk_base,
@@ -323,10 +325,12 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, int RT, unsigned grad_
         pf_co[q] = geo.conic_opacity[roff + id];
         pf_sg[q] = geo.signal[roff + id];
         pf_bb[q] = geo.box[roff + id];
-        const float sh = wrap_shift(pf_xy[q].x, tile_x, grid);   // as the forward: the nearer copy
-        pf_xy[q].x += sh;
-        pf_bb[q].x += sh;
-        pf_bb[q].y += sh;
+        if constexpr (kWrap) {   // as the forward: the nearer copy
+          const float sh = wrap_shift(pf_xy[q].x, tile_x, grid);
+          pf_xy[q].x += sh;
+          pf_bb[q].x += sh;
+          pf_bb[q].y += sh;
+        }
       }
     }
   };
@@ -456,16 +460,17 @@ cudaError_t launch_blend_forward(int P, int R, int H, int W, const TileGrid& gri
                                  const ImageView& img, const BinningView& bin, float* out_real,
                                  float* out_imag, cudaStream_t stream) {
   if (R == 0 || grid.T == 0) return cudaSuccess;
+  // the seam wrap is a separate instantiation: without it the kernels are the clamped ones, register for register
   if (use_split_tiles(R, grid)) {
     dim3 g(grid.gx * (kBlendThreads / 64), grid.gy, R);
-    blend_forward_kernel<64><<<g, 64, 0, stream>>>(P, H, W, grid, img.ranges, img.chunk_base, bin.point_list,
-                                                   bin.ckpt, geo, img.hdr, img.final_T, img.n_contrib, img.accum,
-                                                   out_real, out_imag);
+    auto k = grid.wrap ? blend_forward_kernel<64, true> : blend_forward_kernel<64, false>;
+    k<<<g, 64, 0, stream>>>(P, H, W, grid, img.ranges, img.chunk_base, bin.point_list, bin.ckpt, geo, img.hdr,
+                            img.final_T, img.n_contrib, img.accum, out_real, out_imag);
   } else {
     dim3 g(grid.gx, grid.gy, R);
-    blend_forward_kernel<kBlendThreads><<<g, kBlendThreads, 0, stream>>>(
-        P, H, W, grid, img.ranges, img.chunk_base, bin.point_list, bin.ckpt, geo, img.hdr, img.final_T,
-        img.n_contrib, img.accum, out_real, out_imag);
+    auto k = grid.wrap ? blend_forward_kernel<kBlendThreads, true> : blend_forward_kernel<kBlendThreads, false>;
+    k<<<g, kBlendThreads, 0, stream>>>(P, H, W, grid, img.ranges, img.chunk_base, bin.point_list, bin.ckpt, geo,
+                                       img.hdr, img.final_T, img.n_contrib, img.accum, out_real, out_imag);
   }
   return cudaGetLastError();
 }
@@ -483,7 +488,8 @@ cudaError_t launch_blend_backward(int P, int R, int H, int W, const TileGrid& gr
   const int RT = R * grid.T;
   const long long items = capacity / kBwdChunk + RT;
   if (items > 0x7fffffffLL) return cudaErrorInvalidValue;
-  blend_backward_kernel<kBlendThreads><<<(unsigned)items, kBlendThreads, 0, stream>>>(
+  auto k = grid.wrap ? blend_backward_kernel<kBlendThreads, true> : blend_backward_kernel<kBlendThreads, false>;
+  k<<<(unsigned)items, kBlendThreads, 0, stream>>>(
       P, H, W, grid, RT, grad_mode, img.ranges, img.chunk_base, bin.point_list, bin.ckpt, img.accum, geo, img.hdr,
       img.final_T, img.n_contrib, dL_dout_real, dL_dout_imag, dmean2D, dconic, dsig, dopac);
   return cudaGetLastError();
