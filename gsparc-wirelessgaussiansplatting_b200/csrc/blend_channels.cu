@@ -30,6 +30,7 @@ namespace {
 constexpr int kMcThreads = 256;   // one thread per pixel: every tile shape holds 256 pixels
 constexpr int kMcBatch = 32;      // list entries staged per round
 constexpr int kMcWs = kMcThreads + 1;   // row stride of the (entry, pixel) weights
+constexpr int kMcGs = kMaxChannels + 4;  // row stride of the tile's dL/dout: float4 rows on distinct banks
 }  // namespace
 
 __device__ __forceinline__ int2 mc_pixel(int li, int tile_w) { return make_int2(li % tile_w, li / tile_w); }
@@ -53,6 +54,7 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
   const uint2 range = ranges[(size_t)r * grid.T + tile];
   const int n = (int)(range.y - range.x);
   const size_t roff = (size_t)r * P;
+  const int C4 = (C + 3) & ~3;
   float T = 1.0f;
   float acc[kMaxChannels];
 #pragma unroll
@@ -69,10 +71,10 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
       s_xy[li] = xy;
       s_co[li] = geo.conic_opacity[roff + id];
     }
-    for (int i = li; i < cnt * C; i += kMcThreads) {
-      const int e = i / C, c = i - e * C;
+    for (int i = li; i < cnt * C4; i += kMcThreads) {   // channels padded with zeros to a multiple of 4
+      const int e = i / C4, c = i - e * C4;
       const uint32_t id = checked_id(point_list[range.x + b0 + e], P, hdr);
-      s_f[e][c] = features[(roff + id) * C + c];
+      s_f[e][c] = c < C ? features[(roff + id) * C + c] : 0.0f;
     }
     __syncthreads();
     if (done) continue;
@@ -91,8 +93,14 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
       }
       const float w = alpha * T;
 #pragma unroll
-      for (int c = 0; c < kMaxChannels; ++c)
-        if (c < C) acc[c] = fmaf(s_f[e][c], w, acc[c]);
+      for (int q = 0; q < kMaxChannels / 4; ++q)
+        if (4 * q < C) {
+          const float4 f = *reinterpret_cast<const float4*>(&s_f[e][4 * q]);
+          acc[4 * q] = fmaf(f.x, w, acc[4 * q]);
+          acc[4 * q + 1] = fmaf(f.y, w, acc[4 * q + 1]);
+          acc[4 * q + 2] = fmaf(f.z, w, acc[4 * q + 2]);
+          acc[4 * q + 3] = fmaf(f.w, w, acc[4 * q + 3]);
+        }
       T = test_T;
       last = (uint32_t)(b0 + e + 1);
     }
@@ -118,8 +126,8 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
                                float* __restrict__ dconic, float* __restrict__ dopacity) {
   if (hdr->error) return;
   extern __shared__ __align__(16) float mc_sm[];
-  float* s_g = mc_sm;                                   // [256 pixels][64] dL/dout of the tile
-  float* s_w = s_g + kMcThreads * kMaxChannels;         // [kMcBatch][257] alpha T of (entry, pixel)
+  float* s_g = mc_sm;                                   // [256 pixels][68] dL/dout of the tile
+  float* s_w = s_g + kMcThreads * kMcGs;                // [kMcBatch][257] alpha T of (entry, pixel)
   __shared__ float2 s_xy[kMcBatch];
   __shared__ float4 s_co[kMcBatch];
   __shared__ uint32_t s_id[kMcBatch];
@@ -139,12 +147,14 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
   const size_t pix = (size_t)r * H * W + (size_t)py * W + px;
   float T = inside ? final_T[pix] : 1.0f;
   const int last = inside ? (int)n_contrib[pix] : 0;
+  const int C4 = (C + 3) & ~3;
   float g[kMaxChannels];
 #pragma unroll
-  for (int c = 0; c < kMaxChannels; ++c) {
+  for (int c = 0; c < kMaxChannels; ++c)
     g[c] = (inside && c < C) ? dL_dout[(size_t)r * C * plane + c * plane + (size_t)py * W + px] : 0.0f;
-    s_g[li * kMaxChannels + c] = g[c];
-  }
+#pragma unroll
+  for (int q = 0; q < kMaxChannels / 4; ++q)
+    *reinterpret_cast<float4*>(s_g + li * kMcGs + 4 * q) = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
   if (li == 0) s_top = 0;
   for (int i = li; i < kMcBatch * 8; i += kMcThreads) (&s_grad[0][0])[i] = 0.0f;
   __syncthreads();
@@ -165,10 +175,10 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
       s_xy[li] = xy;
       s_co[li] = geo.conic_opacity[roff + id];
     }
-    for (int i = li; i < cnt * C; i += kMcThreads) {
-      const int e = i / C, c = i - e * C;
+    for (int i = li; i < cnt * C4; i += kMcThreads) {   // channels padded with zeros to a multiple of 4
+      const int e = i / C4, c = i - e * C4;
       const uint32_t id = checked_id(point_list[range.x + lo + e], P, hdr);
-      s_f[e][c] = features[(roff + id) * C + c];
+      s_f[e][c] = c < C ? features[(roff + id) * C + c] : 0.0f;
     }
     __syncthreads();
     for (int e = cnt - 1; e >= 0; --e) {
@@ -187,8 +197,14 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
         const float Tn = T * __frcp_rn(1.f - alpha);
         float fg = 0.0f;
 #pragma unroll
-        for (int c = 0; c < kMaxChannels; ++c)
-          if (c < C) fg = fmaf(s_f[e][c], g[c], fg);
+        for (int q = 0; q < kMaxChannels / 4; ++q)
+          if (4 * q < C) {
+            const float4 f = *reinterpret_cast<const float4*>(&s_f[e][4 * q]);
+            fg = fmaf(f.x, g[4 * q], fg);
+            fg = fmaf(f.y, g[4 * q + 1], fg);
+            fg = fmaf(f.z, g[4 * q + 2], fg);
+            fg = fmaf(f.w, g[4 * q + 3], fg);
+          }
         float dL_dalpha = (fg - B / T) * Tn;
         if (a_raw > 0.99f) dL_dalpha = 0.0f;   // clamp blocks the gradient
         const float dL_dG = con_o.w * dL_dalpha;
@@ -230,8 +246,8 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
 #pragma unroll 4
         for (int p = 0; p < kMcThreads; ++p) {
           const float wv = wrow[p];
-          const float4 ga = *reinterpret_cast<const float4*>(s_g + p * kMaxChannels + c0);
-          const float4 gb = *reinterpret_cast<const float4*>(s_g + p * kMaxChannels + c0 + 4);
+          const float4 ga = *reinterpret_cast<const float4*>(s_g + p * kMcGs + c0);
+          const float4 gb = *reinterpret_cast<const float4*>(s_g + p * kMcGs + c0 + 4);
           y[0] = fmaf(wv, ga.x, y[0]); y[1] = fmaf(wv, ga.y, y[1]);
           y[2] = fmaf(wv, ga.z, y[2]); y[3] = fmaf(wv, ga.w, y[3]);
           y[4] = fmaf(wv, gb.x, y[4]); y[5] = fmaf(wv, gb.y, y[5]);
@@ -263,7 +279,7 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
 }
 
 static size_t blend_channels_backward_smem() {
-  return ((size_t)kMcThreads * kMaxChannels + (size_t)kMcBatch * kMcWs) * sizeof(float);
+  return ((size_t)kMcThreads * kMcGs + (size_t)kMcBatch * kMcWs) * sizeof(float);
 }
 
 cudaError_t launch_blend_channels_forward(int P, int R, int H, int W, int C, const TileGrid& grid,
