@@ -33,7 +33,24 @@ constexpr int kMcWs = kMcThreads + 1;   // row stride of the (entry, pixel) weig
 constexpr int kMcGs = kMaxChannels + 4;  // row stride of the tile's dL/dout: float4 rows on distinct banks
 }  // namespace
 
-__device__ __forceinline__ int2 mc_pixel(int li, int tile_w) { return make_int2(li % tile_w, li / tile_w); }
+// Pixel of thread li in its tile: every warp covers an 8x4 block, and skips
+// the staged entries whose footprint box (alpha < 1/255 outside it, from the
+// preprocess) misses its block -- no result changes.
+__device__ __forceinline__ int2 mc_pixel(int li, int tile_w) {
+  const int w = li >> 5, ln = li & 31, bx = tile_w >> 3;
+  return make_int2((w % bx) * 8 + (ln & 7), (w / bx) * 4 + (ln >> 3));
+}
+struct McRect {
+  float x0, x1, y0, y1;
+};
+__device__ __forceinline__ McRect mc_warp_rect(int px, int py) {
+  McRect w;
+  w.x0 = (float)__reduce_min_sync(0xffffffffu, px);
+  w.x1 = (float)__reduce_max_sync(0xffffffffu, px);
+  w.y0 = (float)__reduce_min_sync(0xffffffffu, py);
+  w.y1 = (float)__reduce_max_sync(0xffffffffu, py);
+  return w;
+}
 
 __global__ void __launch_bounds__(kMcThreads)
 blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const uint2* __restrict__ ranges,
@@ -43,6 +60,7 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
   if (hdr->error) return;
   __shared__ float2 s_xy[kMcBatch];
   __shared__ float4 s_co[kMcBatch];
+  __shared__ float4 s_bb[kMcBatch];
   __shared__ __align__(16) float s_f[kMcBatch][kMaxChannels];
   const int r = blockIdx.y, tile = blockIdx.x;
   const int tx = tile % grid.gx, ty = tile / grid.gx;
@@ -51,6 +69,7 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
   const int px = tx * grid.tile_w + lp.x, py = ty * grid.tile_h + lp.y;
   const bool inside = px < W && py < H;
   const float2 pixf = make_float2((float)px, (float)py);
+  const McRect wr = mc_warp_rect(px, py);
   const uint2 range = ranges[(size_t)r * grid.T + tile];
   const int n = (int)(range.y - range.x);
   const size_t roff = (size_t)r * P;
@@ -67,8 +86,13 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
     if (li < cnt) {
       const uint32_t id = checked_id(point_list[range.x + b0 + li], P, hdr);
       float2 xy = geo.means2D[roff + id];
-      xy.x += wrap_shift(xy.x, tx, grid);
+      float4 bb = geo.box[roff + id];
+      const float sh = wrap_shift(xy.x, tx, grid);
+      xy.x += sh;
+      bb.x += sh;
+      bb.y += sh;
       s_xy[li] = xy;
+      s_bb[li] = bb;
       s_co[li] = geo.conic_opacity[roff + id];
     }
     for (int i = li; i < cnt * C4; i += kMcThreads) {   // channels padded with zeros to a multiple of 4
@@ -79,6 +103,7 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
     __syncthreads();
     if (done) continue;
     for (int e = 0; e < cnt; ++e) {
+      if (box_outside(s_bb[e], wr.x0, wr.x1, wr.y0, wr.y1)) continue;   // warp-uniform
       const float2 xy = s_xy[e];
       const float4 con_o = s_co[e];
       const float2 d = make_float2(xy.x - pixf.x, xy.y - pixf.y);
@@ -130,9 +155,11 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
   float* s_w = s_g + kMcThreads * kMcGs;                // [kMcBatch][257] alpha T of (entry, pixel)
   __shared__ float2 s_xy[kMcBatch];
   __shared__ float4 s_co[kMcBatch];
+  __shared__ float4 s_bb[kMcBatch];
   __shared__ uint32_t s_id[kMcBatch];
   __shared__ __align__(16) float s_f[kMcBatch][kMaxChannels];
   __shared__ float s_grad[kMcBatch][8];
+  __shared__ uint32_t s_hit[kMcBatch];   // per entry: the warps with a contributing pixel
   __shared__ int s_top;
   const int r = blockIdx.y, tile = blockIdx.x;
   const int tx = tile % grid.gx, ty = tile / grid.gx;
@@ -141,6 +168,7 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
   const int px = tx * grid.tile_w + lp.x, py = ty * grid.tile_h + lp.y;
   const bool inside = px < W && py < H;
   const float2 pixf = make_float2((float)px, (float)py);
+  const McRect wr = mc_warp_rect(px, py);
   const uint2 range = ranges[(size_t)r * grid.T + tile];
   const size_t roff = (size_t)r * P;
   const size_t plane = (size_t)H * W;
@@ -157,6 +185,7 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
     *reinterpret_cast<float4*>(s_g + li * kMcGs + 4 * q) = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
   if (li == 0) s_top = 0;
   for (int i = li; i < kMcBatch * 8; i += kMcThreads) (&s_grad[0][0])[i] = 0.0f;
+  if (li < kMcBatch) s_hit[li] = 0u;
   __syncthreads();
   atomicMax(&s_top, last);
   __syncthreads();
@@ -171,8 +200,13 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
       const uint32_t id = checked_id(point_list[range.x + lo + li], P, hdr);
       s_id[li] = id;
       float2 xy = geo.means2D[roff + id];
-      xy.x += wrap_shift(xy.x, tx, grid);
+      float4 bb = geo.box[roff + id];
+      const float sh = wrap_shift(xy.x, tx, grid);
+      xy.x += sh;
+      bb.x += sh;
+      bb.y += sh;
       s_xy[li] = xy;
+      s_bb[li] = bb;
       s_co[li] = geo.conic_opacity[roff + id];
     }
     for (int i = li; i < cnt * C4; i += kMcThreads) {   // channels padded with zeros to a multiple of 4
@@ -182,6 +216,8 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
     }
     __syncthreads();
     for (int e = cnt - 1; e >= 0; --e) {
+      // warp-uniform: no pixel of the warp takes the entry, so its weights stay unread (s_hit)
+      if (box_outside(s_bb[e], wr.x0, wr.x1, wr.y0, wr.y1)) continue;
       const int pos = lo + e;
       const float2 xy = s_xy[e];
       const float4 con_o = s_co[e];
@@ -229,6 +265,7 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
       v[7] = 0.0f;
       s_w[e * kMcWs + li] = wgt;
       if (__any_sync(0xffffffffu, c_ok)) {
+        if (lane == 0) atomicOr(&s_hit[e], 1u << (li >> 5));
         const float z = warp_reduce8(v, lane);
         if ((lane & 3) == 0) {
           const int vidx = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
@@ -243,15 +280,19 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
       if (e < cnt && c0 < C) {
         float y[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         const float* wrow = s_w + e * kMcWs;
+        // only the warps (32-pixel blocks) where the entry contributed have nonzero weights
+        for (uint32_t m = s_hit[e]; m; m &= m - 1) {
+          const int p0 = (__ffs(m) - 1) * 32;
 #pragma unroll 4
-        for (int p = 0; p < kMcThreads; ++p) {
-          const float wv = wrow[p];
-          const float4 ga = *reinterpret_cast<const float4*>(s_g + p * kMcGs + c0);
-          const float4 gb = *reinterpret_cast<const float4*>(s_g + p * kMcGs + c0 + 4);
-          y[0] = fmaf(wv, ga.x, y[0]); y[1] = fmaf(wv, ga.y, y[1]);
-          y[2] = fmaf(wv, ga.z, y[2]); y[3] = fmaf(wv, ga.w, y[3]);
-          y[4] = fmaf(wv, gb.x, y[4]); y[5] = fmaf(wv, gb.y, y[5]);
-          y[6] = fmaf(wv, gb.z, y[6]); y[7] = fmaf(wv, gb.w, y[7]);
+          for (int p = p0; p < p0 + 32; ++p) {
+            const float wv = wrow[p];
+            const float4 ga = *reinterpret_cast<const float4*>(s_g + p * kMcGs + c0);
+            const float4 gb = *reinterpret_cast<const float4*>(s_g + p * kMcGs + c0 + 4);
+            y[0] = fmaf(wv, ga.x, y[0]); y[1] = fmaf(wv, ga.y, y[1]);
+            y[2] = fmaf(wv, ga.z, y[2]); y[3] = fmaf(wv, ga.w, y[3]);
+            y[4] = fmaf(wv, gb.x, y[4]); y[5] = fmaf(wv, gb.y, y[5]);
+            y[6] = fmaf(wv, gb.z, y[6]); y[7] = fmaf(wv, gb.w, y[7]);
+          }
         }
         float* dst = dL_dfeatures + (roff + s_id[e]) * C;
 #pragma unroll
@@ -275,6 +316,7 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
       }
     }
     __syncthreads();
+    if (li < kMcBatch) s_hit[li] = 0u;   // read above by every thread; the next batch sets it after a barrier
   }
 }
 
