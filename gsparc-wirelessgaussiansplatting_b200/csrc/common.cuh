@@ -267,7 +267,7 @@ __device__ __forceinline__ void scan_segments_cta(int n, const uint32_t* __restr
 
 // Scratch of the fused training loss (ssim.cu), in floats.
 struct LossLayout {
-  size_t nblk, dmu1, ds11, ds12, partial, pre, coef, sync, total;
+  size_t nblk, dmu1, ds11, ds12, partial, pre, coef, share, psync, sync, total;
 };
 
 // ---------------------------------------------------------------------------

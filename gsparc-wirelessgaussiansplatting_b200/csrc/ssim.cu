@@ -163,10 +163,20 @@ ssim_backward_kernel(int H, int W, const float* __restrict__ img1, const float* 
 //   conf_r  = 1 + exp(fc2(relu(fc1(rx_r))))              (gaussian.py:575-609)
 //   loss    = mean_r (conf_r recon_r - alpha log conf_r)
 // and its adjoint with respect to pred and the confidence-MLP parameters,
-// in two launches: tile moments + per-tile partial sums, whose last CTA runs
-// the head (reductions, MLP forward/backward, per-receiver gradient scales),
-// then the SSIM/L1 backward with the per-receiver scales applied while
-// staging.
+// in two launches:
+//   1. SSIM moments, map derivatives and per-block partial sums of |p - t|
+//      and the map.  The last block of each spectrum runs that spectrum's
+//      head (its means, the confidence MLP forward, the per-spectrum
+//      gradient scales and its share of every confidence-parameter
+//      gradient); the last head sums the shares and the loss in spectrum
+//      order.
+//   2. The SSIM/L1 backward with the per-spectrum scales applied while
+//      staging.
+// Two block layouts run the same per-pixel arithmetic: 32x8 tiles with their
+// halo (few spectra: 144 blocks per 90x360 spectrum), or 128-column strips
+// that walk down a band of rows with the vertical window in registers (many
+// spectra: each input row is filtered horizontally once instead of 2.25
+// times, and no halo rows are staged twice).
 // Every reduction has a fixed order, so the loss is deterministic.
 // ---------------------------------------------------------------------------
 
@@ -176,26 +186,200 @@ __device__ __forceinline__ float warp_sum_all(float v) {
   return v;
 }
 
-__device__ __forceinline__ void loss_head_body(int R, int nblk, int HW, int hidden, float lambda1, float alpha,
-                                               const float* __restrict__ rx, const float* __restrict__ cp,
-                                               const float2* __restrict__ partial, float* __restrict__ pre,
-                                               float4* __restrict__ coef, float* __restrict__ terms,
-                                               float* __restrict__ loss_out, float* __restrict__ dconf);
+// SSIM of one pixel from its five window moments (mu1, E[x^2], mu2, E[y^2],
+// E[xy]), and the three partial derivatives the backward convolves
+// (fused-ssim/ssim.cu:262-283): the same quantities, with the seven
+// divisions by A B, A^2 B and A B^2 taken as products with the correctly
+// rounded reciprocals of A and B (a few ulps from the quotient form).
+__device__ __forceinline__ float ssim_pixel(const float (&v)[5], float C1, float C2, float& d_mu1, float& d_s11,
+                                            float& d_s12) {
+  const float mu1 = v[0];
+  const float sigma1_sq = v[1] - mu1 * mu1;
+  const float mu2 = v[2];
+  const float sigma2_sq = v[3] - mu2 * mu2;
+  const float sigma12 = v[4] - mu1 * mu2;
+  const float C = (2.0f * (mu1 * mu2) + C1);
+  const float D = (2.0f * sigma12 + C2);
+  const float A = (mu1 * mu1 + mu2 * mu2 + C1);
+  const float B = (sigma1_sq + sigma2_sq + C2);
+  const float ia = __frcp_rn(A), ib = __frcp_rn(B);
+  const float iab = ia * ib;
+  const float m = (C * D) * iab;
+  const float m2 = (mu1 * 2.0f) * m;
+  d_mu1 = (mu2 * 2.0f) * (D - C) * iab - m2 * ia + m2 * ib;
+  d_s11 = -m * ib;
+  d_s12 = (2.0f * C) * iab;
+  return m;
+}
 
-// Tile moments, SSIM partial derivatives and per-tile partial sums; the last
-// CTA to finish (arrival counter in the scratch) runs the head.
+struct LossHead {
+  int R, hidden;
+  float lambda1, alpha;
+  const float* rx;   // [R][3]
+  const float* cp;   // confidence MLP: fc1.weight [hidden][3], fc1.bias, fc2.weight [hidden], fc2.bias
+  float* pre;        // [R][hidden] fc1 pre-activations
+  float4* coef;      // [R]
+  float* terms;      // [R][4] or null
+  float* loss_out;
+  float* dconf;      // [5 hidden + 1]
+  float* share;      // [R][5 hidden + 1] per-spectrum parameter-gradient terms
+  unsigned* psync;   // [R] arrivals per spectrum
+  unsigned* sync;    // heads done
+};
+
+// Spectrum r's head: mean L1 and SSIM (block partials in block order), the
+// confidence MLP forward, coef[r] = (dL/dpred scale of the L1 term, dL/dmap
+// of the SSIM term, loss_r, dL/draw_r), and r's term of every confidence
+// parameter's gradient.
+__device__ void loss_spectrum_head(int r, int nblk, int HW, const LossHead& h, const float2* __restrict__ partial) {
+  __shared__ float s_draw;
+  const int hidden = h.hidden;
+  const float* w1 = h.cp;
+  const float* b1 = h.cp + 3 * hidden;
+  const float* w2 = b1 + hidden;
+  const float b2 = w2[hidden];
+  const float* x = h.rx + 3 * r;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    float a = 0.0f, b = 0.0f;
+    for (int i = lane; i < nblk; i += 32) {
+      const float2 p = __ldcg(partial + (size_t)r * nblk + i);   // written by other blocks
+      a += p.x;
+      b += p.y;
+    }
+    a = warp_sum_all(a);
+    b = warp_sum_all(b);
+    const float n = (float)HW, fR = (float)h.R;
+    const float l1 = a / n, ssim = b / n;
+    float acc = 0.0f;
+    for (int j = lane; j < hidden; j += 32) {
+      const float p = w1[3 * j] * x[0] + w1[3 * j + 1] * x[1] + w1[3 * j + 2] * x[2] + b1[j];
+      h.pre[(size_t)r * hidden + j] = p;
+      acc += w2[j] * fmaxf(p, 0.0f);
+    }
+    acc = warp_sum_all(acc);
+    const float e = expf(acc + b2);
+    const float conf = 1.0f + e;
+    const float recon = (1.0f - h.lambda1) * l1 + h.lambda1 * (1.0f - ssim);
+    const float loss_r = conf * recon - h.alpha * logf(conf);
+    const float g_rec = conf / fR;
+    const float draw = ((recon - h.alpha / conf) / fR) * e;
+    if (lane == 0) {
+      h.coef[r] = make_float4((g_rec * (1.0f - h.lambda1)) / n, -(g_rec * h.lambda1) / n, loss_r, draw);
+      if (h.terms) {
+        h.terms[4 * r] = l1;
+        h.terms[4 * r + 1] = ssim;
+        h.terms[4 * r + 2] = conf;
+        h.terms[4 * r + 3] = loss_r;
+      }
+      s_draw = draw;
+    }
+  }
+  __syncthreads();
+  const float cw = s_draw;
+  const int np = 5 * hidden + 1;
+  float* sh = h.share + (size_t)r * np;
+  for (int p = threadIdx.x; p < np; p += blockDim.x) {
+    float g;
+    if (p < 3 * hidden) {            // fc1.weight [hidden, 3]
+      const int j = p / 3, k = p % 3;
+      g = __ldcg(h.pre + (size_t)r * hidden + j) > 0.0f ? (cw * w2[j]) * x[k] : 0.0f;
+    } else if (p < 4 * hidden) {     // fc1.bias
+      const int j = p - 3 * hidden;
+      g = __ldcg(h.pre + (size_t)r * hidden + j) > 0.0f ? cw * w2[j] : 0.0f;
+    } else if (p < 5 * hidden) {     // fc2.weight [1, hidden]
+      const int j = p - 4 * hidden;
+      g = cw * fmaxf(__ldcg(h.pre + (size_t)r * hidden + j), 0.0f);
+    } else {                         // fc2.bias
+      g = cw;
+    }
+    sh[p] = g;
+  }
+}
+
+// The confidence-parameter gradients and the loss: sums over the spectra in
+// spectrum order.
+// The confidence-parameter gradients and the loss: sums over the spectra in a
+// fixed order (eight interleaved partial sums per parameter, so that eight
+// loads are in flight; lane-strided sums for the loss).
+__device__ void loss_final(const LossHead& h) {
+  const int np = 5 * h.hidden + 1;
+  for (int p = threadIdx.x; p < np; p += blockDim.x) {
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int r = 0;
+    for (; r + 8 <= h.R; r += 8)
+#pragma unroll
+      for (int i = 0; i < 8; ++i) acc[i] += __ldcg(h.share + (size_t)(r + i) * np + p);
+#pragma unroll
+    for (int i = 0; i < 7; ++i)
+      if (r + i < h.R) acc[i] += __ldcg(h.share + (size_t)(r + i) * np + p);
+    h.dconf[p] = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+  }
+  if (threadIdx.x < 32) {
+    float s = 0.0f;
+    for (int r = threadIdx.x; r < h.R; r += 32) s += __ldcg(h.coef + r).z;
+    s = warp_sum_all(s);
+    if (threadIdx.x == 0) h.loss_out[0] = s / (float)h.R;
+  }
+}
+
+// Called by every thread after thread 0 wrote the block's partial: the last
+// block of spectrum blockIdx.z runs its head, the last head the final sums.
+// Each counter is reset by its last user, so the scratch stays reusable.
+__device__ void loss_arrive(int nblk, int HW, const LossHead& h, const float2* __restrict__ partial) {
+  __shared__ int s_last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(h.psync + blockIdx.z, 1u) == (unsigned)nblk - 1u;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  loss_spectrum_head((int)blockIdx.z, nblk, HW, h, partial);
+  __threadfence();   // this block's coef / terms / share before the head count
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    h.psync[blockIdx.z] = 0u;
+    s_last = atomicAdd(h.sync, 1u) == (unsigned)h.R - 1u;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  loss_final(h);
+  if (threadIdx.x == 0) *h.sync = 0u;
+}
+
+// Block partial (sum of |p - t|, sum of the map) from every thread's values,
+// reduced in a fixed order; written by thread 0.
+__device__ __forceinline__ void block_partial(float l1, float sm, float2* __restrict__ partial) {
+  __shared__ float red[2][32];
+  l1 = warp_sum_all(l1);
+  sm = warp_sum_all(sm);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = l1;
+    red[1][threadIdx.x >> 5] = sm;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float a = 0.0f, b = 0.0f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a += red[0][w];
+      b += red[1][w];
+    }
+    partial[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = make_float2(a, b);
+  }
+}
+
+// ---- tile layout: 32x8 outputs per block with the 5-pixel halo --------------
+
 __global__ void __launch_bounds__(256)
 loss_forward_kernel(int H, int W, float C1, float C2, const float* __restrict__ pred,
                     const float* __restrict__ target, float* __restrict__ dm_dmu1,
                     float* __restrict__ dm_dsigma1_sq, float* __restrict__ dm_dsigma12,
-                    float2* __restrict__ partial, int hidden, float lambda1, float alpha,
-                    const float* __restrict__ rx, const float* __restrict__ cp, float* __restrict__ pre,
-                    float4* __restrict__ coef, float* __restrict__ terms, float* __restrict__ loss_out,
-                    float* __restrict__ dconf, unsigned* __restrict__ arrived) {
+                    float2* __restrict__ partial, LossHead head) {
   __shared__ float s1[kTH][kTW + 1];
   __shared__ float s2[kTH][kTW + 1];
   __shared__ float hx[5][kTH][kSW];
-  __shared__ float red[2][8];
   const size_t plane = (size_t)blockIdx.z * H * W;
   const int x0 = blockIdx.x * kSW - kHalo, y0 = blockIdx.y * kSH - kHalo;
   stage_tile(s1, pred + plane, H, W, x0, y0);
@@ -223,127 +407,19 @@ loss_forward_kernel(int H, int W, float C1, float C2, const float* __restrict__ 
   for (int q = 0; q < 5; ++q)
 #pragma unroll
     for (int k = 0; k < 11; ++k) v[q] += kSsimWin[k] * hx[q][ly + k][lx];
-  const float mu1 = v[0];
-  const float sigma1_sq = v[1] - mu1 * mu1;
-  const float mu2 = v[2];
-  const float sigma2_sq = v[3] - mu2 * mu2;
-  const float sigma12 = v[4] - mu1 * mu2;
-  const float C = (2.0f * (mu1 * mu2) + C1);
-  const float D = (2.0f * sigma12 + C2);
-  const float A = (mu1 * mu1 + mu2 * mu2 + C1);
-  const float B = (sigma1_sq + sigma2_sq + C2);
   const int px = blockIdx.x * kSW + lx, py = blockIdx.y * kSH + ly;
   float l1 = 0.0f, sm = 0.0f;
   if (px < W && py < H) {
     const size_t idx = plane + (size_t)py * W + px;
-    sm = (C * D) / (A * B);
+    float d1, d2, d3;
+    sm = ssim_pixel(v, C1, C2, d1, d2, d3);
     l1 = fabsf(s1[ly + kHalo][lx + kHalo] - s2[ly + kHalo][lx + kHalo]);
-    dm_dmu1[idx] = ((mu2 * 2.0f * D) / (A * B) - (mu2 * 2.0f * C) / (A * B) - (mu1 * 2.0f * C * D) / (A * A * B) +
-                    (mu1 * 2.0f * C * D) / (A * B * B));
-    dm_dsigma1_sq[idx] = ((-C * D) / (A * B * B));
-    dm_dsigma12[idx] = ((2 * C) / (A * B));
+    dm_dmu1[idx] = d1;
+    dm_dsigma1_sq[idx] = d2;
+    dm_dsigma12[idx] = d3;
   }
-  l1 = warp_sum_all(l1);
-  sm = warp_sum_all(sm);
-  if ((threadIdx.x & 31) == 0) {
-    red[0][threadIdx.x >> 5] = l1;
-    red[1][threadIdx.x >> 5] = sm;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float a = 0.0f, b = 0.0f;
-#pragma unroll
-    for (int w = 0; w < 8; ++w) { a += red[0][w]; b += red[1][w]; }
-    partial[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = make_float2(a, b);
-  }
-  __shared__ bool s_last;
-  if (threadIdx.x == 0) {
-    __threadfence();
-    s_last = atomicAdd(arrived, 1u) == gridDim.x * gridDim.y * gridDim.z - 1;
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();
-    loss_head_body(gridDim.z, gridDim.x * gridDim.y, H * W, hidden, lambda1, alpha, rx, cp, partial, pre, coef,
-                   terms, loss_out, dconf);
-    if (threadIdx.x == 0) *arrived = 0u;
-  }
-}
-
-// One CTA: warp per receiver for the reductions and the confidence MLP
-// forward, then thread per MLP parameter for its gradient (sum over
-// receivers in receiver order).  coef[r] = (dL/dpred scale of the L1 term,
-// dL/dmap of the SSIM term, loss_r, dL/draw_r).
-__device__ __forceinline__ void loss_head_body(int R, int nblk, int HW, int hidden, float lambda1, float alpha,
-                                               const float* __restrict__ rx,
-                 const float* __restrict__ cp, const float2* __restrict__ partial, float* __restrict__ pre,
-                 float4* __restrict__ coef, float* __restrict__ terms, float* __restrict__ loss_out,
-                 float* __restrict__ dconf) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const float* w1 = cp;
-  const float* b1 = cp + 3 * hidden;
-  const float* w2 = b1 + hidden;
-  const float b2 = w2[hidden];
-  const float n = (float)HW, fR = (float)R;
-  for (int r = warp; r < R; r += 8) {
-    float a = 0.0f, b = 0.0f;
-    for (int i = lane; i < nblk; i += 32) {
-      const float2 p = __ldcg(partial + (size_t)r * nblk + i);   // written by other CTAs
-      a += p.x;
-      b += p.y;
-    }
-    a = warp_sum_all(a);
-    b = warp_sum_all(b);
-    const float l1 = a / n, ssim = b / n;
-    const float x0 = rx[3 * r], x1 = rx[3 * r + 1], x2 = rx[3 * r + 2];
-    float acc = 0.0f;
-    for (int j = lane; j < hidden; j += 32) {
-      const float p = w1[3 * j] * x0 + w1[3 * j + 1] * x1 + w1[3 * j + 2] * x2 + b1[j];
-      pre[(size_t)r * hidden + j] = p;
-      acc += w2[j] * fmaxf(p, 0.0f);
-    }
-    acc = warp_sum_all(acc);
-    const float e = expf(acc + b2);
-    const float conf = 1.0f + e;
-    const float recon = (1.0f - lambda1) * l1 + lambda1 * (1.0f - ssim);
-    const float loss_r = conf * recon - alpha * logf(conf);
-    const float g_rec = conf / fR;
-    const float draw = ((recon - alpha / conf) / fR) * e;
-    if (lane == 0) {
-      coef[r] = make_float4((g_rec * (1.0f - lambda1)) / n, -(g_rec * lambda1) / n, loss_r, draw);
-      if (terms) {
-        terms[4 * r] = l1;
-        terms[4 * r + 1] = ssim;
-        terms[4 * r + 2] = conf;
-        terms[4 * r + 3] = loss_r;
-      }
-    }
-  }
-  __syncthreads();
-  const int np = 5 * hidden + 1;
-  for (int p = threadIdx.x; p < np; p += blockDim.x) {
-    float g = 0.0f;
-    if (p < 3 * hidden) {            // fc1.weight [hidden, 3]
-      const int j = p / 3, k = p % 3;
-      for (int r = 0; r < R; ++r)
-        if (pre[(size_t)r * hidden + j] > 0.0f) g += (coef[r].w * w2[j]) * rx[3 * r + k];
-    } else if (p < 4 * hidden) {     // fc1.bias
-      const int j = p - 3 * hidden;
-      for (int r = 0; r < R; ++r)
-        if (pre[(size_t)r * hidden + j] > 0.0f) g += coef[r].w * w2[j];
-    } else if (p < 5 * hidden) {     // fc2.weight [1, hidden]
-      const int j = p - 4 * hidden;
-      for (int r = 0; r < R; ++r) g += coef[r].w * fmaxf(pre[(size_t)r * hidden + j], 0.0f);
-    } else {                         // fc2.bias
-      for (int r = 0; r < R; ++r) g += coef[r].w;
-    }
-    dconf[p] = g;
-  }
-  if (threadIdx.x == 0) {
-    float s = 0.0f;
-    for (int r = 0; r < R; ++r) s += coef[r].z;
-    loss_out[0] = s / fR;
-  }
+  block_partial(l1, sm, partial);
+  loss_arrive(gridDim.x * gridDim.y, H * W, head, partial);
 }
 
 __device__ __forceinline__ void stage_scaled(float (*dst)[kTW + 1], const float* __restrict__ a, float c, int H,
@@ -355,8 +431,19 @@ __device__ __forceinline__ void stage_scaled(float (*dst)[kTW + 1], const float*
   }
 }
 
-// SSIM backward (as ssim_backward_kernel) with a map gradient that is the
-// same for every pixel of a spectrum, plus the L1 term scale * sign(p - t).
+// The L1 and SSIM terms of dL/dpred for one pixel: the map gradient is the
+// same for every pixel of a spectrum, so the three convolved derivative maps
+// arrive already scaled by it (fused-ssim/ssim.cu:288-366).
+__device__ __forceinline__ float loss_pixel_grad(const float (&v)[3], float pix1, float pix2, float l1_scale) {
+  float g = 0.0f;
+  g += v[0];
+  g += pix1 * 2.0f * v[1];
+  g += pix2 * v[2];
+  const float d = pix1 - pix2;
+  const float sgn = (d > 0.0f) ? 1.0f : ((d < 0.0f) ? -1.0f : 0.0f);
+  return l1_scale * sgn + g;
+}
+
 __global__ void __launch_bounds__(256)
 loss_backward_kernel(int H, int W, const float* __restrict__ pred, const float* __restrict__ target,
                      const float* __restrict__ dm_dmu1, const float* __restrict__ dm_dsigma1_sq,
@@ -393,29 +480,287 @@ loss_backward_kernel(int H, int W, const float* __restrict__ pred, const float* 
     for (int k = 0; k < 11; ++k) v[q] += kSsimWin[k] * hx[q][ly + k][lx];
   if (px < W && py < H) {
     const size_t idx = plane + (size_t)py * W + px;
-    const float pix1 = pred[idx], pix2 = target[idx];
-    float g = 0.0f;
-    g += v[0];
-    g += pix1 * 2.0f * v[1];
-    g += pix2 * v[2];
-    const float d = pix1 - pix2;
-    const float sgn = (d > 0.0f) ? 1.0f : ((d < 0.0f) ? -1.0f : 0.0f);
-    dL_dpred[idx] = cf.x * sgn + g;
+    dL_dpred[idx] = loss_pixel_grad(v, pred[idx], target[idx], cf.x);
   }
+}
+
+// ---- strip layout: 128 columns per block, walking down a band of rows ------
+// Input rows are staged 11 at a time (one window height) by cp.async into a
+// double buffer; each thread filters its column of every input row
+// horizontally into a ring of 11 rows held in registers, and an output row is
+// the vertical window over the ring once the 11 rows around it are in.
+// Paired quantities (p and t, their squares, two of the three derivative
+// maps) are staged interleaved and filtered with the FP32x2 instructions of
+// sm_100, whose lanes round exactly as the scalar ones: the per-pixel
+// arithmetic and its order are the tile layout's.
+
+constexpr int kBandThreads = 128;                     // output columns per strip
+constexpr int kBandCols = kBandThreads + 2 * kHalo;   // 138 staged columns
+constexpr int kBandPitch = kBandCols + 2;
+constexpr int kRing = 11;                             // window height = rows per staged chunk
+constexpr int kBandMinPlanes = 16;                    // fewer spectra: tile layout
+constexpr size_t kBandTargetBlocks = 592;             // four 4-warp blocks per SM
+
+// {w_k, w_k}: the window as FP32x2 operands
+__constant__ float2 kSsimWin2[11] = {
+    {0.001028380123898387f, 0.001028380123898387f},   {0.0075987582094967365f, 0.0075987582094967365f},
+    {0.036000773310661316f, 0.036000773310661316f},   {0.10936068743467331f, 0.10936068743467331f},
+    {0.21300552785396576f, 0.21300552785396576f},     {0.26601171493530273f, 0.26601171493530273f},
+    {0.21300552785396576f, 0.21300552785396576f},     {0.10936068743467331f, 0.10936068743467331f},
+    {0.036000773310661316f, 0.036000773310661316f},   {0.0075987582094967365f, 0.0075987582094967365f},
+    {0.001028380123898387f, 0.001028380123898387f}};
+
+__device__ __forceinline__ unsigned long long f2_bits(float2 v) {
+  return ((unsigned long long)__float_as_uint(v.y) << 32) | __float_as_uint(v.x);
+}
+__device__ __forceinline__ float2 bits_f2(unsigned long long b) {
+  return make_float2(__uint_as_float((unsigned)b), __uint_as_float((unsigned)(b >> 32)));
+}
+// a * b + c and a * b per lane (fma.rn.f32x2 / mul.rn.f32x2)
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
+  return bits_f2(d);
+}
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return bits_f2(d);
+}
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool ok) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(ok ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Staged chunk: rows yin0 .. yin0 + 10, columns x0 - 5 .. x0 + 132, zero
+// outside the image (nothing is read there; the source address stays the
+// plane's base).  Images 0 and 1 interleave as float2 [row][column]; image 2
+// (if any) follows as float [row][column].  Thread i copies columns i and
+// i + 128 of every row and image, and scales its own copies in the backward.
+__device__ __forceinline__ int band_slot(int im, int j, int col) {
+  return im < 2 ? (j * kBandPitch + col) * 2 + im : 2 * kRing * kBandPitch + j * kBandPitch + col;
+}
+template <int kImgs>
+__device__ __forceinline__ void band_stage(float* dst, const float* const (&src)[kImgs], int H, int W, int x0,
+                                           int yin0) {
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    const int col = (int)threadIdx.x + half * kBandThreads;
+    if (col < kBandCols) {
+      const int gx = x0 - kHalo + col;
+      const bool cok = gx >= 0 && gx < W;
+#pragma unroll
+      for (int j = 0; j < kRing; ++j) {
+        const int gy = yin0 + j;
+        const bool ok = cok && gy >= 0 && gy < H;
+        const size_t o = ok ? (size_t)gy * W + gx : 0;
+#pragma unroll
+        for (int im = 0; im < kImgs; ++im) cp_async4(dst + band_slot(im, j, col), src[im] + o, ok);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBandThreads)
+loss_forward_band_kernel(int H, int W, int hb, float C1, float C2, const float* __restrict__ pred,
+                         const float* __restrict__ target, float* __restrict__ dm_dmu1,
+                         float* __restrict__ dm_dsigma1_sq, float* __restrict__ dm_dsigma12,
+                         float2* __restrict__ partial, LossHead head) {
+  __shared__ __align__(16) float s_in[2][2 * kRing * kBandPitch];
+  const size_t plane = (size_t)blockIdx.z * H * W;
+  const int x0 = blockIdx.x * kBandThreads, x = x0 + (int)threadIdx.x;
+  const int y0 = blockIdx.y * hb, y1 = min(H, y0 + hb);
+  const int n_in = y1 - y0 + 2 * kHalo;   // input rows y0 - 5 .. y1 + 4
+  const int nchunks = (n_in + kRing - 1) / kRing;
+  const float* const src[2] = {pred + plane, target + plane};
+  float2 w2[11];
+#pragma unroll
+  for (int k = 0; k < 11; ++k) w2[k] = kSsimWin2[k];
+  // ring of horizontal moments per input row: (a, c) = (mu1, mu2), (b, d) = (E x^2, E y^2), e = E xy
+  float2 r_ac[kRing], r_bd[kRing];
+  float r_e[kRing];
+  float l1 = 0.0f, sm = 0.0f;
+  band_stage<2>(s_in[0], src, H, W, x0, y0 - kHalo);
+  cp_async_commit();
+  for (int ci = 0; ci < nchunks; ++ci) {
+    if (ci + 1 < nchunks) band_stage<2>(s_in[(ci + 1) & 1], src, H, W, x0, y0 - kHalo + (ci + 1) * kRing);
+    cp_async_commit();
+    cp_async_wait_prev();
+    __syncthreads();
+    const float2* spq = reinterpret_cast<const float2*>(s_in[ci & 1]) + threadIdx.x;   // (p, t) pairs
+#pragma unroll
+    for (int j = 0; j < kRing; ++j) {
+      const int g = ci * kRing + j;   // input row y0 - 5 + g; its ring slot is g % 11 = j
+      if (g < n_in) {
+        float2 ac = make_float2(0.0f, 0.0f), bd = make_float2(0.0f, 0.0f);
+        float e = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 11; ++k) {
+          const float2 pq = spq[j * kBandPitch + k];
+          ac = ffma2(w2[k], pq, ac);               // a += w p;      c += w q
+          bd = ffma2(w2[k], fmul2(pq, pq), bd);    // b += w (p p);  d += w (q q)
+          e = fmaf(w2[k].x, pq.x * pq.y, e);       // e += w (p q)
+        }
+        r_ac[j] = ac;
+        r_bd[j] = bd;
+        r_e[j] = e;
+        if (g >= kHalo && g < n_in - kHalo && x < W) {
+          const float2 c = spq[j * kBandPitch + kHalo];
+          l1 += fabsf(c.x - c.y);
+        }
+        if (g >= 2 * kHalo) {   // output row y0 + g - 10: window rows g - 10 .. g
+          float2 vac = make_float2(0.0f, 0.0f), vbd = make_float2(0.0f, 0.0f);
+          float ve = 0.0f;
+#pragma unroll
+          for (int k = 0; k < 11; ++k) {
+            const int s = (j + 1 + k) % kRing;
+            vac = ffma2(w2[k], r_ac[s], vac);
+            vbd = ffma2(w2[k], r_bd[s], vbd);
+            ve = fmaf(w2[k].x, r_e[s], ve);
+          }
+          if (x < W) {
+            const float v[5] = {vac.x, vbd.x, vac.y, vbd.y, ve};
+            const size_t idx = plane + (size_t)(y0 + g - 2 * kHalo) * W + x;
+            float d1, d2, d3;
+            sm += ssim_pixel(v, C1, C2, d1, d2, d3);
+            dm_dmu1[idx] = d1;
+            dm_dsigma1_sq[idx] = d2;
+            dm_dsigma12[idx] = d3;
+          }
+        }
+      }
+    }
+    __syncthreads();   // the buffer is restaged two chunks on
+  }
+  block_partial(l1, sm, partial);
+  loss_arrive(gridDim.x * gridDim.y, H * W, head, partial);
+}
+
+__global__ void __launch_bounds__(kBandThreads)
+loss_backward_band_kernel(int H, int W, int hb, const float* __restrict__ pred, const float* __restrict__ target,
+                          const float* __restrict__ dm_dmu1, const float* __restrict__ dm_dsigma1_sq,
+                          const float* __restrict__ dm_dsigma12, const float4* __restrict__ coef,
+                          float* __restrict__ dL_dpred) {
+  __shared__ __align__(16) float s_in[2][3 * kRing * kBandPitch];
+  const size_t plane = (size_t)blockIdx.z * H * W;
+  const float4 cf = coef[blockIdx.z];
+  const int x0 = blockIdx.x * kBandThreads, x = x0 + (int)threadIdx.x;
+  const int y0 = blockIdx.y * hb, y1 = min(H, y0 + hb);
+  const int n_in = y1 - y0 + 2 * kHalo;
+  const int nchunks = (n_in + kRing - 1) / kRing;
+  const float* const src[3] = {dm_dmu1 + plane, dm_dsigma1_sq + plane, dm_dsigma12 + plane};
+  float2 w2[11];
+#pragma unroll
+  for (int k = 0; k < 11; ++k) w2[k] = kSsimWin2[k];
+  float2 r_ab[kRing];   // horizontal sums of the dm/dmu1 and dm/dsigma1^2 maps
+  float r_c[kRing];     // and of dm/dsigma12
+  band_stage<3>(s_in[0], src, H, W, x0, y0 - kHalo);
+  cp_async_commit();
+  for (int ci = 0; ci < nchunks; ++ci) {
+    if (ci + 1 < nchunks) band_stage<3>(s_in[(ci + 1) & 1], src, H, W, x0, y0 - kHalo + (ci + 1) * kRing);
+    cp_async_commit();
+    // pred and target of this chunk's output rows, loaded while the chunk lands
+    float pv[kRing], tv[kRing];
+#pragma unroll
+    for (int j = 0; j < kRing; ++j) {
+      const int g = ci * kRing + j;
+      const bool ok = g >= 2 * kHalo && g < n_in && x < W;
+      const size_t idx = plane + (ok ? (size_t)(y0 + g - 2 * kHalo) * W + x : 0);
+      pv[j] = ok ? pred[idx] : 0.0f;
+      tv[j] = ok ? target[idx] : 0.0f;
+    }
+    cp_async_wait_prev();
+    {   // the staged derivative maps times the spectrum's map gradient, as the tile layout stages them
+      float* own = s_in[ci & 1];
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        const int col = (int)threadIdx.x + half * kBandThreads;
+        if (col < kBandCols)
+#pragma unroll
+          for (int j = 0; j < kRing; ++j)
+#pragma unroll
+            for (int im = 0; im < 3; ++im) own[band_slot(im, j, col)] *= cf.y;
+      }
+    }
+    __syncthreads();
+    const float2* s01 = reinterpret_cast<const float2*>(s_in[ci & 1]) + threadIdx.x;
+    const float* s2 = s_in[ci & 1] + 2 * kRing * kBandPitch + threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < kRing; ++j) {
+      const int g = ci * kRing + j;
+      if (g < n_in) {
+        float2 ab = make_float2(0.0f, 0.0f);
+        float c = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 11; ++k) {
+          ab = ffma2(w2[k], s01[j * kBandPitch + k], ab);
+          c = fmaf(w2[k].x, s2[j * kBandPitch + k], c);
+        }
+        r_ab[j] = ab;
+        r_c[j] = c;
+        if (g >= 2 * kHalo && x < W) {
+          float2 vab = make_float2(0.0f, 0.0f);
+          float vc = 0.0f;
+#pragma unroll
+          for (int k = 0; k < 11; ++k) {
+            const int s = (j + 1 + k) % kRing;
+            vab = ffma2(w2[k], r_ab[s], vab);
+            vc = fmaf(w2[k].x, r_c[s], vc);
+          }
+          const float v[3] = {vab.x, vab.y, vc};
+          const size_t idx = plane + (size_t)(y0 + g - 2 * kHalo) * W + x;
+          dL_dpred[idx] = loss_pixel_grad(v, pv[j], tv[j], cf.x);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Block layout of the loss for R spectra of H x W (the scratch layout and
+// the launch both follow it).
+struct LossGeom {
+  bool band;
+  int gx, gy, hb;
+};
+static LossGeom loss_geom(size_t R, size_t H, size_t W) {
+  LossGeom g;
+  g.band = R >= (size_t)kBandMinPlanes;
+  if (g.band) {
+    g.gx = (int)((W + kBandThreads - 1) / kBandThreads);
+    const size_t per_band = R * (size_t)g.gx;
+    size_t nb = (kBandTargetBlocks + per_band - 1) / per_band;
+    const size_t max_bands = (H + 7) / 8;   // bands of at least 8 rows
+    nb = nb < 1 ? 1 : (nb > max_bands ? max_bands : nb);
+    g.hb = (int)((H + nb - 1) / nb);
+    g.gy = (int)((H + g.hb - 1) / g.hb);
+  } else {
+    g.gx = (int)((W + kSW - 1) / kSW);
+    g.gy = (int)((H + kSH - 1) / kSH);
+    g.hb = kSH;
+  }
+  return g;
 }
 
 LossLayout loss_layout(size_t R, size_t H, size_t W, size_t hidden) {
   auto a = [](size_t x) { return (x + 63) / 64 * 64; };
+  const LossGeom g = loss_geom(R, H, W);
   LossLayout L;
   const size_t n = R * H * W;
-  L.nblk = ((W + kSW - 1) / kSW) * ((H + kSH - 1) / kSH);
+  L.nblk = (size_t)g.gx * g.gy;
   L.dmu1 = 0;
   L.ds11 = a(n);
   L.ds12 = L.ds11 + a(n);
   L.partial = L.ds12 + a(n);
   L.pre = L.partial + a(2 * R * L.nblk);
   L.coef = L.pre + a(R * hidden);
-  L.sync = L.coef + a(4 * R);
+  L.share = L.coef + a(4 * R);
+  L.psync = L.share + a(R * (5 * hidden + 1));
+  L.sync = L.psync + a(R);
   L.total = L.sync + 64;
   return L;
 }
@@ -424,18 +769,42 @@ cudaError_t launch_splat_loss(int R, int H, int W, int hidden, float lambda1, fl
                               const float* pred, const float* target, const float* rx, const float* conf_params,
                               float* scratch, float* loss_out, float* terms, float* dL_dpred, float* dconf,
                               cudaStream_t stream) {
+  const LossGeom G = loss_geom(R, H, W);
   const LossLayout L = loss_layout(R, H, W, hidden);
-  dim3 grid((W + kSW - 1) / kSW, (H + kSH - 1) / kSH, R);
   float2* partial = reinterpret_cast<float2*>(scratch + L.partial);
   float4* coef = reinterpret_cast<float4*>(scratch + L.coef);
-  loss_forward_kernel<<<grid, 256, 0, stream>>>(H, W, C1, C2, pred, target, scratch + L.dmu1, scratch + L.ds11,
-                                                scratch + L.ds12, partial, hidden, lambda1, alpha, rx, conf_params,
-                                                scratch + L.pre, coef, terms, loss_out, dconf,
-                                                reinterpret_cast<unsigned*>(scratch + L.sync));
+  LossHead head;
+  head.R = R;
+  head.hidden = hidden;
+  head.lambda1 = lambda1;
+  head.alpha = alpha;
+  head.rx = rx;
+  head.cp = conf_params;
+  head.pre = scratch + L.pre;
+  head.coef = coef;
+  head.terms = terms;
+  head.loss_out = loss_out;
+  head.dconf = dconf;
+  head.share = scratch + L.share;
+  head.psync = reinterpret_cast<unsigned*>(scratch + L.psync);
+  head.sync = reinterpret_cast<unsigned*>(scratch + L.sync);
+  const dim3 grid((unsigned)G.gx, (unsigned)G.gy, (unsigned)R);
+  if (G.band) {
+    loss_forward_band_kernel<<<grid, kBandThreads, 0, stream>>>(H, W, G.hb, C1, C2, pred, target, scratch + L.dmu1,
+                                                                scratch + L.ds11, scratch + L.ds12, partial, head);
+  } else {
+    loss_forward_kernel<<<grid, 256, 0, stream>>>(H, W, C1, C2, pred, target, scratch + L.dmu1, scratch + L.ds11,
+                                                  scratch + L.ds12, partial, head);
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  loss_backward_kernel<<<grid, 256, 0, stream>>>(H, W, pred, target, scratch + L.dmu1, scratch + L.ds11,
-                                                 scratch + L.ds12, coef, dL_dpred);
+  if (G.band) {
+    loss_backward_band_kernel<<<grid, kBandThreads, 0, stream>>>(H, W, G.hb, pred, target, scratch + L.dmu1,
+                                                                 scratch + L.ds11, scratch + L.ds12, coef, dL_dpred);
+  } else {
+    loss_backward_kernel<<<grid, 256, 0, stream>>>(H, W, pred, target, scratch + L.dmu1, scratch + L.ds11,
+                                                   scratch + L.ds12, coef, dL_dpred);
+  }
   return cudaGetLastError();
 }
 

@@ -47,7 +47,11 @@ def _reference(pred, target, rxs, mlp, lambda1=0.2, alpha=0.3):
     return loss.detach(), p.grad.detach(), grads, torch.stack([l1, s, conf], 1).detach()
 
 
-@pytest.mark.parametrize("R,H,W,hidden", [(1, 90, 360, 32), (5, 90, 360, 32), (3, 37, 53, 16), (2, 8, 8, 48)])
+# R < 16: 32x8 tile blocks; R >= 16: 128-column strips over row bands (one
+# band at R = 16 x 90x360 ... several at R = 40, single-strip images below)
+@pytest.mark.parametrize("R,H,W,hidden", [(1, 90, 360, 32), (5, 90, 360, 32), (3, 37, 53, 16), (2, 8, 8, 48),
+                                          (16, 90, 360, 32), (40, 90, 360, 32), (24, 37, 53, 16), (17, 8, 8, 48),
+                                          (16, 45, 300, 8)])
 def test_splat_loss_matches_torch_autograd(R, H, W, hidden):
     torch.backends.cudnn.allow_tf32 = False
     dev = torch.device("cuda")
@@ -76,9 +80,10 @@ def test_splat_loss_matches_torch_autograd(R, H, W, hidden):
     assert ((dconf - ref_dconf).abs() <= 1e-5 * gs + 1e-4 * ref_dconf.abs()).all()
 
 
-def test_splat_loss_is_deterministic():
+@pytest.mark.parametrize("R", [4, 20])
+def test_splat_loss_is_deterministic(R):
     dev = torch.device("cuda")
-    R, H, W = 4, 90, 360
+    H, W = 90, 360
     gen = torch.Generator().manual_seed(7)
     target = torch.rand((R, H, W), generator=gen).to(dev)
     pred = torch.rand((R, H, W), generator=gen).to(dev)
