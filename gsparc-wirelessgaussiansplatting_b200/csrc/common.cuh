@@ -499,6 +499,30 @@ __device__ __forceinline__ bool box_outside(const float4 b, float x0, float x1, 
   return b.y < x0 || b.x > x1 || b.w < y0 || b.z > y1;
 }
 
+// Two FP32 lanes per instruction (add / mul / fma .rn.f32x2, sm_100): each
+// lane rounds exactly as the scalar instruction.
+__device__ __forceinline__ unsigned long long f2_bits(float2 v) {
+  return ((unsigned long long)__float_as_uint(v.y) << 32) | __float_as_uint(v.x);
+}
+__device__ __forceinline__ float2 bits_f2(unsigned long long b) {
+  return make_float2(__uint_as_float((unsigned)b), __uint_as_float((unsigned)(b >> 32)));
+}
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
+  return bits_f2(d);
+}
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return bits_f2(d);
+}
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return bits_f2(d);
+}
+
 __device__ __forceinline__ void atomic_or_error(ImageHeader* hdr, uint32_t bits) {
   atomicOr(&hdr->error, bits);
 }

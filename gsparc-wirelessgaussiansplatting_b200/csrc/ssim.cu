@@ -510,24 +510,6 @@ __constant__ float2 kSsimWin2[11] = {
     {0.036000773310661316f, 0.036000773310661316f},   {0.0075987582094967365f, 0.0075987582094967365f},
     {0.001028380123898387f, 0.001028380123898387f}};
 
-__device__ __forceinline__ unsigned long long f2_bits(float2 v) {
-  return ((unsigned long long)__float_as_uint(v.y) << 32) | __float_as_uint(v.x);
-}
-__device__ __forceinline__ float2 bits_f2(unsigned long long b) {
-  return make_float2(__uint_as_float((unsigned)b), __uint_as_float((unsigned)(b >> 32)));
-}
-// a * b + c and a * b per lane (fma.rn.f32x2 / mul.rn.f32x2)
-__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
-  unsigned long long d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
-  return bits_f2(d);
-}
-__device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
-  unsigned long long d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
-  return bits_f2(d);
-}
-
 __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool ok) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
                "l"(src), "r"(ok ? 4 : 0)
