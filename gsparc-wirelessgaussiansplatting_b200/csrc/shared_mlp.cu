@@ -289,10 +289,12 @@ __device__ __forceinline__ void store_row(float* dst, const float* v) {
 // W [64][K] (row-major, global) -> W^T [K][64] in shared memory.  Each thread
 // takes four consecutive inputs of one output row, consecutive threads
 // consecutive outputs, so the shared-memory writes of a warp are contiguous;
-// every load is independent (all of them in flight at once).  blockDim.x must
+// every load is independent (all of them in flight at once).  When `rows` is
+// given, the row-major copy is written from the same loads.  blockDim.x must
 // be kFusedRows.
 template <int K>
-__device__ __forceinline__ void stage_transposed(float* __restrict__ dst, const float* __restrict__ W) {
+__device__ __forceinline__ void stage_transposed(float* __restrict__ dst, const float* __restrict__ W,
+                                                 float* __restrict__ rows = nullptr) {
   constexpr int kItems = kW64 * (K / 4);
 #pragma unroll
   for (int it = 0; it < (kItems + kFusedRows - 1) / kFusedRows; ++it) {
@@ -304,6 +306,7 @@ __device__ __forceinline__ void stage_transposed(float* __restrict__ dst, const 
       dst[(k + 1) * kW64 + j] = w1;
       dst[(k + 2) * kW64 + j] = w2;
       dst[(k + 3) * kW64 + j] = w3;
+      if (rows) *reinterpret_cast<float4*>(rows + j * K + k) = make_float4(w0, w1, w2, w3);
     }
   }
 }
@@ -524,14 +527,8 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
   using TL = FusedTiles<kL>;
   extern __shared__ __align__(16) float sm[];
   const int t = threadIdx.x, lane = t & 31;
-#pragma unroll 4
-  for (int i = t; i < kW64 * kFeat; i += kFusedRows) sm[TL::kW0 + i] = params[FP::kW0 + i];
-  stage_transposed<kFeat>(sm + TL::kWt0, params + FP::kW0);
-  if (kL == 2) {
-#pragma unroll 4
-    for (int i = t; i < kW64 * kW64; i += kFusedRows) sm[TL::kW1 + i] = params[FP::kW1 + i];
-    stage_transposed<kW64>(sm + TL::kWt1, params + FP::kW1);
-  }
+  stage_transposed<kFeat>(sm + TL::kWt0, params + FP::kW0, sm + TL::kW0);
+  if (kL == 2) stage_transposed<kW64>(sm + TL::kWt1, params + FP::kW1, sm + TL::kW1);
   for (int i = t; i < kW64; i += kFusedRows) {
     sm[TL::kB0 + i] = params[FP::kB0 + i];
     if (kL == 2) sm[TL::kB1 + i] = params[FP::kB1 + i];
