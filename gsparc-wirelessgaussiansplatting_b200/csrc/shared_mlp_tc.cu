@@ -54,23 +54,6 @@ constexpr uint32_t kSboA = ((kH + 16) / 8) * 128u;    // [rows x 144] K-major (a
 constexpr uint32_t kPolls = 1u << 24;
 constexpr float kPiF = 3.14159265358979323846f;
 
-// GELU's normal CDF Phi(z) = (1 + erf(z / sqrt 2)) / 2 by Abramowitz & Stegun
-// 7.1.26 (Hastings' rational approximation, |error of erf| <= 1.5e-7, three
-// orders below the BF16 rounding the results go through):
-//   erf(x) = 1 - t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2),
-//   t = 1 / (1 + p x), x >= 0, odd extension for x < 0.
-// exp(-z^2 / 2) is returned too: it is also the density term of GELU'.
-__device__ __forceinline__ float gelu_cdf(float z, float& ez) {
-  const float ax = fabsf(z) * 0.70710678118654752f;
-  ez = __expf(-0.5f * z * z);
-  const float tt = __fdividef(1.0f, fmaf(0.3275911f, ax, 1.0f));
-  float p = fmaf(tt, 1.061405429f, -1.453152027f);
-  p = fmaf(tt, p, 1.421413741f);
-  p = fmaf(tt, p, -0.284496736f);
-  p = fmaf(tt, p, 0.254829592f);
-  const float e = fmaf(-(tt * p), ez, 1.0f);   // erf(|z| / sqrt 2)
-  return 0.5f + copysignf(0.5f * e, z);
-}
 // GELU of two pre-activations at once (FP32x2) for the forward, where no
 // density term is needed: Phi from Abramowitz & Stegun 7.1.28,
 //   erf(x) = 1 - (1 + a1 x + a2 x^2 + ... + a6 x^6)^-16,  x >= 0, |error| <= 3e-7,
@@ -98,25 +81,18 @@ __device__ __forceinline__ float2 gelu2(float2 z) {
   const float2 ph = ffma2(h, fadd2(r, make_float2(-1.0f, -1.0f)), make_float2(0.5f, 0.5f));
   return fmul2(z, ph);
 }
-// activation and its derivative from one evaluation
-__device__ __forceinline__ void act_and_grad(int act, float z, float& a, float& d) {
-  if (act == 1) {
-    a = fmaxf(z, 0.0f);
-    d = z > 0.0f ? 1.0f : 0.0f;
-  } else {
-    float ez;
-    const float ph = gelu_cdf(z, ez);
-    a = z * ph;
-    d = fmaf(z * 0.39894228040143268f, ez, ph);
-  }
-}
 __device__ __forceinline__ float ex2_approx(float x) {
   float r;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
 }
-// The same for two elements at once (FP32x2), GELU by the 7.1.26 form of
-// gelu_cdf with the exponential shared with the density term:
+// Activation and derivative of two elements from one evaluation (FP32x2), for
+// the adjoint.  GELU's normal CDF Phi(z) = (1 + erf(z / sqrt 2)) / 2 by
+// Abramowitz & Stegun 7.1.26 (Hastings' rational approximation, |error of
+// erf| <= 1.5e-7, three orders below the BF16 rounding the results go through):
+//   erf(x) = 1 - t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2),
+//   t = 1 / (1 + p x), x >= 0, odd extension for x < 0,
+// whose exponential is also the density term of GELU':
 //   a = z Phi(z),  d = Phi(z) + z phi(z),  phi(z) = exp(-z^2 / 2) / sqrt(2 pi).
 __device__ __forceinline__ void act_and_grad2(int act, float2 z, float2& a, float2& d) {
   if (act == 1) {

@@ -210,9 +210,40 @@ def test_oracle_shared_mlp_matches_torch_autograd():
         assert np.abs(dmeans - m.grad.numpy()).max() <= 1e-4 * np.abs(m.grad.numpy()).max()
 
 
+def test_gelu_forward_reciprocal_power_approximation_error_bound():
+    """The BF16 tensor-core MLP's forward evaluates GELU's normal CDF with
+    Abramowitz & Stegun 7.1.28, erf(x) = 1 - (1 + a1 x + ... + a6 x^6)^-16,
+    in FP32 (one reciprocal, four squarings).  Against scipy's erf in float64:
+    the method itself within its published 3e-7; restated in float32 step for
+    step as the kernel does it (the reciprocal correctly rounded here; the
+    kernel's approximate one adds about 1 ulp before the 16th power), Phi
+    within 1.5e-6 and GELU within 1e-6 relative to max(1, |z|), below the BF16
+    rounding (2^-9 relative) that every result goes through."""
+    from scipy.special import erf
+    z = np.linspace(-9.0, 9.0, 400001).astype(np.float32)
+    f = np.float32
+    x = (np.abs(z) * f(0.70710678118654752)).astype(np.float32)
+    p = (x * f(4.30638e-5) + f(2.765672e-4)).astype(np.float32)
+    for c in (1.520143e-4, 9.2705272e-3, 4.22820123e-2, 7.05230784e-2, 1.0):
+        p = (p * x + f(c)).astype(np.float32)
+    r = (f(1.0) / p).astype(np.float32)
+    for _ in range(4):
+        r = (r * r).astype(np.float32)
+    h = np.copysign(f(0.5), -z).astype(np.float32)
+    ph = (h * (r - f(1.0)) + f(0.5)).astype(np.float32)
+    zd = z.astype(np.float64)
+    xd = np.abs(zd) / np.sqrt(2.0)
+    pd = 1.0 + xd * (0.0705230784 + xd * (0.0422820123 + xd * (0.0092705272 + xd * (0.0001520143 + xd * (
+        0.0002765672 + xd * 0.0000430638)))))
+    assert np.max(np.abs(1.0 - pd ** -16 - erf(xd))) <= 3e-7
+    phi = 0.5 * (1.0 + erf(zd / np.sqrt(2.0)))
+    assert np.max(np.abs(ph - phi)) <= 1.5e-6
+    assert np.max(np.abs(z * ph - zd * phi) / np.maximum(1.0, np.abs(zd))) <= 1e-6
+
+
 def test_gelu_cdf_rational_approximation_error_bound():
-    """The BF16 tensor-core MLP evaluates GELU's normal CDF with Abramowitz &
-    Stegun 7.1.26 (Hastings) in FP32.  Against scipy's erf in float64: the
+    """The BF16 tensor-core MLP's adjoint evaluates GELU's normal CDF with
+    Abramowitz & Stegun 7.1.26 (Hastings) in FP32.  Against scipy's erf in float64: the
     method itself (evaluated in float64) within its published 1.5e-7; restated
     in float32 step for step as the kernel does it, erf within 6e-7 and GELU /
     GELU' within 4e-7 (GELU relative to max(1, |z|)), three orders below the
