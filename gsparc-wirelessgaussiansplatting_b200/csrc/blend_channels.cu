@@ -6,21 +6,30 @@
 // single-channel kernels' (blend.cu), so final T and contributor counts equal
 // a single-channel render of the same geometry.
 //
-// Forward: one 256-thread CTA per (tile, receiver), one pixel per thread; the
-// tile's list is staged 32 entries at a time (position, conic, features), each
-// pixel keeps its C accumulators in registers: out[c] += f_c * (alpha * T).
+// The channels are split into groups of up to 16, one CTA per (tile,
+// receiver, channel group): every group walks the tile's list with the same
+// transmittance decisions, so a long list is walked by C / 16 CTAs at once,
+// each with a quarter of the per-entry work.
+//
+// Forward: one 256-thread CTA per (tile, receiver, group), one pixel per
+// thread; the tile's list is staged 32 entries at a time (position, conic, the
+// group's features), each pixel keeps the group's accumulators in registers:
+// out[c] += f_c * (alpha * T).  Group 0 writes final T and contributor counts.
 //
 // Adjoint (the true derivative; the 0.99 alpha clamp blocks the gradient):
 // back to front from each pixel's contributor count, T recomputed by division
 // from final T.  The colour behind entry j enters dL/dalpha only through its
 // dot product with dL/dout, so one scalar per pixel carries it:
 //   B_j = sum_{k>j} alpha_k T_k (f_k . g),  dL/dalpha_j = T_j (f_j . g - B_j / T_{j+1}).
+// dL/dalpha, and through it the position, conic and opacity gradients, is
+// linear in the per-channel products, so each channel group adds its share.
 // dL/df_j,c = sum over pixels of alpha_j T_j g_c is a small GEMM per staged
 // batch: the batch's (entry, pixel) weights alpha T go to shared memory and
-// every thread sums one entry's eight channels over the tile's pixels against
-// the tile's dL/dout, held in shared memory for the whole walk.  Position,
-// conic and opacity gradients are reduced per warp (warp_reduce8) and summed
-// per batch in shared memory before one global atomic per (CTA, entry, term).
+// every thread sums one entry's two channels over the pixel blocks the entry
+// reached, against the tile's dL/dout of the group, held in shared memory for
+// the whole walk.  Position, conic and opacity gradients are reduced per warp
+// (warp_reduce8) and summed per batch in shared memory before one global
+// atomic per (CTA, entry, term).
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -30,7 +39,8 @@ namespace {
 constexpr int kMcThreads = 256;   // one thread per pixel: every tile shape holds 256 pixels
 constexpr int kMcBatch = 32;      // list entries staged per round
 constexpr int kMcWs = kMcThreads + 1;   // row stride of the (entry, pixel) weights
-constexpr int kMcGs = kMaxChannels + 4;  // row stride of the tile's dL/dout: float4 rows on distinct banks
+constexpr int kMcGroupFwd = 32;          // channels per forward CTA
+constexpr int kMcGroupBwd = 64;          // channels per adjoint CTA
 }  // namespace
 
 // Pixel of thread li in its tile: every warp covers an 8x4 block, and skips
@@ -52,6 +62,7 @@ __device__ __forceinline__ McRect mc_warp_rect(int px, int py) {
   return w;
 }
 
+template <int kMcGroup>
 __global__ void __launch_bounds__(kMcThreads)
 blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const uint2* __restrict__ ranges,
                               const uint32_t* __restrict__ point_list, GeomView geo, ImageHeader* __restrict__ hdr,
@@ -61,8 +72,9 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
   __shared__ float2 s_xy[kMcBatch];
   __shared__ float4 s_co[kMcBatch];
   __shared__ float4 s_bb[kMcBatch];
-  __shared__ __align__(16) float s_f[kMcBatch][kMaxChannels];
+  __shared__ __align__(16) float s_f[kMcBatch][kMcGroup];
   const int r = blockIdx.y, tile = blockIdx.x;
+  const int c_lo = blockIdx.z * kMcGroup, Cg = min(kMcGroup, C - c_lo);   // this CTA's channels
   const int tx = tile % grid.gx, ty = tile / grid.gx;
   const int li = threadIdx.x;
   const int2 lp = mc_pixel(li, grid.tile_w);
@@ -73,11 +85,11 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
   const uint2 range = ranges[(size_t)r * grid.T + tile];
   const int n = (int)(range.y - range.x);
   const size_t roff = (size_t)r * P;
-  const int C4 = (C + 3) & ~3;
+  const int C4 = (Cg + 3) & ~3;
   float T = 1.0f;
-  float acc[kMaxChannels];
+  float acc[kMcGroup];
 #pragma unroll
-  for (int c = 0; c < kMaxChannels; ++c) acc[c] = 0.0f;
+  for (int c = 0; c < kMcGroup; ++c) acc[c] = 0.0f;
   uint32_t last = 0;
   bool done = !inside;
   for (int b0 = 0; b0 < n; b0 += kMcBatch) {
@@ -98,7 +110,7 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
     for (int i = li; i < cnt * C4; i += kMcThreads) {   // channels padded with zeros to a multiple of 4
       const int e = i / C4, c = i - e * C4;
       const uint32_t id = checked_id(point_list[range.x + b0 + e], P, hdr);
-      s_f[e][c] = c < C ? features[(roff + id) * C + c] : 0.0f;
+      s_f[e][c] = c < Cg ? features[(roff + id) * C + c_lo + c] : 0.0f;
     }
     __syncthreads();
     if (done) continue;
@@ -118,8 +130,8 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
       }
       const float w = alpha * T;
 #pragma unroll
-      for (int q = 0; q < kMaxChannels / 4; ++q)
-        if (4 * q < C) {
+      for (int q = 0; q < kMcGroup / 4; ++q)
+        if (4 * q < Cg) {
           const float4 f = *reinterpret_cast<const float4*>(&s_f[e][4 * q]);
           acc[4 * q] = fmaf(f.x, w, acc[4 * q]);
           acc[4 * q + 1] = fmaf(f.y, w, acc[4 * q + 1]);
@@ -132,16 +144,19 @@ blend_channels_forward_kernel(int P, int H, int W, int C, TileGrid grid, const u
   }
   if (inside) {
     const size_t pix = (size_t)r * H * W + (size_t)py * W + px;
-    final_T[pix] = T;
-    n_contrib[pix] = last;
+    if (blockIdx.z == 0) {
+      final_T[pix] = T;
+      n_contrib[pix] = last;
+    }
     const size_t plane = (size_t)H * W;
-    float* o = out + (size_t)r * C * plane + (size_t)py * W + px;
+    float* o = out + ((size_t)r * C + c_lo) * plane + (size_t)py * W + px;
 #pragma unroll
-    for (int c = 0; c < kMaxChannels; ++c)
-      if (c < C) o[c * plane] = acc[c];
+    for (int c = 0; c < kMcGroup; ++c)
+      if (c < Cg) o[c * plane] = acc[c];
   }
 }
 
+template <int kMcGroup>
 __global__ void __launch_bounds__(kMcThreads)
 blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const uint2* __restrict__ ranges,
                                const uint32_t* __restrict__ point_list, GeomView geo, ImageHeader* __restrict__ hdr,
@@ -150,18 +165,22 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
                                float* __restrict__ dL_dfeatures, float* __restrict__ dmean2D,
                                float* __restrict__ dconic, float* __restrict__ dopacity) {
   if (hdr->error) return;
+  constexpr int kMcGs = kMcGroup + 4;      // row stride of the tile's dL/dout: float4 rows on distinct banks
+  constexpr int kCpt = kMcGroup / 8;       // channels per thread in the dL/df GEMM
+  static_assert(kCpt % 4 == 0, "the dL/df GEMM reads float4 channel quads");
   extern __shared__ __align__(16) float mc_sm[];
-  float* s_g = mc_sm;                                   // [256 pixels][68] dL/dout of the tile
+  float* s_g = mc_sm;                                   // [256 pixels][kMcGs] dL/dout of the tile (group)
   float* s_w = s_g + kMcThreads * kMcGs;                // [kMcBatch][257] alpha T of (entry, pixel)
   __shared__ float2 s_xy[kMcBatch];
   __shared__ float4 s_co[kMcBatch];
   __shared__ float4 s_bb[kMcBatch];
   __shared__ uint32_t s_id[kMcBatch];
-  __shared__ __align__(16) float s_f[kMcBatch][kMaxChannels];
+  __shared__ __align__(16) float s_f[kMcBatch][kMcGroup];
   __shared__ float s_grad[kMcBatch][8];
   __shared__ uint32_t s_hit[kMcBatch];   // per entry: the warps with a contributing pixel
   __shared__ int s_top;
   const int r = blockIdx.y, tile = blockIdx.x;
+  const int c_lo = blockIdx.z * kMcGroup, Cg = min(kMcGroup, C - c_lo);   // this CTA's channels
   const int tx = tile % grid.gx, ty = tile / grid.gx;
   const int li = threadIdx.x, lane = li & 31;
   const int2 lp = mc_pixel(li, grid.tile_w);
@@ -175,13 +194,13 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
   const size_t pix = (size_t)r * H * W + (size_t)py * W + px;
   float T = inside ? final_T[pix] : 1.0f;
   const int last = inside ? (int)n_contrib[pix] : 0;
-  const int C4 = (C + 3) & ~3;
-  float g[kMaxChannels];
+  const int C4 = (Cg + 3) & ~3;
+  float g[kMcGroup];
 #pragma unroll
-  for (int c = 0; c < kMaxChannels; ++c)
-    g[c] = (inside && c < C) ? dL_dout[(size_t)r * C * plane + c * plane + (size_t)py * W + px] : 0.0f;
+  for (int c = 0; c < kMcGroup; ++c)
+    g[c] = (inside && c < Cg) ? dL_dout[((size_t)r * C + c_lo + c) * plane + (size_t)py * W + px] : 0.0f;
 #pragma unroll
-  for (int q = 0; q < kMaxChannels / 4; ++q)
+  for (int q = 0; q < kMcGroup / 4; ++q)
     *reinterpret_cast<float4*>(s_g + li * kMcGs + 4 * q) = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
   if (li == 0) s_top = 0;
   for (int i = li; i < kMcBatch * 8; i += kMcThreads) (&s_grad[0][0])[i] = 0.0f;
@@ -212,7 +231,7 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
     for (int i = li; i < cnt * C4; i += kMcThreads) {   // channels padded with zeros to a multiple of 4
       const int e = i / C4, c = i - e * C4;
       const uint32_t id = checked_id(point_list[range.x + lo + e], P, hdr);
-      s_f[e][c] = c < C ? features[(roff + id) * C + c] : 0.0f;
+      s_f[e][c] = c < Cg ? features[(roff + id) * C + c_lo + c] : 0.0f;
     }
     __syncthreads();
     for (int e = cnt - 1; e >= 0; --e) {
@@ -233,8 +252,8 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
         const float Tn = T * __frcp_rn(1.f - alpha);
         float fg = 0.0f;
 #pragma unroll
-        for (int q = 0; q < kMaxChannels / 4; ++q)
-          if (4 * q < C) {
+        for (int q = 0; q < kMcGroup / 4; ++q)
+          if (4 * q < Cg) {
             const float4 f = *reinterpret_cast<const float4*>(&s_f[e][4 * q]);
             fg = fmaf(f.x, g[4 * q], fg);
             fg = fmaf(f.y, g[4 * q + 1], fg);
@@ -274,11 +293,13 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
       }
     }
     __syncthreads();
-    // dL/df for the batch: thread = (entry e, eight channels c0..c0+7), summed over the tile's pixels
+    // dL/df for the batch: thread = (entry e, kCpt channels from c0), summed over the tile's pixels
     {
-      const int e = li >> 3, c0 = (li & 7) * 8;
-      if (e < cnt && c0 < C) {
-        float y[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      const int e = li >> 3, c0 = (li & 7) * kCpt;
+      if (e < cnt && c0 < Cg) {
+        float y[kCpt];
+#pragma unroll
+        for (int k = 0; k < kCpt; ++k) y[k] = 0.0f;
         const float* wrow = s_w + e * kMcWs;
         // only the warps (32-pixel blocks) where the entry contributed have nonzero weights
         for (uint32_t m = s_hit[e]; m; m &= m - 1) {
@@ -286,18 +307,20 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
 #pragma unroll 4
           for (int p = p0; p < p0 + 32; ++p) {
             const float wv = wrow[p];
-            const float4 ga = *reinterpret_cast<const float4*>(s_g + p * kMcGs + c0);
-            const float4 gb = *reinterpret_cast<const float4*>(s_g + p * kMcGs + c0 + 4);
-            y[0] = fmaf(wv, ga.x, y[0]); y[1] = fmaf(wv, ga.y, y[1]);
-            y[2] = fmaf(wv, ga.z, y[2]); y[3] = fmaf(wv, ga.w, y[3]);
-            y[4] = fmaf(wv, gb.x, y[4]); y[5] = fmaf(wv, gb.y, y[5]);
-            y[6] = fmaf(wv, gb.z, y[6]); y[7] = fmaf(wv, gb.w, y[7]);
+#pragma unroll
+            for (int k = 0; k < kCpt; k += 4) {
+              const float4 gv = *reinterpret_cast<const float4*>(s_g + p * kMcGs + c0 + k);
+              y[k] = fmaf(wv, gv.x, y[k]);
+              y[k + 1] = fmaf(wv, gv.y, y[k + 1]);
+              y[k + 2] = fmaf(wv, gv.z, y[k + 2]);
+              y[k + 3] = fmaf(wv, gv.w, y[k + 3]);
+            }
           }
         }
-        float* dst = dL_dfeatures + (roff + s_id[e]) * C;
+        float* dst = dL_dfeatures + (roff + s_id[e]) * C + c_lo;
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
-          if (c0 + k < C && y[k] != 0.0f) atomicAdd(dst + c0 + k, y[k]);
+        for (int k = 0; k < kCpt; ++k)
+          if (c0 + k < Cg && y[k] != 0.0f) atomicAdd(dst + c0 + k, y[k]);
       }
       if (li < cnt) {
         const size_t rg = roff + s_id[li];
@@ -321,14 +344,14 @@ blend_channels_backward_kernel(int P, int H, int W, int C, TileGrid grid, const 
 }
 
 static size_t blend_channels_backward_smem() {
-  return ((size_t)kMcThreads * kMcGs + (size_t)kMcBatch * kMcWs) * sizeof(float);
+  return ((size_t)kMcThreads * (kMcGroupBwd + 4) + (size_t)kMcBatch * kMcWs) * sizeof(float);
 }
 
 cudaError_t launch_blend_channels_forward(int P, int R, int H, int W, int C, const TileGrid& grid,
                                           const GeomView& geo, const ImageView& img, const BinningView& bin,
                                           const float* features, float* out, cudaStream_t s) {
-  dim3 g((unsigned)grid.T, (unsigned)R);
-  blend_channels_forward_kernel<<<g, kMcThreads, 0, s>>>(P, H, W, C, grid, img.ranges, bin.point_list, geo, img.hdr,
+  dim3 g((unsigned)grid.T, (unsigned)R, (unsigned)((C + kMcGroupFwd - 1) / kMcGroupFwd));
+  blend_channels_forward_kernel<kMcGroupFwd><<<g, kMcThreads, 0, s>>>(P, H, W, C, grid, img.ranges, bin.point_list, geo, img.hdr,
                                                          features, img.final_T, img.n_contrib, out);
   return cudaGetLastError();
 }
@@ -343,12 +366,13 @@ cudaError_t launch_blend_channels_backward(int P, int R, int H, int W, int C, co
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64 || !attr_done[dev]) {
-    e = cudaFuncSetAttribute(blend_channels_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(blend_channels_backward_kernel<kMcGroupBwd>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
     if (e != cudaSuccess) return e;
     if (dev >= 0 && dev < 64) attr_done[dev] = true;
   }
-  dim3 g((unsigned)grid.T, (unsigned)R);
-  blend_channels_backward_kernel<<<g, kMcThreads, smem, s>>>(P, H, W, C, grid, img.ranges, bin.point_list, geo,
+  dim3 g((unsigned)grid.T, (unsigned)R, (unsigned)((C + kMcGroupBwd - 1) / kMcGroupBwd));
+  blend_channels_backward_kernel<kMcGroupBwd><<<g, kMcThreads, smem, s>>>(P, H, W, C, grid, img.ranges, bin.point_list, geo,
                                                              img.hdr, features, img.final_T, img.n_contrib, dL_dout,
                                                              dL_dfeatures, dmean2D, dconic, dopacity);
   return cudaGetLastError();

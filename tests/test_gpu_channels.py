@@ -33,7 +33,9 @@ def _render(sc, mlp, params, tile=(16, 16), wrap=False):
     return out, radii, st
 
 
-@pytest.mark.parametrize("C,R,tile,wrap", [(8, 2, (16, 16), False), (64, 1, (8, 32), True), (3, 1, (32, 8), False)])
+# 16 channels per CTA: C = 8 and 3 run one group, 64 four, 21 a full and a 5-channel group
+@pytest.mark.parametrize("C,R,tile,wrap", [(8, 2, (16, 16), False), (64, 1, (8, 32), True), (3, 1, (32, 8), False),
+                                           (21, 2, (16, 16), True)])
 def test_channels_forward_and_adjoint_match_oracle(C, R, tile, wrap):
     P = 3000
     sc = _scene(P, R, seed=5)
