@@ -329,11 +329,18 @@ __device__ __forceinline__ void gemm_8x8(const float* __restrict__ AT, int lda, 
     const float4 b0 = *reinterpret_cast<const float4*>(BT + k * ldb + c0);
     const float4 b1 = *reinterpret_cast<const float4*>(BT + k * ldb + c0 + 32);
     const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-    const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+    const float2 b[4] = {make_float2(b0.x, b0.y), make_float2(b0.z, b0.w), make_float2(b1.x, b1.y),
+                         make_float2(b1.z, b1.w)};
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < 8; ++i) {
+      const float2 ai = make_float2(a[i], a[i]);
 #pragma unroll
-      for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+      for (int j = 0; j < 4; ++j) {   // two columns per FP32x2 FMA, each lane rounded as fmaf
+        const float2 c = ffma2(ai, b[j], make_float2(acc[i][2 * j], acc[i][2 * j + 1]));
+        acc[i][2 * j] = c.x;
+        acc[i][2 * j + 1] = c.y;
+      }
+    }
   }
 }
 
@@ -447,11 +454,17 @@ __device__ __forceinline__ void gemm_8x4(const float* __restrict__ AT, int lda, 
     const float4 a1 = *reinterpret_cast<const float4*>(AT + k * lda + r0 + 64);
     const float4 b0 = *reinterpret_cast<const float4*>(B + k * ldb + c0);
     const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-    const float b[4] = {b0.x, b0.y, b0.z, b0.w};
+    const float2 b[2] = {make_float2(b0.x, b0.y), make_float2(b0.z, b0.w)};
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < 8; ++i) {
+      const float2 ai = make_float2(a[i], a[i]);
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+      for (int j = 0; j < 2; ++j) {
+        const float2 c = ffma2(ai, b[j], make_float2(acc[i][2 * j], acc[i][2 * j + 1]));
+        acc[i][2 * j] = c.x;
+        acc[i][2 * j + 1] = c.y;
+      }
+    }
   }
 }
 
@@ -488,8 +501,13 @@ __device__ __forceinline__ void tile_outer(const float* __restrict__ D, const fl
     const float dd[4] = {d.x, d.y, d.z, d.w};
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
+      const float2 du = make_float2(dd[u], dd[u]);
 #pragma unroll
-      for (int i = 0; i < NI; ++i) acc[u][i] = fmaf(dd[u], a[i], acc[u][i]);
+      for (int i = 0; i < NI; i += 2) {   // two inputs per FP32x2 FMA, each lane rounded as fmaf
+        const float2 c = ffma2(du, make_float2(a[i], a[i + 1]), make_float2(acc[u][i], acc[u][i + 1]));
+        acc[u][i] = c.x;
+        acc[u][i + 1] = c.y;
+      }
       if (bias) bsum[u] += dd[u];
     }
   }
