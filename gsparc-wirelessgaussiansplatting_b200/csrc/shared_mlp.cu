@@ -513,31 +513,35 @@ __device__ __forceinline__ void tile_outer(const float* __restrict__ D, const fl
   }
 }
 
-// the thread's 8x8 GEMM block column c (j = 0..7) and row (i = 0..7) indices
-__device__ __forceinline__ int blk_col(int c0, int j) { return c0 + (j & 3) + (j >> 2) * 32; }
+// the thread's GEMM block row (i = 0..7) indices: r0..r0+3, r0+64..r0+67
 __device__ __forceinline__ int blk_row(int r0, int i) { return r0 + (i & 3) + (i >> 2) * 64; }
 
-// v[8][8] of the thread's block -> T [col][row] (transposed tile, 128 rows)
-__device__ __forceinline__ void store_block_T(float* T, int r0, int c0, const float (&v)[8][8]) {
+// The adjoint runs 256 threads on each 128-row tile (8 warps per SM where the
+// tile buffers allow one CTA): every GEMM over the tile's 64 columns uses 8x4
+// register blocks (16 row groups x 16 column groups); the per-row phases
+// (features, output layer) and the 32-wide ones (dW0, dX) run on the first
+// 128 threads with the forward's mapping.  Each element's sum keeps its order
+// (k ascending, rows ascending), so the results are those of 8x8 blocks.
+constexpr int kAdjThreads = 256;
+
+// v[8][4] of the thread's block (rows r0..r0+3, r0+64..r0+67; columns c0..c0+3)
+// -> T [col][row] (transposed tile, 128 rows)
+__device__ __forceinline__ void store_block4_T(float* T, int r0, int c0, const float (&v)[8][4]) {
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int c = blk_col(c0, j);
-    *reinterpret_cast<float4*>(T + c * kFusedRows + r0) = make_float4(v[0][j], v[1][j], v[2][j], v[3][j]);
-    *reinterpret_cast<float4*>(T + c * kFusedRows + r0 + 64) = make_float4(v[4][j], v[5][j], v[6][j], v[7][j]);
+  for (int j = 0; j < 4; ++j) {
+    *reinterpret_cast<float4*>(T + (c0 + j) * kFusedRows + r0) = make_float4(v[0][j], v[1][j], v[2][j], v[3][j]);
+    *reinterpret_cast<float4*>(T + (c0 + j) * kFusedRows + r0 + 64) = make_float4(v[4][j], v[5][j], v[6][j], v[7][j]);
   }
 }
-// v[8][8] -> D [row][col] (row tiles, stride kHs)
-__device__ __forceinline__ void store_block_rows(float* D, int r0, int c0, const float (&v)[8][8]) {
+// v[8][4] -> D [row][col] (row tiles, stride kHs)
+__device__ __forceinline__ void store_block4_rows(float* D, int r0, int c0, const float (&v)[8][4]) {
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = blk_row(r0, i);
-    *reinterpret_cast<float4*>(D + r * kHs + c0) = make_float4(v[i][0], v[i][1], v[i][2], v[i][3]);
-    *reinterpret_cast<float4*>(D + r * kHs + c0 + 32) = make_float4(v[i][4], v[i][5], v[i][6], v[i][7]);
-  }
+  for (int i = 0; i < 8; ++i)
+    *reinterpret_cast<float4*>(D + blk_row(r0, i) * kHs + c0) = make_float4(v[i][0], v[i][1], v[i][2], v[i][3]);
 }
 
 template <int kL, int kAct>
-__global__ void __launch_bounds__(kFusedRows, 1)
+__global__ void __launch_bounds__(kAdjThreads, 1)
 mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, const float* __restrict__ rx_pos,
                       const float* __restrict__ params, const int* __restrict__ radii,
                       const float* __restrict__ dL_dsignal, float* __restrict__ dX, float* __restrict__ dparams) {
@@ -545,15 +549,18 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
   using TL = FusedTiles<kL>;
   extern __shared__ __align__(16) float sm[];
   const int t = threadIdx.x, lane = t & 31;
-  stage_transposed<kFeat>(sm + TL::kWt0, params + FP::kW0, sm + TL::kW0);
-  if (kL == 2) stage_transposed<kW64>(sm + TL::kWt1, params + FP::kW1, sm + TL::kW1);
-  for (int i = t; i < kW64; i += kFusedRows) {
+  const bool row_thread = t < kFusedRows;   // one tile row per thread in the per-row phases
+  if (row_thread) {
+    stage_transposed<kFeat>(sm + TL::kWt0, params + FP::kW0, sm + TL::kW0);
+    if (kL == 2) stage_transposed<kW64>(sm + TL::kWt1, params + FP::kW1, sm + TL::kW1);
+  }
+  for (int i = t; i < kW64; i += kAdjThreads) {
     sm[TL::kB0 + i] = params[FP::kB0 + i];
     if (kL == 2) sm[TL::kB1 + i] = params[FP::kB1 + i];
     sm[TL::kWo + i] = params[FP::kWo + i];
   }
   if (t == 0) sm[TL::kBo] = params[FP::kBo];
-  for (int i = t; i < kW64 + 4; i += kFusedRows) sm[TL::kDwo + i] = 0.0f;
+  for (int i = t; i < kW64 + 4; i += kAdjThreads) sm[TL::kDwo + i] = 0.0f;
   float* XT = sm + TL::kXT;
   float* Xr = sm + TL::kX;
   float* HT = sm + TL::kHT;
@@ -563,17 +570,18 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
   float* sdO = sm + TL::kDO;
   float* dwo = sm + TL::kDwo;
   const float* wo = sm + TL::kWo;
-  const int r0 = (t & 15) * 4, c0 = (t >> 4) * 4;   // GEMM block of this thread (as the forward)
-  const int j0 = (t >> 3) * 4;                      // weight-gradient blocks
-  const bool bias_owner = (t & 7) == 0;
-  float g1[4][8] = {}, gb1[4] = {};   // dW1: outputs j0..j0+3 x inputs (t & 7) * 8 ..+7, accumulated over tiles
-  float g0[4][4] = {}, gb0[4] = {};   // dW0: outputs j0..j0+3 x features (t & 7) * 4 ..+3
+  const int r0 = (t & 15) * 4, c0 = (t >> 4) * 4;    // 8x4 block over the 64 columns
+  const int r0x = (t & 15) * 4, c0x = (t >> 4) * 4;  // dX (32 columns, first 128 threads)
+  const int j1 = (t >> 4) * 4, i1 = (t & 15) * 4;    // dW1: outputs j1..j1+3 x inputs i1..i1+3
+  const int j0 = (t >> 3) * 4, i0 = (t & 7) * 4;     // dW0: outputs j0..j0+3 x features i0..i0+3 (first 128)
+  float g1[4][4] = {}, gb1[4] = {};   // accumulated over tiles
+  float g0[4][4] = {}, gb0[4] = {};
   const size_t ntiles = (rows + kFusedRows - 1) / kFusedRows;
   for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const size_t row = tile * kFusedRows + t;
-    const bool vis = row < rows && radii[row] > 0;
+    const bool vis = row_thread && row < rows && radii[row] > 0;
     __syncthreads();   // weights staged / the previous tile's reads done
-    {
+    if (row_thread) {
       float x[kFeat];
       if (vis) pair_features_fp32(means3D, rx_pos, (int)(row % P), (int)(row / P), x);
       else
@@ -585,36 +593,36 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
     }
     __syncthreads();
     // ---- forward recompute (the sums of mlp64_forward_kernel)
-    float acc[8][8];
+    float acc[8][4];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
-    gemm_8x8<kFeat>(XT, kFusedRows, sm + TL::kWt0, kW64, r0, c0, acc);
+      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+    gemm_8x4<kFeat>(XT, kFusedRows, sm + TL::kWt0, kW64, r0, c0, acc);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const float b = sm[TL::kB0 + blk_col(c0, j)];
+    for (int j = 0; j < 4; ++j) {
+      const float b = sm[TL::kB0 + c0 + j];
 #pragma unroll
       for (int i = 0; i < 8; ++i) acc[i][j] += b;
     }
     if (kL == 2) {
-      float h[8][8], gd[8][8];
+      float h[8][4], gd[8][4];
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) act_both(kAct, acc[i][j], h[i][j], gd[i][j]);
-      store_block_T(HT, r0, c0, h);
-      store_block_rows(A0, r0, c0, h);
-      store_block_T(G0T, r0, c0, gd);
+        for (int j = 0; j < 4; ++j) act_both(kAct, acc[i][j], h[i][j], gd[i][j]);
+      store_block4_T(HT, r0, c0, h);
+      store_block4_rows(A0, r0, c0, h);
+      store_block4_T(G0T, r0, c0, gd);
       __syncthreads();
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
-      gemm_8x8<kW64>(HT, kFusedRows, sm + TL::kWt1, kW64, r0, c0, acc);
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+      gemm_8x4<kW64>(HT, kFusedRows, sm + TL::kWt1, kW64, r0, c0, acc);
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const float b = sm[TL::kB1 + blk_col(c0, j)];
+      for (int j = 0; j < 4; ++j) {
+        const float b = sm[TL::kB1 + c0 + j];
 #pragma unroll
         for (int i = 0; i < 8; ++i) acc[i][j] += b;
       }
@@ -622,15 +630,15 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
     }
     // acc = Z of the last hidden layer.  Its activations -> HT, output per row
     {
-      float h[8][8];
+      float h[8][4];
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) h[i][j] = act_fwd(kAct, acc[i][j]);
-      store_block_T(HT, r0, c0, h);
+        for (int j = 0; j < 4; ++j) h[i][j] = act_fwd(kAct, acc[i][j]);
+      store_block4_T(HT, r0, c0, h);
     }
     __syncthreads();
-    {
+    if (row_thread) {
       float o = 0.0f;
 #pragma unroll 8
       for (int j = 0; j < kW64; ++j) o = fmaf(HT[j * kFusedRows + t], wo[j], o);
@@ -648,69 +656,68 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
       float dOr[8];
 #pragma unroll
       for (int i = 0; i < 8; ++i) dOr[i] = sdO[blk_row(r0, i)];
-      float part[8];
+      float part[4];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
+      for (int j = 0; j < 4; ++j) {
         float p = 0.0f;
 #pragma unroll
         for (int i = 0; i < 8; ++i) p = fmaf(dOr[i], act_fwd(kAct, acc[i][j]), p);
         part[j] = p;
       }
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
+      for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int q = 8; q > 0; q >>= 1) part[j] += __shfl_xor_sync(0xffffffffu, part[j], q);
       if ((t & 15) == 0)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) atomicAdd(&dwo[blk_col(c0, j)], part[j]);
+        for (int j = 0; j < 4; ++j) atomicAdd(&dwo[c0 + j], part[j]);
       // dZ of the last hidden layer -> rows (D) and transposed (HT)
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const float w = wo[blk_col(c0, j)];
+      for (int j = 0; j < 4; ++j) {
+        const float w = wo[c0 + j];
 #pragma unroll
         for (int i = 0; i < 8; ++i) acc[i][j] = dOr[i] * w * act_grad(kAct, acc[i][j]);
       }
-      store_block_rows(D, r0, c0, acc);
-      store_block_T(HT, r0, c0, acc);
+      store_block4_rows(D, r0, c0, acc);
+      store_block4_T(HT, r0, c0, acc);
     }
     __syncthreads();
     if (kL == 2) {
       // second layer: dW1 += dZ1^T A0, db1 += column sums of dZ1
-      tile_outer<8, kHs>(D, A0, j0, (t & 7) * 8, bias_owner, g1, gb1);
+      tile_outer<4, kHs>(D, A0, j1, i1, (t & 15) == 0, g1, gb1);
       // dZ0 = (dZ1 W1) * act'(Z0)
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
-      gemm_8x8<kW64>(HT, kFusedRows, sm + TL::kW1, kW64, r0, c0, acc);
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+      gemm_8x4<kW64>(HT, kFusedRows, sm + TL::kW1, kW64, r0, c0, acc);
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int c = blk_col(c0, j);
-        const float4 ga = *reinterpret_cast<const float4*>(G0T + c * kFusedRows + r0);
-        const float4 gb = *reinterpret_cast<const float4*>(G0T + c * kFusedRows + r0 + 64);
+      for (int j = 0; j < 4; ++j) {
+        const float4 ga = *reinterpret_cast<const float4*>(G0T + (c0 + j) * kFusedRows + r0);
+        const float4 gb = *reinterpret_cast<const float4*>(G0T + (c0 + j) * kFusedRows + r0 + 64);
         acc[0][j] *= ga.x; acc[1][j] *= ga.y; acc[2][j] *= ga.z; acc[3][j] *= ga.w;
         acc[4][j] *= gb.x; acc[5][j] *= gb.y; acc[6][j] *= gb.z; acc[7][j] *= gb.w;
       }
       __syncthreads();   // D (dZ1) and HT (dZ1^T) fully read
-      store_block_rows(D, r0, c0, acc);
-      store_block_T(HT, r0, c0, acc);
+      store_block4_rows(D, r0, c0, acc);
+      store_block4_T(HT, r0, c0, acc);
       __syncthreads();
     }
-    // first layer: dW0 += dZ0^T X, db0 += column sums of dZ0
-    tile_outer<4, kXs>(D, Xr, j0, (t & 7) * 4, bias_owner, g0, gb0);
-    // dX = dZ0 W0 (feature gradient, to HBM)
-    {
+    if (row_thread) {
+      // first layer: dW0 += dZ0^T X, db0 += column sums of dZ0
+      tile_outer<4, kXs>(D, Xr, j0, i0, (t & 7) == 0, g0, gb0);
+      // dX = dZ0 W0 (feature gradient, to HBM)
       float dx[8][4];
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) dx[i][j] = 0.0f;
-      gemm_8x4<kW64>(HT, kFusedRows, sm + TL::kW0, kFeat, r0, c0, dx);
+      gemm_8x4<kW64>(HT, kFusedRows, sm + TL::kW0, kFeat, r0x, c0x, dx);
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        const size_t rr = tile * kFusedRows + blk_row(r0, i);
+        const size_t rr = tile * kFusedRows + blk_row(r0x, i);
         if (rr < rows)
-          *reinterpret_cast<float4*>(dX + rr * kFeat + c0) = make_float4(dx[i][0], dx[i][1], dx[i][2], dx[i][3]);
+          *reinterpret_cast<float4*>(dX + rr * kFeat + c0x) = make_float4(dx[i][0], dx[i][1], dx[i][2], dx[i][3]);
       }
     }
   }
@@ -718,16 +725,18 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
   // this CTA's share -> global
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
+    if (row_thread) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) atomicAdd(&dparams[FP::kW0 + (size_t)(j0 + u) * kFeat + (t & 7) * 4 + i], g0[u][i]);
-    if (bias_owner) atomicAdd(&dparams[FP::kB0 + j0 + u], gb0[u]);
+      for (int i = 0; i < 4; ++i) atomicAdd(&dparams[FP::kW0 + (size_t)(j0 + u) * kFeat + i0 + i], g0[u][i]);
+      if ((t & 7) == 0) atomicAdd(&dparams[FP::kB0 + j0 + u], gb0[u]);
+    }
     if (kL == 2) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) atomicAdd(&dparams[FP::kW1 + (size_t)(j0 + u) * kW64 + (t & 7) * 8 + i], g1[u][i]);
-      if (bias_owner) atomicAdd(&dparams[FP::kB1 + j0 + u], gb1[u]);
+      for (int i = 0; i < 4; ++i) atomicAdd(&dparams[FP::kW1 + (size_t)(j1 + u) * kW64 + i1 + i], g1[u][i]);
+      if ((t & 15) == 0) atomicAdd(&dparams[FP::kB1 + j1 + u], gb1[u]);
     }
   }
-  for (int j = t; j <= kW64; j += kFusedRows) atomicAdd(&dparams[FP::kWo + j], dwo[j]);   // kWo + 64 = kBo
+  for (int j = t; j <= kW64; j += kAdjThreads) atomicAdd(&dparams[FP::kWo + j], dwo[j]);   // kWo + 64 = kBo
 }
 
 template <int kL, int kAct>
@@ -761,7 +770,7 @@ static cudaError_t launch_fused(bool fwd, int P, size_t rows, const float* means
     return cudaGetLastError();
   }
   const unsigned grid = (unsigned)(ntiles < (size_t)sms ? ntiles : (size_t)sms);
-  mlp64_backward_kernel<kL, kAct><<<grid, kFusedRows, smem, s>>>(P, rows, means3D, rx_pos, params, geo.radii,
+  mlp64_backward_kernel<kL, kAct><<<grid, kAdjThreads, smem, s>>>(P, rows, means3D, rx_pos, params, geo.radii,
                                                                  dL_dsignal, work + L.d0, dparams);
   return cudaGetLastError();
 }
