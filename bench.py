@@ -28,8 +28,9 @@ shared MLP 3x128 GELU): the training step with 32 receivers per step and the
 MLP in BF16 on the tcgen05 tensor cores, against the plain per-receiver FP32
 step, in spectra/s, with the SSIM difference of their renders.
 Also reported: the same step with the reference's per-Gaussian emission MLPs,
-the eager drop-in path (reference call surface), a 16-receiver batched step
-and per-kernel device times (eager runs of the same step; graph replays
+the eager drop-in path (reference call surface), a 16-receiver batched step,
+16-receiver inference with the evaluation metrics of train.py:672-701
+(forward-only render + one batched metrics launch), and per-kernel device times (eager runs of the same step; graph replays
 bypass the library's event hooks).
 N > 1: one process per GPU (torchrun), receivers sharded, Gaussians
 replicated, gradients all-reduced over NCCL every step (weak scaling).
@@ -373,6 +374,12 @@ def run_ours(args):
     btr.plan.check()
     batched16 = {"receivers_per_step": POOL, "steps_per_s": n_b * world / bsec,
                  "spectra_per_s": n_b * POOL * world / bsec}
+    # inference: forward-only render of the 16 receivers and their batched
+    # evaluation (PSNR, RSSI difference, MAE, SSIM, confidence, loss per spectrum)
+    isec = timed(lambda i: btr.evaluate(views_d, rxs_d, tx, targets_d), n_b)
+    btr.plan.check()
+    inference16 = {"receivers_per_call": POOL, "spectra_per_s": n_b * POOL * world / isec,
+                   "metrics": ["psnr", "rssi_diff", "mae", "ssim", "confidence", "loss"]}
     del btr
 
     # ---- 50,000 clustered Gaussians, 64 receivers per step, tile shape autotuned
@@ -496,6 +503,7 @@ def run_ours(args):
                 "reference_mlp_steps_per_s": n_ref * world / ref_sec,
                 "dropin_eager_steps_per_s": dropin,
                 "batched": batched16,
+                "inference_eval": inference16,
                 "path": "CUDA-graph-captured step (gsparc_b200.fused.FusedTrainer): flat training state, shared "
                         "emission MLP, fused L1+SSIM+confidence loss, fused activation-adjoint Adam; binning "
                         f"capacity {capacity}",

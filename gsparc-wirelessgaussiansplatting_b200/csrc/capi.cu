@@ -47,7 +47,7 @@ bool valid_tile(int th, int tw) {
 enum KernelId {
   KID_PREPROCESS, KID_CHECK, KID_SCATTER, KID_DEPTH_SORT, KID_PLACE, KID_BLEND_FWD, KID_BLEND_BWD,
   KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_ADAM, KID_LOSS, KID_ACTIVATE, KID_SHARED_MLP, KID_SHARED_MLP_BWD,
-  KID_BLEND_MC_FWD, KID_BLEND_MC_BWD,
+  KID_BLEND_MC_FWD, KID_BLEND_MC_BWD, KID_EVAL,
   KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
@@ -55,7 +55,8 @@ const char* const kKernelNames[KID_COUNT] = {
     "depth_sort_kernels", "segment_place_kernel", "blend_forward_kernel", "blend_backward_kernel", "geometry_backward_kernel",
     "emission_backward_kernel", "ssim_forward_kernel", "ssim_backward_kernel", "mark_visible_kernel",
     "gaussian_adam_kernels", "splat_loss_kernels", "gaussian_activate_kernel", "shared_mlp_forward_kernels",
-    "shared_mlp_backward_kernels", "blend_channels_forward_kernel", "blend_channels_backward_kernel"};
+    "shared_mlp_backward_kernels", "blend_channels_forward_kernel", "blend_channels_backward_kernel",
+    "eval_metrics_kernel"};
 
 struct PendingTiming {
   int id;
@@ -109,7 +110,7 @@ int report_cuda(cudaError_t e, const char* where) { return cuda_fail(e, where); 
 
 extern "C" {
 
-int gsparc_abi_version(void) { return 5; }
+int gsparc_abi_version(void) { return 6; }
 
 const char* gsparc_status_string(int status) {
   switch (status) {
@@ -554,6 +555,30 @@ int gsparc_splat_loss(int R, int H, int W, int hidden, float lambda1, float alph
   GS_CHECK(launch_splat_loss(R, H, W, hidden, lambda1, alpha, C1, C2, pred, target, rx_pos, conf_params, scratch,
                              loss_out, terms, dL_dpred, dL_dconf_params, s),
            "splat loss");
+  return GSPARC_OK;
+}
+
+// ---- evaluation metrics --------------------------------------------------------
+
+size_t gsparc_eval_scratch_floats(int R, int H, int W) {
+  if (R < 0 || H < 0 || W < 0) return 0;
+  return eval_scratch_floats((size_t)R, (size_t)H, (size_t)W);
+}
+
+int gsparc_eval_metrics(int R, int H, int W, int hidden, float lambda1, float C1, float C2, const float* pred,
+                        const float* target, const float* rx_pos, const float* conf_params, float* scratch,
+                        float* metrics, void* stream) {
+  if (R < 1 || H < 1 || W < 1) return invalid("R, H and W must be positive");
+  if (R > 65535 || (H + 7) / 8 > 65535) return invalid("R or H too large for the block grid");
+  if ((size_t)H * W > (size_t)INT32_MAX) return invalid("H*W too large");
+  if (hidden < 1 || hidden > 4096) return invalid("hidden must be in [1, 4096]");
+  if (!pred || !target || !rx_pos || !conf_params || !scratch || !metrics) return invalid("null pointer");
+  if (((uintptr_t)scratch) & 15u) return invalid("scratch must be 16-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  Timed t(KID_EVAL, s);
+  GS_CHECK(launch_eval_metrics(R, H, W, hidden, lambda1, C1, C2, pred, target, rx_pos, conf_params, scratch, metrics,
+                               s),
+           "eval metrics");
   return GSPARC_OK;
 }
 

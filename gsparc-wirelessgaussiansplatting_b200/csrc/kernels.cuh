@@ -67,6 +67,10 @@ cudaError_t launch_gaussian_activate(int P, const float* params, float* act_scal
                                      float* act_opac, cudaStream_t stream);
 
 LossLayout loss_layout(size_t R, size_t H, size_t W, size_t hidden);
+size_t eval_scratch_floats(size_t R, size_t H, size_t W);
+cudaError_t launch_eval_metrics(int R, int H, int W, int hidden, float lambda1, float C1, float C2, const float* pred,
+                                const float* target, const float* rx, const float* conf_params, float* scratch,
+                                float* metrics, cudaStream_t stream);
 
 cudaError_t launch_splat_loss(int R, int H, int W, int hidden, float lambda1, float alpha, float C1, float C2,
                               const float* pred, const float* target, const float* rx, const float* conf_params,

@@ -370,13 +370,100 @@ __device__ __forceinline__ void block_partial(float l1, float sm, float2* __rest
   }
 }
 
+// ---- evaluation metrics (train.py:76-102, 686-694) ---------------------------
+// Per spectrum: PSNR = 20 log10(1 / sqrt(mse)) (infinite when mse = 0), the
+// RSSI difference 10 log10(mean pred^2) - 10 log10(mean target^2) (the -30 dBm
+// reference cancels), MAE, mean SSIM (the window SSIM of utils.py:81-114,
+// the same map), the confidence 1 + exp(fc2(relu(fc1(rx)))) and the
+// evaluation loss (1 - lambda1) MAE + lambda1 (1 - SSIM).  The SSIM pass of
+// the loss runs without its map derivatives and sums five per-block values.
+struct EvalOut {
+  float* partial;     // [R][nblk][kEvalSums]
+  unsigned* psync;    // [R] arrivals per spectrum
+  const float* rx;    // [R][3]
+  const float* cp;    // confidence MLP
+  int hidden;
+  float lambda1;
+  float* metrics;     // [R][GSPARC_EVAL_METRICS]
+};
+constexpr int kEvalSums = 8;   // |p - t|, map, (p - t)^2, p^2, t^2, (three unused)
+
+__device__ void eval_spectrum_head(int r, int nblk, int HW, const EvalOut& ev) {
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  float s[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int i = lane; i < nblk; i += 32) {
+    const float* q = ev.partial + ((size_t)r * nblk + i) * kEvalSums;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s[k] += __ldcg(q + k);   // written by other blocks
+  }
+#pragma unroll
+  for (int k = 0; k < 5; ++k) s[k] = warp_sum_all(s[k]);
+  const int hidden = ev.hidden;
+  const float* w1 = ev.cp;
+  const float* b1 = ev.cp + 3 * hidden;
+  const float* w2 = b1 + hidden;
+  const float* x = ev.rx + 3 * r;
+  float acc = 0.0f;
+  for (int j = lane; j < hidden; j += 32) {
+    const float p = w1[3 * j] * x[0] + w1[3 * j + 1] * x[1] + w1[3 * j + 2] * x[2] + b1[j];
+    acc += w2[j] * fmaxf(p, 0.0f);
+  }
+  acc = warp_sum_all(acc);
+  if (lane == 0) {
+    const float n = (float)HW;
+    const float mae = s[0] / n, ssim = s[1] / n, mse = s[2] / n;
+    const float psnr = mse == 0.0f ? __int_as_float(0x7f800000) : 20.0f * log10f(1.0f / sqrtf(mse));
+    const float rssi_p = 10.0f * log10f(s[3] / n) - 30.0f, rssi_t = 10.0f * log10f(s[4] / n) - 30.0f;
+    float* m = ev.metrics + (size_t)r * GSPARC_EVAL_METRICS;
+    m[0] = psnr;
+    m[1] = rssi_p - rssi_t;
+    m[2] = mae;
+    m[3] = ssim;
+    m[4] = 1.0f + expf(acc + w2[hidden]);
+    m[5] = (1.0f - ev.lambda1) * mae + ev.lambda1 * (1.0f - ssim);
+  }
+}
+
+// Block sums (fixed order) written by thread 0, then the last block of the
+// spectrum runs its head.
+__device__ void eval_arrive(const float (&v)[5], int nblk, int HW, const EvalOut& ev) {
+  __shared__ float red[5][32];
+  __shared__ int s_last;
+  float w[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) w[k] = warp_sum_all(v[k]);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int k = 0; k < 5; ++k) red[k][threadIdx.x >> 5] = w[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float* q = ev.partial + (((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * kEvalSums;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      float a = 0.0f;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) a += red[k][i];
+      q[k] = a;
+    }
+    __threadfence();
+    s_last = atomicAdd(ev.psync + blockIdx.z, 1u) == (unsigned)nblk - 1u;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  eval_spectrum_head((int)blockIdx.z, nblk, HW, ev);
+  if (threadIdx.x == 0) ev.psync[blockIdx.z] = 0u;
+}
+
 // ---- tile layout: 32x8 outputs per block with the 5-pixel halo --------------
 
+// kEval: the evaluation pass (no map derivatives; EvalOut sums and heads)
+template <bool kEval>
 __global__ void __launch_bounds__(256)
 loss_forward_kernel(int H, int W, float C1, float C2, const float* __restrict__ pred,
                     const float* __restrict__ target, float* __restrict__ dm_dmu1,
                     float* __restrict__ dm_dsigma1_sq, float* __restrict__ dm_dsigma12,
-                    float2* __restrict__ partial, LossHead head) {
+                    float2* __restrict__ partial, LossHead head, EvalOut ev) {
   __shared__ float s1[kTH][kTW + 1];
   __shared__ float s2[kTH][kTW + 1];
   __shared__ float hx[5][kTH][kSW];
@@ -408,18 +495,30 @@ loss_forward_kernel(int H, int W, float C1, float C2, const float* __restrict__ 
 #pragma unroll
     for (int k = 0; k < 11; ++k) v[q] += kSsimWin[k] * hx[q][ly + k][lx];
   const int px = blockIdx.x * kSW + lx, py = blockIdx.y * kSH + ly;
-  float l1 = 0.0f, sm = 0.0f;
+  float l1 = 0.0f, sm = 0.0f, sq = 0.0f, pp = 0.0f, tt = 0.0f;
   if (px < W && py < H) {
     const size_t idx = plane + (size_t)py * W + px;
     float d1, d2, d3;
     sm = ssim_pixel(v, C1, C2, d1, d2, d3);
-    l1 = fabsf(s1[ly + kHalo][lx + kHalo] - s2[ly + kHalo][lx + kHalo]);
-    dm_dmu1[idx] = d1;
-    dm_dsigma1_sq[idx] = d2;
-    dm_dsigma12[idx] = d3;
+    const float p = s1[ly + kHalo][lx + kHalo], q = s2[ly + kHalo][lx + kHalo];
+    l1 = fabsf(p - q);
+    if constexpr (kEval) {
+      sq = (p - q) * (p - q);
+      pp = p * p;
+      tt = q * q;
+    } else {
+      dm_dmu1[idx] = d1;
+      dm_dsigma1_sq[idx] = d2;
+      dm_dsigma12[idx] = d3;
+    }
   }
-  block_partial(l1, sm, partial);
-  loss_arrive(gridDim.x * gridDim.y, H * W, head, partial);
+  if constexpr (kEval) {
+    const float vals[5] = {l1, sm, sq, pp, tt};
+    eval_arrive(vals, gridDim.x * gridDim.y, H * W, ev);
+  } else {
+    block_partial(l1, sm, partial);
+    loss_arrive(gridDim.x * gridDim.y, H * W, head, partial);
+  }
 }
 
 __device__ __forceinline__ void stage_scaled(float (*dst)[kTW + 1], const float* __restrict__ a, float c, int H,
@@ -547,11 +646,12 @@ __device__ __forceinline__ void band_stage(float* dst, const float* const (&src)
   }
 }
 
+template <bool kEval>
 __global__ void __launch_bounds__(kBandThreads)
 loss_forward_band_kernel(int H, int W, int hb, float C1, float C2, const float* __restrict__ pred,
                          const float* __restrict__ target, float* __restrict__ dm_dmu1,
                          float* __restrict__ dm_dsigma1_sq, float* __restrict__ dm_dsigma12,
-                         float2* __restrict__ partial, LossHead head) {
+                         float2* __restrict__ partial, LossHead head, EvalOut ev) {
   __shared__ __align__(16) float s_in[2][2 * kRing * kBandPitch];
   const size_t plane = (size_t)blockIdx.z * H * W;
   const int x0 = blockIdx.x * kBandThreads, x = x0 + (int)threadIdx.x;
@@ -565,7 +665,7 @@ loss_forward_band_kernel(int H, int W, int hb, float C1, float C2, const float* 
   // ring of horizontal moments per input row: (a, c) = (mu1, mu2), (b, d) = (E x^2, E y^2), e = E xy
   float2 r_ac[kRing], r_bd[kRing];
   float r_e[kRing];
-  float l1 = 0.0f, sm = 0.0f;
+  float l1 = 0.0f, sm = 0.0f, sq = 0.0f, pp = 0.0f, tt = 0.0f;
   band_stage<2>(s_in[0], src, H, W, x0, y0 - kHalo);
   cp_async_commit();
   for (int ci = 0; ci < nchunks; ++ci) {
@@ -593,6 +693,11 @@ loss_forward_band_kernel(int H, int W, int hb, float C1, float C2, const float* 
         if (g >= kHalo && g < n_in - kHalo && x < W) {
           const float2 c = spq[j * kBandPitch + kHalo];
           l1 += fabsf(c.x - c.y);
+          if constexpr (kEval) {
+            sq += (c.x - c.y) * (c.x - c.y);
+            pp += c.x * c.x;
+            tt += c.y * c.y;
+          }
         }
         if (g >= 2 * kHalo) {   // output row y0 + g - 10: window rows g - 10 .. g
           float2 vac = make_float2(0.0f, 0.0f), vbd = make_float2(0.0f, 0.0f);
@@ -609,17 +714,24 @@ loss_forward_band_kernel(int H, int W, int hb, float C1, float C2, const float* 
             const size_t idx = plane + (size_t)(y0 + g - 2 * kHalo) * W + x;
             float d1, d2, d3;
             sm += ssim_pixel(v, C1, C2, d1, d2, d3);
-            dm_dmu1[idx] = d1;
-            dm_dsigma1_sq[idx] = d2;
-            dm_dsigma12[idx] = d3;
+            if constexpr (!kEval) {
+              dm_dmu1[idx] = d1;
+              dm_dsigma1_sq[idx] = d2;
+              dm_dsigma12[idx] = d3;
+            }
           }
         }
       }
     }
     __syncthreads();   // the buffer is restaged two chunks on
   }
-  block_partial(l1, sm, partial);
-  loss_arrive(gridDim.x * gridDim.y, H * W, head, partial);
+  if constexpr (kEval) {
+    const float vals[5] = {l1, sm, sq, pp, tt};
+    eval_arrive(vals, gridDim.x * gridDim.y, H * W, ev);
+  } else {
+    block_partial(l1, sm, partial);
+    loss_arrive(gridDim.x * gridDim.y, H * W, head, partial);
+  }
 }
 
 __global__ void __launch_bounds__(kBandThreads)
@@ -771,12 +883,13 @@ cudaError_t launch_splat_loss(int R, int H, int W, int hidden, float lambda1, fl
   head.psync = reinterpret_cast<unsigned*>(scratch + L.psync);
   head.sync = reinterpret_cast<unsigned*>(scratch + L.sync);
   const dim3 grid((unsigned)G.gx, (unsigned)G.gy, (unsigned)R);
+  const EvalOut ev{};
   if (G.band) {
-    loss_forward_band_kernel<<<grid, kBandThreads, 0, stream>>>(H, W, G.hb, C1, C2, pred, target, scratch + L.dmu1,
-                                                                scratch + L.ds11, scratch + L.ds12, partial, head);
+    loss_forward_band_kernel<false><<<grid, kBandThreads, 0, stream>>>(
+        H, W, G.hb, C1, C2, pred, target, scratch + L.dmu1, scratch + L.ds11, scratch + L.ds12, partial, head, ev);
   } else {
-    loss_forward_kernel<<<grid, 256, 0, stream>>>(H, W, C1, C2, pred, target, scratch + L.dmu1, scratch + L.ds11,
-                                                  scratch + L.ds12, partial, head);
+    loss_forward_kernel<false><<<grid, 256, 0, stream>>>(H, W, C1, C2, pred, target, scratch + L.dmu1,
+                                                         scratch + L.ds11, scratch + L.ds12, partial, head, ev);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -787,6 +900,35 @@ cudaError_t launch_splat_loss(int R, int H, int W, int hidden, float lambda1, fl
     loss_backward_kernel<<<grid, 256, 0, stream>>>(H, W, pred, target, scratch + L.dmu1, scratch + L.ds11,
                                                    scratch + L.ds12, coef, dL_dpred);
   }
+  return cudaGetLastError();
+}
+
+size_t eval_scratch_floats(size_t R, size_t H, size_t W) {
+  const LossGeom g = loss_geom(R, H, W);
+  return (R * (size_t)g.gx * g.gy * kEvalSums + 63) / 64 * 64 + (R + 63) / 64 * 64;
+}
+
+cudaError_t launch_eval_metrics(int R, int H, int W, int hidden, float lambda1, float C1, float C2, const float* pred,
+                                const float* target, const float* rx, const float* conf_params, float* scratch,
+                                float* metrics, cudaStream_t stream) {
+  const LossGeom G = loss_geom(R, H, W);
+  const size_t np = ((size_t)R * G.gx * G.gy * kEvalSums + 63) / 64 * 64;
+  EvalOut ev;
+  ev.partial = scratch;
+  ev.psync = reinterpret_cast<unsigned*>(scratch + np);
+  ev.rx = rx;
+  ev.cp = conf_params;
+  ev.hidden = hidden;
+  ev.lambda1 = lambda1;
+  ev.metrics = metrics;
+  const LossHead head{};
+  const dim3 grid((unsigned)G.gx, (unsigned)G.gy, (unsigned)R);
+  if (G.band)
+    loss_forward_band_kernel<true><<<grid, kBandThreads, 0, stream>>>(H, W, G.hb, C1, C2, pred, target, nullptr,
+                                                                      nullptr, nullptr, nullptr, head, ev);
+  else
+    loss_forward_kernel<true><<<grid, 256, 0, stream>>>(H, W, C1, C2, pred, target, nullptr, nullptr, nullptr, nullptr,
+                                                        head, ev);
   return cudaGetLastError();
 }
 

@@ -69,6 +69,9 @@ _SIGS = {
     "gsparc_splat_loss_scratch_floats": (_c_size, [_c_int, _c_int, _c_int, _c_int]),
     "gsparc_splat_loss": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_float, _c_float, _c_float, _c_float,
                                    _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gsparc_eval_scratch_floats": (_c_size, [_c_int, _c_int, _c_int]),
+    "gsparc_eval_metrics": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_float, _c_float, _c_float,
+                                     _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gsparc_gaussian_state_floats": (_c_size, [_c_int, _c_ll, _c_int]),
     "gsparc_gaussian_state_layout": (_c_int, [_c_int, _c_ll, _c_int, ctypes.POINTER(_c_size)]),
     "gsparc_gaussian_activate": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _vp]),

@@ -36,7 +36,7 @@ import torch
 from . import _lib, raster, scenes
 from ._lib import check, ptr, stream_of
 from .autograd import RasterPlan
-from .loss import SplatLoss, conf_floats
+from .loss import Evaluator, SplatLoss, conf_floats
 from .trainer import ConfidenceMLP
 
 # centre, scaling, rotation, opacity, emission MLP (optimizer.py:9-17), confidence MLP (optimizer.py:29)
@@ -187,6 +187,33 @@ class FusedTrainer:
                         **self._shared_kw())
         self._reduce_and_adam()
         return loss
+
+    def evaluate(self, views, rxs, tx, targets, plan=None):
+        """Render R test receivers with the current parameters (forward only)
+        and evaluate them as train.py:672-701 does: returns a [R, 6] tensor
+        (R*C rows with C channels, receiver-major) of PSNR, RSSI difference,
+        MAE, SSIM, confidence and evaluation loss (loss.METRICS).  `plan` is a
+        RasterPlan for R receivers (default: the training step's)."""
+        plan = self.plan if plan is None else plan
+        R, C, H, W, dev = plan.R, self.channels, self.H, self.W, self.device
+        with torch.no_grad():
+            if C > 1:
+                out, _, _ = raster.forward_channels(
+                    self.centre, self.act_opac, self.act_scales, self.act_rots, H, W, 1.0, views, tx, rxs,
+                    self.shared, self.mlp, tile=plan.tile, capacity=plan.capacity, binning=plan.binning,
+                    geom=plan.geom, image=plan.image, wrap=plan.wrap)
+                out = out.view(R * C, H, W)
+                rxs = rxs.repeat_interleave(C, dim=0).contiguous()
+            else:
+                out, _, _, _ = raster.forward(
+                    self.centre, self._mlp_arg(), self.act_opac, self.act_scales, self.act_rots, H, W, 1.0, views,
+                    tx, rxs, tile=plan.tile, capacity=plan.capacity, binning=plan.binning, geom=plan.geom,
+                    image=plan.image, wrap=plan.wrap, **self._shared_kw())
+            plan.record_status()
+            ev = getattr(self, "_evaluator", None)
+            if ev is None or ev.R != R * C:
+                ev = self._evaluator = Evaluator(R * C, H, W, self.conf_hidden, dev, self.lambda1)
+            return ev(out, targets.reshape(R * C, H, W), rxs, self.conf_params)
 
     def _reduce_and_adam(self):
         if self.group is not None:

@@ -63,6 +63,36 @@ class SplatLoss:
         return self.loss, self.dpred
 
 
+METRICS = ("psnr", "rssi_diff", "mae", "ssim", "confidence", "loss")
+
+
+class Evaluator:
+    """Batched evaluation of R test spectra (train.py:672-701): per spectrum
+    the PSNR (train.py:76-83), the RSSI difference rssi(pred) - rssi(target)
+    (train.py:86-91), the MAE (train.py:99-101), the mean SSIM (utils.py:81-114),
+    the confidence 1 + exp(fc2(relu(fc1(rx)))) and the evaluation loss
+    (1 - lambda1) MAE + lambda1 (1 - SSIM), in one launch over the C ABI.
+    ``__call__`` returns a [R, 6] tensor in the order of ``METRICS``."""
+
+    def __init__(self, R, H, W, hidden=32, device="cuda", lambda1=LAMBDA1):
+        self.R, self.H, self.W, self.hidden = int(R), int(H), int(W), int(hidden)
+        self.lambda1 = float(lambda1)
+        dev = torch.device(device)
+        n = int(_lib.lib().gsparc_eval_scratch_floats(self.R, self.H, self.W))
+        self.scratch = torch.zeros(max(n, 1), dtype=torch.float32, device=dev)   # zero once: arrival counters
+        self.metrics = torch.zeros((self.R, len(METRICS)), dtype=torch.float32, device=dev)
+
+    def __call__(self, pred, target, rx_pos, conf_params):
+        for name, t, shape in (("pred", pred, (self.R, self.H, self.W)), ("target", target, (self.R, self.H, self.W)),
+                               ("rx_pos", rx_pos, (self.R, 3)), ("conf_params", conf_params, (conf_floats(self.hidden),))):
+            if t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous() or t.numel() != _numel(shape):
+                raise ValueError(f"{name} must be a contiguous float32 CUDA tensor of shape {shape}")
+        check("eval_metrics", _lib.lib().gsparc_eval_metrics(
+            self.R, self.H, self.W, self.hidden, self.lambda1, C1, C2, ptr(pred), ptr(target), ptr(rx_pos),
+            ptr(conf_params), ptr(self.scratch), ptr(self.metrics), stream_of(pred.device)))
+        return self.metrics
+
+
 def _numel(shape):
     n = 1
     for s in shape:

@@ -303,6 +303,34 @@ GSPARC_API int gsparc_splat_loss(int R, int H, int W, int hidden, float lambda1,
                                  float* loss_out, float* terms, float* dL_dpred,
                                  float* dL_dconf_params, void* stream);
 
+/* ---- evaluation metrics --------------------------------------------------- */
+
+/* Metrics per spectrum written by gsparc_eval_metrics, in this order. */
+#define GSPARC_EVAL_METRICS 6
+enum {
+  GSPARC_EVAL_PSNR = 0,       /* 20 log10(1 / sqrt(mse)); +inf when mse = 0 (train.py:76-83) */
+  GSPARC_EVAL_RSSI_DIFF = 1,  /* rssi(pred) - rssi(target), rssi = 10 log10(mean x^2) - 30 (train.py:86-91) */
+  GSPARC_EVAL_MAE = 2,        /* mean |pred - target| (train.py:99-101) */
+  GSPARC_EVAL_SSIM = 3,       /* mean SSIM map, 11x11 window, "same" padding (utils.py:81-114) */
+  GSPARC_EVAL_CONFIDENCE = 4, /* 1 + exp(fc2(relu(fc1(rx_pos)))) (gaussian.py:575-609) */
+  GSPARC_EVAL_LOSS = 5        /* (1 - lambda1) MAE + lambda1 (1 - SSIM) (train.py:696-697) */
+};
+
+/* Scratch floats gsparc_eval_metrics needs for R spectra of H x W. */
+GSPARC_API size_t gsparc_eval_scratch_floats(int R, int H, int W);
+
+/* The per-spectrum evaluation of train.py:672-701 (calculate_psnr,
+ * calculate_rssi difference, calculate_mae, ssim, the confidence and the
+ * evaluation loss), batched over R test spectra in one pass that shares the
+ * SSIM moments of the training loss.  pred, target: [R,H,W]; rx_pos: [R,3];
+ * conf_params: as gsparc_splat_loss; metrics: [R, GSPARC_EVAL_METRICS];
+ * scratch: gsparc_eval_scratch_floats floats, zero-filled before its first
+ * use (per-spectrum arrival counters that every call leaves at zero).  All
+ * device memory. */
+GSPARC_API int gsparc_eval_metrics(int R, int H, int W, int hidden, float lambda1, float C1, float C2,
+                                   const float* pred, const float* target, const float* rx_pos,
+                                   const float* conf_params, float* scratch, float* metrics, void* stream);
+
 /* ---- fused optimizer over the per-Gaussian parameters ------------------- */
 
 /* Floats in a flat training-state buffer for P Gaussians, an emission-MLP

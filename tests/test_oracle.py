@@ -387,3 +387,29 @@ def test_multichannel_blend_adjoint_matches_fd_and_single_channel():
         fd = (L(R.blend_forward_channels(ranges, vals, m2, cp, f, H, W, dtype=np.float64)[0]) -
               L(R.blend_forward_channels(ranges, vals, m2, cm, f, H, W, dtype=np.float64)[0])) / (2 * h)
         assert abs(fd - do[k]) <= 1e-6 * max(1.0, abs(fd))
+
+
+def test_eval_metric_oracle_matches_the_reference_formulas():
+    """oracle/metrics.py against the reference's metric helpers written out in
+    torch (train.py:76-101: calculate_psnr, calculate_rssi, calculate_mae) and
+    the window SSIM (utils.py:81-114, pinned separately by the golden tests)."""
+    import torch
+    from oracle import metrics as om
+    rng = np.random.default_rng(5)
+    pred = rng.random((2, 20, 30))
+    target = np.clip(pred + 0.1 * rng.standard_normal(pred.shape), 0, None)
+    rx = rng.random((2, 3))
+    cp = 0.2 * rng.standard_normal(5 * 8 + 1)
+    m = om.evaluate(pred, target, rx, cp, 8, lambda1=0.2)
+    for r in range(2):
+        p, t = torch.tensor(pred[r]), torch.tensor(target[r])
+        mse = torch.mean((p - t) ** 2)
+        assert np.isclose(m[r, 0], float(20 * torch.log10(1.0 / torch.sqrt(mse))))
+        rssi = lambda s: 10 * torch.log10(torch.mean(s ** 2)) - 30
+        assert np.isclose(m[r, 1], float(rssi(p) - rssi(t)))
+        assert np.isclose(m[r, 2], float(torch.mean(torch.abs(p - t))))
+        assert np.isclose(m[r, 5], 0.8 * m[r, 2] + 0.2 * (1 - m[r, 3]))
+    w1, b1, w2, b2 = cp[:24].reshape(8, 3), cp[24:32], cp[32:40], cp[40]
+    assert np.isclose(m[0, 4], 1 + np.exp(w2 @ np.maximum(w1 @ rx[0] + b1, 0) + b2))
+    same = om.evaluate(pred[:1], pred[:1], rx[:1], cp, 8)
+    assert np.isinf(same[0, 0]) and same[0, 1] == 0 and same[0, 2] == 0 and np.isclose(same[0, 3], 1.0)
