@@ -47,7 +47,7 @@ bool valid_tile(int th, int tw) {
 enum KernelId {
   KID_PREPROCESS, KID_CHECK, KID_SCATTER, KID_DEPTH_SORT, KID_PLACE, KID_BLEND_FWD, KID_BLEND_BWD,
   KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_ADAM, KID_LOSS, KID_ACTIVATE, KID_SHARED_MLP, KID_SHARED_MLP_BWD,
-  KID_BLEND_MC_FWD, KID_BLEND_MC_BWD, KID_EVAL,
+  KID_BLEND_MC_FWD, KID_BLEND_MC_BWD, KID_EVAL, KID_DENSIFY,
   KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
@@ -56,7 +56,7 @@ const char* const kKernelNames[KID_COUNT] = {
     "emission_backward_kernel", "ssim_forward_kernel", "ssim_backward_kernel", "mark_visible_kernel",
     "gaussian_adam_kernels", "splat_loss_kernels", "gaussian_activate_kernel", "shared_mlp_forward_kernels",
     "shared_mlp_backward_kernels", "blend_channels_forward_kernel", "blend_channels_backward_kernel",
-    "eval_metrics_kernel"};
+    "eval_metrics_kernel", "densify_kernels"};
 
 struct PendingTiming {
   int id;
@@ -110,7 +110,7 @@ int report_cuda(cudaError_t e, const char* where) { return cuda_fail(e, where); 
 
 extern "C" {
 
-int gsparc_abi_version(void) { return 6; }
+int gsparc_abi_version(void) { return 7; }
 
 const char* gsparc_status_string(int status) {
   switch (status) {
@@ -579,6 +579,84 @@ int gsparc_eval_metrics(int R, int H, int W, int hidden, float lambda1, float C1
   GS_CHECK(launch_eval_metrics(R, H, W, hidden, lambda1, C1, C2, pred, target, rx_pos, conf_params, scratch, metrics,
                                s),
            "eval metrics");
+  return GSPARC_OK;
+}
+
+// ---- densification ---------------------------------------------------------------
+
+int gsparc_densify_stats(int P, int R, const int* radii, const float* dL_dmeans2D, float* accum, float* denom,
+                         float* max_radii2D, void* stream) {
+  if (P < 0 || R < 1) return invalid("sizes");
+  if (P == 0) return GSPARC_OK;
+  if (!radii || !dL_dmeans2D || !accum || !denom || !max_radii2D) return invalid("null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  Timed t(KID_DENSIFY, s);
+  GS_CHECK(launch_densify_stats(P, R, radii, dL_dmeans2D, accum, denom, max_radii2D, s), "densify stats");
+  return GSPARC_OK;
+}
+
+size_t gsparc_densify_work_ints(int P) { return P < 0 ? 0 : densify_work_ints(P); }
+
+namespace {
+int densify_check(int P, long long mlp_floats, int per_gaussian_mlp, int conf_floats, const float* box6) {
+  if (P < 0 || mlp_floats < 0 || conf_floats < 0) return invalid("sizes");
+  if (per_gaussian_mlp && mlp_floats != 194LL * P) return invalid("a per-Gaussian MLP segment holds 194*P floats");
+  if (!box6) return invalid("null scene box");
+  return GSPARC_OK;
+}
+}  // namespace
+
+int gsparc_densify_count(int P, long long mlp_floats, int per_gaussian_mlp, int conf_floats, const float* params,
+                         const float* accum, const float* denom, float grad_threshold, float percent_dense,
+                         float extent, float min_opacity, float max_screen_size, const float* scene_box6,
+                         unsigned long long seed, int* work, int* P_new, void* stream) {
+  const int st = densify_check(P, mlp_floats, per_gaussian_mlp, conf_floats, scene_box6);
+  if (st != GSPARC_OK) return st;
+  if (!params || !accum || !denom || !work || !P_new) return invalid("null pointer");
+  const GaussianLayout L = gaussian_layout((size_t)P, (size_t)mlp_floats, (size_t)conf_floats);
+  const size_t off[6] = {L.centre, L.scale, L.quat, L.opacity, L.mlp, L.conf};
+  cudaStream_t s = (cudaStream_t)stream;
+  Timed t(KID_DENSIFY, s);
+  GS_CHECK(launch_densify_count(P, params, off, accum, denom, grad_threshold, percent_dense, extent, min_opacity,
+                                max_screen_size, scene_box6, seed, work, P_new, s),
+           "densify count");
+  return GSPARC_OK;
+}
+
+int gsparc_densify_apply(int P, int P_new, long long mlp_floats, int per_gaussian_mlp, int conf_floats,
+                         const float* params, const float* exp_avg, const float* exp_avg_sq, float grad_threshold,
+                         float percent_dense, float extent, float min_opacity, float max_screen_size,
+                         const float* scene_box6, unsigned long long seed, const int* work, float* new_params,
+                         float* new_exp_avg, float* new_exp_avg_sq, void* stream) {
+  const int st = densify_check(P, mlp_floats, per_gaussian_mlp, conf_floats, scene_box6);
+  if (st != GSPARC_OK) return st;
+  if (P_new < 0) return invalid("P_new");
+  if (!params || !exp_avg || !exp_avg_sq || !work || !new_params || !new_exp_avg || !new_exp_avg_sq)
+    return invalid("null pointer");
+  const GaussianLayout L = gaussian_layout((size_t)P, (size_t)mlp_floats, (size_t)conf_floats);
+  const size_t off[6] = {L.centre, L.scale, L.quat, L.opacity, L.mlp, L.conf};
+  const long long new_mlp = per_gaussian_mlp ? 194LL * P_new : mlp_floats;
+  const GaussianLayout N = gaussian_layout((size_t)P_new, (size_t)new_mlp, (size_t)conf_floats);
+  const size_t noff[6] = {N.centre, N.scale, N.quat, N.opacity, N.mlp, N.conf};
+  cudaStream_t s = (cudaStream_t)stream;
+  Timed t(KID_DENSIFY, s);
+  GS_CHECK(launch_densify_apply(P, P_new, params, exp_avg, exp_avg_sq, off, mlp_floats, per_gaussian_mlp, conf_floats,
+                                grad_threshold, percent_dense, extent, min_opacity, max_screen_size, scene_box6, seed,
+                                work, new_params, new_exp_avg, new_exp_avg_sq, noff, s),
+           "densify apply");
+  return GSPARC_OK;
+}
+
+int gsparc_reset_opacity(int P, long long mlp_floats, int conf_floats, float* params, float* exp_avg,
+                         float* exp_avg_sq, void* stream) {
+  if (P < 0 || mlp_floats < 0 || conf_floats < 0) return invalid("sizes");
+  if (P == 0) return GSPARC_OK;
+  if (!params || !exp_avg || !exp_avg_sq) return invalid("null pointer");
+  const GaussianLayout L = gaussian_layout((size_t)P, (size_t)mlp_floats, (size_t)conf_floats);
+  cudaStream_t s = (cudaStream_t)stream;
+  Timed t(KID_DENSIFY, s);
+  GS_CHECK(launch_reset_opacity(P, params + L.opacity, exp_avg + L.opacity, exp_avg_sq + L.opacity, s),
+           "reset opacity");
   return GSPARC_OK;
 }
 

@@ -68,6 +68,20 @@ cudaError_t launch_gaussian_activate(int P, const float* params, float* act_scal
 
 LossLayout loss_layout(size_t R, size_t H, size_t W, size_t hidden);
 size_t eval_scratch_floats(size_t R, size_t H, size_t W);
+size_t densify_work_ints(int P);
+cudaError_t launch_densify_stats(int P, int R, const int* radii, const float* dmeans2D, float* accum, float* denom,
+                                 float* max_radii, cudaStream_t s);
+cudaError_t launch_densify_count(int P, const float* params, const size_t* off, const float* accum,
+                                 const float* denom, float grad_threshold, float percent_dense, float extent,
+                                 float min_opacity, float max_screen_size, const float* box6,
+                                 unsigned long long seed, int* work, int* P_new, cudaStream_t s);
+cudaError_t launch_densify_apply(int P, int P_new, const float* params, const float* exp_avg, const float* exp_avg_sq,
+                                 const size_t* off, long long mlp_floats, int per_gaussian_mlp, int conf_floats,
+                                 float grad_threshold, float percent_dense, float extent, float min_opacity,
+                                 float max_screen_size, const float* box6, unsigned long long seed, const int* work,
+                                 float* new_params, float* new_exp_avg, float* new_exp_avg_sq, const size_t* new_off,
+                                 cudaStream_t s);
+cudaError_t launch_reset_opacity(int P, float* logit, float* m1, float* m2, cudaStream_t s);
 cudaError_t launch_eval_metrics(int R, int H, int W, int hidden, float lambda1, float C1, float C2, const float* pred,
                                 const float* target, const float* rx, const float* conf_params, float* scratch,
                                 float* metrics, cudaStream_t stream);

@@ -72,6 +72,13 @@ _SIGS = {
     "gsparc_eval_scratch_floats": (_c_size, [_c_int, _c_int, _c_int]),
     "gsparc_eval_metrics": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_float, _c_float, _c_float,
                                      _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gsparc_densify_stats": (_c_int, [_c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gsparc_densify_work_ints": (_c_size, [_c_int]),
+    "gsparc_densify_count": (_c_int, [_c_int, _c_ll, _c_int, _c_int, _vp, _vp, _vp, _c_float, _c_float, _c_float,
+                                      _c_float, _c_float, _vp, ctypes.c_ulonglong, _vp, _vp, _vp]),
+    "gsparc_densify_apply": (_c_int, [_c_int, _c_int, _c_ll, _c_int, _c_int, _vp, _vp, _vp, _c_float, _c_float,
+                                      _c_float, _c_float, _c_float, _vp, ctypes.c_ulonglong, _vp, _vp, _vp, _vp, _vp]),
+    "gsparc_reset_opacity": (_c_int, [_c_int, _c_ll, _c_int, _vp, _vp, _vp, _vp]),
     "gsparc_gaussian_state_floats": (_c_size, [_c_int, _c_ll, _c_int]),
     "gsparc_gaussian_state_layout": (_c_int, [_c_int, _c_ll, _c_int, ctypes.POINTER(_c_size)]),
     "gsparc_gaussian_activate": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _vp]),

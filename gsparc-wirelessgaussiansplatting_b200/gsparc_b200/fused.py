@@ -69,16 +69,48 @@ class FusedTrainer:
         self.betas, self.eps = betas, eps
         self.conf_hidden = int(conf_hidden)
         self.n_conf = conf_floats(self.conf_hidden)
-        P = scene.P
-        self.P = P
         self.shared = shared
-        self.n_mlp = 194 * P if shared is None else shared.n_params
-        (oC, oS, oQ, oO, oM, oG), total = state_layout(P, self.n_mlp, self.n_conf)
         dev = self.device
-        self.params = torch.zeros(total, dtype=torch.float32, device=dev)
+        P = scene.P
+        n_mlp = 194 * P if shared is None else shared.n_params
+        total = state_layout(P, n_mlp, self.n_conf)[1]
+        z = lambda: torch.zeros(total, dtype=torch.float32, device=dev)
+        torch.manual_seed(seed)
+        self.confidence = ConfidenceMLP(self.conf_hidden).to(dev)
+        conf0 = torch.cat([q.detach().reshape(-1) for q in self.confidence.parameters()])
+        self.densify_stats = False
+        self._bind(P, z(), z(), z())
+        t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
+        with torch.no_grad():
+            self.centre.copy_(t(scene.means))
+            self.log_scale.copy_(t(scene.log_scales))
+            self.rotation.copy_(t(scene.quats))
+            self.opacity_logit.copy_(t(scene.opacity_logits).reshape(-1))
+            self.mlp.copy_(t(scene.mlp) if shared is None else shared.init_params(seed, dev))
+            self.conf_params.copy_(conf0)
+        self.step_count = torch.zeros(2, dtype=torch.float32, device=dev)   # step, arrival counter (0)
+        self.lr6 = torch.tensor(lr, dtype=torch.float32, device=dev)
+        self.lo3 = torch.tensor(scenes.ROOM_LO, dtype=torch.float32, device=dev)
+        self.hi3 = torch.tensor(scenes.ROOM_HI, dtype=torch.float32, device=dev)
+        # amplitude channels per spectrum: the shared MLP's outputs (one = the signal path)
+        self.channels = 1 if shared is None else int(shared.out)
+        self.graph = None
+        self.plan = None
+        self._R = None
+        self.activate()
+
+    def _bind(self, P, params, exp_avg, exp_avg_sq):
+        """Views of a flat training state for P Gaussians (raw parameters and
+        Adam moments), a zeroed gradient buffer, the activation outputs and
+        the densification statistics; step-size buffers are rebuilt on the
+        next step and any captured graph is dropped."""
+        dev = self.device
+        self.P = P
+        self.n_mlp = 194 * P if self.shared is None else self.shared.n_params
+        (oC, oS, oQ, oO, oM, oG), total = state_layout(P, self.n_mlp, self.n_conf)
+        assert params.numel() == total and exp_avg.numel() == total and exp_avg_sq.numel() == total
+        self.params, self.exp_avg, self.exp_avg_sq = params, exp_avg, exp_avg_sq
         self.grads = torch.zeros(total, dtype=torch.float32, device=dev)
-        self.exp_avg = torch.zeros(total, dtype=torch.float32, device=dev)
-        self.exp_avg_sq = torch.zeros(total, dtype=torch.float32, device=dev)
 
         def seg(buf, off, n, shape):
             return buf[off:off + n].view(*shape)
@@ -90,22 +122,11 @@ class FusedTrainer:
         self.mlp = seg(self.params, oM, self.n_mlp, (self.n_mlp,))
         self.conf_params = seg(self.params, oG, self.n_conf, (self.n_conf,))
         self.conf_grads = seg(self.grads, oG, self.n_conf, (self.n_conf,))
-        t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
-        with torch.no_grad():
-            self.centre.copy_(t(scene.means))
-            self.log_scale.copy_(t(scene.log_scales))
-            self.rotation.copy_(t(scene.quats))
-            self.opacity_logit.copy_(t(scene.opacity_logits).reshape(-1))
-            self.mlp.copy_(t(scene.mlp) if shared is None else shared.init_params(seed, dev))
-        torch.manual_seed(seed)
-        self.confidence = ConfidenceMLP(self.conf_hidden).to(dev)
         off = 0
-        with torch.no_grad():   # the module's parameters become views of the flat segment
+        with torch.no_grad():   # the confidence module's parameters are views of the flat segment
             for prm in self.confidence.parameters():
                 n = prm.numel()
-                view = self.conf_params[off:off + n].view_as(prm)
-                view.copy_(prm)
-                prm.data = view
+                prm.data = self.conf_params[off:off + n].view_as(prm)
                 off += n
         self.gout = dict(dmeans3D=seg(self.grads, oC, 3 * P, (P, 3)), dscales=seg(self.grads, oS, 3 * P, (P, 3)),
                          drotations=seg(self.grads, oQ, 4 * P, (P, 4)), dopacity=seg(self.grads, oO, P, (P,)),
@@ -113,15 +134,51 @@ class FusedTrainer:
         self.act_scales = torch.empty((P, 3), dtype=torch.float32, device=dev)
         self.act_rots = torch.empty((P, 4), dtype=torch.float32, device=dev)
         self.act_opac = torch.empty((P,), dtype=torch.float32, device=dev)
-        self.step_count = torch.zeros(2, dtype=torch.float32, device=dev)   # step, arrival counter (0)
-        self.lr6 = torch.tensor(lr, dtype=torch.float32, device=dev)
-        self.lo3 = torch.tensor(scenes.ROOM_LO, dtype=torch.float32, device=dev)
-        self.hi3 = torch.tensor(scenes.ROOM_HI, dtype=torch.float32, device=dev)
-        # amplitude channels per spectrum: the shared MLP's outputs (one = the signal path)
-        self.channels = 1 if shared is None else int(shared.out)
+        # densification statistics (train.py:508-516), accumulated by the step when densify_stats is set
+        self.grad_accum = torch.zeros(P, dtype=torch.float32, device=dev)
+        self.grad_denom = torch.zeros(P, dtype=torch.float32, device=dev)
+        self.max_radii2D = torch.zeros(P, dtype=torch.float32, device=dev)
         self.graph = None
         self.plan = None
         self._R = None
+
+    def densify_and_prune(self, max_grad, min_opacity, extent, max_screen_size=None, scene_min=None, scene_max=None,
+                          percent_dense=0.01, seed=0):
+        """densify_and_prune (gaussian.py:515-542) with the statistics the step
+        accumulated (``densify_stats = True``; train.py:508-516): clone, split
+        into two and prune on the device, in the reference's order.  The flat
+        state is rebuilt for the new Gaussian count (one host read of it),
+        new Gaussians start with zero Adam moments, the statistics restart at
+        zero, and the step has to be captured again.  Returns the new count."""
+        lib, dev, P = _lib.lib(), self.device, self.P
+        per_g = int(self.shared is None)
+        inf = float("inf")
+        lo = list(scene_min) if scene_min is not None else [-inf] * 3
+        hi = list(scene_max) if scene_max is not None else [inf] * 3
+        box = torch.tensor([float(v) for v in lo + hi], dtype=torch.float32)   # host memory
+        work = torch.empty(max(int(lib.gsparc_densify_work_ints(P)), 1), dtype=torch.int32, device=dev)
+        pn = torch.zeros(1, dtype=torch.int32, device=dev)
+        msz = float(max_screen_size) if max_screen_size else 0.0
+        args = (float(max_grad), float(percent_dense), float(extent), float(min_opacity), msz, ptr(box), int(seed))
+        check("densify_count", lib.gsparc_densify_count(
+            P, self.n_mlp, per_g, self.n_conf, ptr(self.params), ptr(self.grad_accum), ptr(self.grad_denom), *args,
+            ptr(work), ptr(pn), stream_of(dev)))
+        P_new = int(pn.item())
+        total = state_layout(P_new, 194 * P_new if per_g else self.n_mlp, self.n_conf)[1]
+        new = [torch.empty(total, dtype=torch.float32, device=dev) for _ in range(3)]
+        check("densify_apply", lib.gsparc_densify_apply(
+            P, P_new, self.n_mlp, per_g, self.n_conf, ptr(self.params), ptr(self.exp_avg), ptr(self.exp_avg_sq), *args,
+            ptr(work), ptr(new[0]), ptr(new[1]), ptr(new[2]), stream_of(dev)))
+        self._bind(P_new, *new)
+        self.activate()
+        return P_new
+
+    def reset_opacity(self):
+        """reset_opacity (gaussian.py:223-230): opacities capped at 0.01, their
+        Adam moments zeroed (in place: a captured step stays valid)."""
+        check("reset_opacity", _lib.lib().gsparc_reset_opacity(
+            self.P, self.n_mlp, self.n_conf, ptr(self.params), ptr(self.exp_avg), ptr(self.exp_avg_sq),
+            stream_of(self.device)))
         self.activate()
 
     def activate(self):
@@ -166,6 +223,8 @@ class FusedTrainer:
                   drotations=self.gout["drotations"], dopacity=self.gout["dopacity"], dshared=self.gout["dmlp"])
         raster.backward_channels(st, self.centre, self.act_scales, self.act_rots, 1.0, views, tx, rxs,
                                  dpred.view(R, C, H, W), self.shared, self.mlp, out=bo)
+        if self.densify_stats:
+            self._accumulate_stats(R)
         return loss
 
     def _body(self, views, rxs, tx, targets):
@@ -185,8 +244,15 @@ class FusedTrainer:
         raster.backward(st, self.centre, self._mlp_arg(), self.act_scales, self.act_rots, 1.0, views, tx, rxs,
                         dpred, self._zero_imag, grad_mode=self.grad_mode, out=self._bwd_out(),
                         **self._shared_kw())
+        if self.densify_stats:
+            self._accumulate_stats(plan.R)
         self._reduce_and_adam()
         return loss
+
+    def _accumulate_stats(self, R):
+        check("densify_stats", _lib.lib().gsparc_densify_stats(
+            self.P, R, ptr(self._radii), ptr(self._scratch["dmeans2D"]), ptr(self.grad_accum), ptr(self.grad_denom),
+            ptr(self.max_radii2D), stream_of(self.device)))
 
     def evaluate(self, views, rxs, tx, targets, plan=None):
         """Render R test receivers with the current parameters (forward only)

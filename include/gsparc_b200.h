@@ -331,6 +331,50 @@ GSPARC_API int gsparc_eval_metrics(int R, int H, int W, int hidden, float lambda
                                    const float* pred, const float* target, const float* rx_pos,
                                    const float* conf_params, float* scratch, float* metrics, void* stream);
 
+/* ---- densification (gaussian.py:223-551, train.py:508-553) --------------- */
+
+/* Statistics of one step (train.py:508-516): for every receiver r and
+ * Gaussian g with radii[r][g] > 0: accum[g] += |dL/dmeans2D[r][g][0:2]|,
+ * denom[g] += 1, max_radii2D[g] = max(max_radii2D[g], radii[r][g]).
+ * radii [R,P] int32 and dL_dmeans2D [R,P,3] as gsparc_rasterize_backward
+ * leaves them; accum, denom, max_radii2D [P]. */
+GSPARC_API int gsparc_densify_stats(int P, int R, const int* radii, const float* dL_dmeans2D, float* accum,
+                                    float* denom, float* max_radii2D, void* stream);
+
+/* Ints of the work buffer gsparc_densify_count / _apply share for P Gaussians. */
+GSPARC_API size_t gsparc_densify_work_ints(int P);
+
+/* densify_and_prune (gaussian.py:515-542) on a flat training state
+ * (gsparc_gaussian_state_layout; a per-Gaussian MLP segment of 194*P floats
+ * when per_gaussian_mlp, else a global one): clone (grad >= grad_threshold,
+ * largest scale <= percent_dense * extent), split into two (grad >=
+ * grad_threshold, largest scale > percent_dense * extent; centre R(q) (s z) +
+ * centre with z ~ N(0,1) from a counter-based generator seeded by `seed`,
+ * log-scale log(s / 1.2)), prune (opacity < min_opacity; largest scale >
+ * 0.1 extent when max_screen_size > 0; centre outside scene_box6 = lo[3],
+ * hi[3], 6 floats in HOST memory), grad = accum / denom (0 where 0/0).  Step 1 classifies and writes
+ * the new count to *P_new (device int; read it, allocate the new state for
+ * P_new, then call step 2, which gathers the survivors in the reference's
+ * order -- kept originals, clones, first and second split copies -- with
+ * zero Adam moments for the new Gaussians).  work: gsparc_densify_work_ints
+ * ints.  Device memory except scene_box6. */
+GSPARC_API int gsparc_densify_count(int P, long long mlp_floats, int per_gaussian_mlp, int conf_floats,
+                                    const float* params, const float* accum, const float* denom,
+                                    float grad_threshold, float percent_dense, float extent, float min_opacity,
+                                    float max_screen_size, const float* scene_box6, unsigned long long seed,
+                                    int* work, int* P_new, void* stream);
+GSPARC_API int gsparc_densify_apply(int P, int P_new, long long mlp_floats, int per_gaussian_mlp, int conf_floats,
+                                    const float* params, const float* exp_avg, const float* exp_avg_sq,
+                                    float grad_threshold, float percent_dense, float extent, float min_opacity,
+                                    float max_screen_size, const float* scene_box6, unsigned long long seed,
+                                    const int* work, float* new_params, float* new_exp_avg,
+                                    float* new_exp_avg_sq, void* stream);
+
+/* reset_opacity (gaussian.py:223-230): opacity logits set to
+ * logit(min(sigmoid(x), 0.01)), their Adam moments zeroed. */
+GSPARC_API int gsparc_reset_opacity(int P, long long mlp_floats, int conf_floats, float* params, float* exp_avg,
+                                    float* exp_avg_sq, void* stream);
+
 /* ---- fused optimizer over the per-Gaussian parameters ------------------- */
 
 /* Floats in a flat training-state buffer for P Gaussians, an emission-MLP

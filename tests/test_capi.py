@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     L = _lib.lib()
-    assert L.gsparc_abi_version() == 6
+    assert L.gsparc_abi_version() == 7
     for code, text in [(0, b"ok"), (1, b"invalid argument"), (2, b"CUDA error"), (3, b"binning capacity exceeded")]:
         assert L.gsparc_status_string(code) == text
 
