@@ -152,6 +152,12 @@ class FusedTrainer:
         zero, and the step has to be captured again.  Returns the new count."""
         lib, dev, P = _lib.lib(), self.device, self.P
         per_g = int(self.shared is None)
+        if self.group is not None:
+            # receivers are sharded: every rank densifies the same way from the summed statistics
+            import torch.distributed as dist
+            dist.all_reduce(self.grad_accum, op=dist.ReduceOp.SUM, group=self.group)
+            dist.all_reduce(self.grad_denom, op=dist.ReduceOp.SUM, group=self.group)
+            dist.all_reduce(self.max_radii2D, op=dist.ReduceOp.MAX, group=self.group)
         inf = float("inf")
         lo = list(scene_min) if scene_min is not None else [-inf] * 3
         hi = list(scene_max) if scene_max is not None else [inf] * 3
