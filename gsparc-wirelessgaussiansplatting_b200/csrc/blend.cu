@@ -225,7 +225,7 @@ blend_forward_kernel(int P, int H, int W, TileGrid grid, const uint2* __restrict
 
 template <int kThreads, bool kWrap>
 __global__ void __launch_bounds__(kThreads)
-blend_backward_kernel(int P, int H, int W, TileGrid grid, int RT, unsigned grad_mode,
+blend_backward_kernel(int P, int H, int W, TileGrid grid, int RT, int span, unsigned grad_mode,
                       const uint2* __restrict__ ranges, const uint32_t* __restrict__ chunk_base,
                       const uint32_t* __restrict__ point_list, const float4* __restrict__ ckpt,
                       const float2* __restrict__ accum, GeomView geo, ImageHeader* __restrict__ hdr,
@@ -256,9 +256,10 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, int RT, unsigned grad_
   }
   const int t = lo;
   const int chunk = item - ((int)chunk_base[t] + t);
+  if (chunk & (span - 1)) return;   // covered by the item `span` chunks before it
   const uint2 range = ranges[t];
   const int jlo = chunk * kBwdChunk;
-  const int jhi = min((int)(range.y - range.x), jlo + kBwdChunk);
+  const int jhi = min((int)(range.y - range.x), jlo + span * kBwdChunk);
   if (jlo >= jhi) return;   // empty segment
 
   const bool ref = grad_mode == GSPARC_GRAD_REFERENCE;
@@ -287,7 +288,7 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, int RT, unsigned grad_
   float T = inside ? final_Ts[pix] : 0.0f;
   float acc_r = 0.0f, acc_i = 0.0f;
   if (last_contributor > jhi) {
-    const float4 c = ckpt[((size_t)chunk_base[t] + chunk) * kBlendThreads + li];
+    const float4 c = ckpt[((size_t)chunk_base[t] + chunk + span - 1) * kBlendThreads + li];
     const float2 tot = accum[pix];
     T = c.x;
     acc_r = (tot.x - c.y) / c.x;
@@ -480,6 +481,13 @@ cudaError_t launch_blend_forward(int P, int R, int H, int W, const TileGrid& gri
 // split would stage every entry and flush its gradients four times).  The
 // number of items is only known on the device (chunk_base[R*T] + R*T); the
 // grid covers its bound capacity / kBwdChunk + R*T and surplus CTAs exit.
+// A work item spans `span` checkpoint intervals (its CTA starts from the
+// checkpoint at its end; the items in between exit at once): 1 while the
+// launch has few items (the chunk length is the critical path of a single
+// receiver), 4 or 8 when there are many waves of them (each CTA's fixed cost
+// -- pixel state, checkpoint, list staging, gradient flush -- is then spread
+// over more entries: 3.43 -> 2.23 ms at 200k x 32 receivers with 8).
+
 cudaError_t launch_blend_backward(int P, int R, int H, int W, const TileGrid& grid, unsigned grad_mode,
                                   long long capacity, const GeomView& geo, const ImageView& img,
                                   const BinningView& bin, const float* dL_dout_real, const float* dL_dout_imag,
@@ -488,9 +496,10 @@ cudaError_t launch_blend_backward(int P, int R, int H, int W, const TileGrid& gr
   const int RT = R * grid.T;
   const long long items = capacity / kBwdChunk + RT;
   if (items > 0x7fffffffLL) return cudaErrorInvalidValue;
+  const int span = items >= 200000 ? 8 : (items >= 16LL * 148 * 8 ? 4 : 1);
   auto k = grid.wrap ? blend_backward_kernel<kBlendThreads, true> : blend_backward_kernel<kBlendThreads, false>;
   k<<<(unsigned)items, kBlendThreads, 0, stream>>>(
-      P, H, W, grid, RT, grad_mode, img.ranges, img.chunk_base, bin.point_list, bin.ckpt, img.accum, geo, img.hdr,
+      P, H, W, grid, RT, span, grad_mode, img.ranges, img.chunk_base, bin.point_list, bin.ckpt, img.accum, geo, img.hdr,
       img.final_T, img.n_contrib, dL_dout_real, dL_dout_imag, dmean2D, dconic, dsig, dopac);
   return cudaGetLastError();
 }
