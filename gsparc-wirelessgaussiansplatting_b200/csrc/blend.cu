@@ -227,6 +227,7 @@ template <int kThreads, bool kWrap>
 __global__ void __launch_bounds__(kThreads)
 blend_backward_kernel(int P, int H, int W, TileGrid grid, int RT, int span, unsigned grad_mode,
                       const uint2* __restrict__ ranges, const uint32_t* __restrict__ chunk_base,
+                      const uint32_t* __restrict__ item_base,
                       const uint32_t* __restrict__ point_list, const float4* __restrict__ ckpt,
                       const float2* __restrict__ accum, GeomView geo, ImageHeader* __restrict__ hdr,
                       const float* __restrict__ final_Ts, const uint32_t* __restrict__ n_contrib,
@@ -244,19 +245,32 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, int RT, int span, unsi
   __shared__ float s_grad[2][kBatch][8];
   __shared__ int s_maxlast;
 
-  // work item -> (segment t, chunk): segment t owns items
-  // [chunk_base[t] + t, chunk_base[t + 1] + t + 1), one per chunk
+  // work item -> (segment t, chunk): with span 1 segment t owns items
+  // [chunk_base[t] + t, chunk_base[t + 1] + t + 1), one per chunk; with a
+  // larger span, items [item_base[t], item_base[t + 1]), one per `span` chunks
   const int item = blockIdx.x / kParts, part = blockIdx.x % kParts;
-  if (item >= (int)chunk_base[RT] + RT) return;
-  int lo = 0, hi = RT - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if ((int)chunk_base[mid] + mid <= item) lo = mid;
-    else hi = mid - 1;
+  int t, chunk;
+  if (span == 1) {
+    if (item >= (int)chunk_base[RT] + RT) return;
+    int lo = 0, hi = RT - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if ((int)chunk_base[mid] + mid <= item) lo = mid;
+      else hi = mid - 1;
+    }
+    t = lo;
+    chunk = item - ((int)chunk_base[t] + t);
+  } else {
+    if (item >= (int)item_base[RT]) return;
+    int lo = 0, hi = RT - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if ((int)item_base[mid] <= item) lo = mid;
+      else hi = mid - 1;
+    }
+    t = lo;
+    chunk = (item - (int)item_base[t]) * span;
   }
-  const int t = lo;
-  const int chunk = item - ((int)chunk_base[t] + t);
-  if (chunk & (span - 1)) return;   // covered by the item `span` chunks before it
   const uint2 range = ranges[t];
   const int jlo = chunk * kBwdChunk;
   const int jhi = min((int)(range.y - range.x), jlo + span * kBwdChunk);
@@ -482,11 +496,35 @@ cudaError_t launch_blend_forward(int P, int R, int H, int W, const TileGrid& gri
 // number of items is only known on the device (chunk_base[R*T] + R*T); the
 // grid covers its bound capacity / kBwdChunk + R*T and surplus CTAs exit.
 // A work item spans `span` checkpoint intervals (its CTA starts from the
-// checkpoint at its end; the items in between exit at once): 1 while the
+// checkpoint at its end; a one-CTA scan first numbers each tile's items): 1 while the
 // launch has few items (the chunk length is the critical path of a single
 // receiver), 4 or 8 when there are many waves of them (each CTA's fixed cost
 // -- pixel state, checkpoint, list staging, gradient flush -- is then spread
 // over more entries: 3.43 -> 2.23 ms at 200k x 32 receivers with 8).
+
+// item_base[t] = sum over tiles t' < t of ceil(chunks(t') / span), chunks(t)
+// = chunk_base[t + 1] - chunk_base[t] + 1; item_base[RT] = the item count
+__global__ void __launch_bounds__(1024)
+blend_item_scan_kernel(int RT, int span, const uint32_t* __restrict__ chunk_base, uint32_t* __restrict__ item_base) {
+  __shared__ uint32_t s_part[1024];
+  uint32_t carry = 0;
+  for (int t0 = 0; t0 < RT; t0 += 1024) {
+    const int t = t0 + (int)threadIdx.x;
+    const uint32_t v = t < RT ? (chunk_base[t + 1] - chunk_base[t] + 1u + (uint32_t)span - 1u) / (uint32_t)span : 0u;
+    s_part[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {   // inclusive Hillis-Steele scan
+      const uint32_t x = (int)threadIdx.x >= off ? s_part[threadIdx.x - off] : 0u;
+      __syncthreads();
+      s_part[threadIdx.x] += x;
+      __syncthreads();
+    }
+    if (t < RT) item_base[t] = carry + s_part[threadIdx.x] - v;
+    carry += s_part[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) item_base[RT] = carry;
+}
 
 cudaError_t launch_blend_backward(int P, int R, int H, int W, const TileGrid& grid, unsigned grad_mode,
                                   long long capacity, const GeomView& geo, const ImageView& img,
@@ -497,9 +535,14 @@ cudaError_t launch_blend_backward(int P, int R, int H, int W, const TileGrid& gr
   const long long items = capacity / kBwdChunk + RT;
   if (items > 0x7fffffffLL) return cudaErrorInvalidValue;
   const int span = items >= 200000 ? 8 : (items >= 16LL * 148 * 8 ? 4 : 1);
+  long long grid_items = items;
+  if (span > 1) {
+    blend_item_scan_kernel<<<1, 1024, 0, stream>>>(RT, span, img.chunk_base, img.item_base);
+    grid_items = capacity / (kBwdChunk * span) + 2LL * RT;   // bounds sum ceil(chunks / span)
+  }
   auto k = grid.wrap ? blend_backward_kernel<kBlendThreads, true> : blend_backward_kernel<kBlendThreads, false>;
-  k<<<(unsigned)items, kBlendThreads, 0, stream>>>(
-      P, H, W, grid, RT, span, grad_mode, img.ranges, img.chunk_base, bin.point_list, bin.ckpt, img.accum, geo, img.hdr,
+  k<<<(unsigned)grid_items, kBlendThreads, 0, stream>>>(
+      P, H, W, grid, RT, span, grad_mode, img.ranges, img.chunk_base, img.item_base, bin.point_list, bin.ckpt, img.accum, geo, img.hdr,
       img.final_T, img.n_contrib, dL_dout_real, dL_dout_imag, dmean2D, dconic, dsig, dopac);
   return cudaGetLastError();
 }

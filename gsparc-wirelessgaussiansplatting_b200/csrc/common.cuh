@@ -94,6 +94,7 @@ struct ImageView {
   uint32_t* n_contrib;
   uint32_t* chunk_base;   // [R*T + 1]: exclusive scan of interior chunk boundaries per tile
   float2* accum;          // [R, H, W]: accumulated (real, imag) of the forward
+  uint32_t* item_base;    // [R*T + 1]: first adjoint work item of each tile (written by the adjoint launch)
 };
 
 // The adjoint walks each tile's list in chunks of kBwdChunk entries, one CTA
@@ -148,10 +149,11 @@ __host__ __device__ inline size_t carve_image(char* base, size_t R, size_t T, si
   char* e = take(R * npix * sizeof(uint32_t));
   char* f = take((R * T + 1) * sizeof(uint32_t));
   char* g = take(R * npix * sizeof(float2));
+  char* i = take((R * T + 1) * sizeof(uint32_t));
   if (v) {
     v->hdr = (ImageHeader*)h; v->ranges = (uint2*)a; v->counts = (uint32_t*)b;
     v->cursor = (uint32_t*)c; v->final_T = (float*)d; v->n_contrib = (uint32_t*)e;
-    v->chunk_base = (uint32_t*)f; v->accum = (float2*)g;
+    v->chunk_base = (uint32_t*)f; v->accum = (float2*)g; v->item_base = (uint32_t*)i;
   }
   return off;
 }
