@@ -498,9 +498,9 @@ cudaError_t launch_blend_forward(int P, int R, int H, int W, const TileGrid& gri
 // A work item spans `span` checkpoint intervals (its CTA starts from the
 // checkpoint at its end; a one-CTA scan first numbers each tile's items): 1 while the
 // launch has few items (the chunk length is the critical path of a single
-// receiver), 4 or 8 when there are many waves of them (each CTA's fixed cost
-// -- pixel state, checkpoint, list staging, gradient flush -- is then spread
-// over more entries: 3.43 -> 2.23 ms at 200k x 32 receivers with 8).
+// receiver), up to 32 when there are many waves of them (each CTA's fixed
+// cost -- pixel state, checkpoint, list staging, gradient flush -- is then
+// spread over more entries: 3.43 -> 0.73 ms at 200k x 32 receivers).
 
 // item_base[t] = sum over tiles t' < t of ceil(chunks(t') / span), chunks(t)
 // = chunk_base[t + 1] - chunk_base[t] + 1; item_base[RT] = the item count
@@ -534,7 +534,8 @@ cudaError_t launch_blend_backward(int P, int R, int H, int W, const TileGrid& gr
   const int RT = R * grid.T;
   const long long items = capacity / kBwdChunk + RT;
   if (items > 0x7fffffffLL) return cudaErrorInvalidValue;
-  const int span = items >= 200000 ? 8 : (items >= 16LL * 148 * 8 ? 4 : 1);
+  int span = 1;   // the largest power of two up to 32 that leaves about 64 items per SM
+  while (span < 32 && items >= 2LL * span * 148 * 64) span *= 2;
   long long grid_items = items;
   if (span > 1) {
     blend_item_scan_kernel<<<1, 1024, 0, stream>>>(RT, span, img.chunk_base, img.item_base);
