@@ -111,7 +111,7 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
                   const float* __restrict__ opacities, const float* __restrict__ scales,
                   const float* __restrict__ rotations, const float* __restrict__ views,
                   const float* __restrict__ tx_pos, const float* __restrict__ rx_pos,
-                  GeomView geo, int* __restrict__ radii_out, ImageView img) {
+                  GeomView geo, int* __restrict__ radii_out, ImageView img, int per_cta) {
   uint32_t* __restrict__ counts = img.counts;
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -119,12 +119,16 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
   uint32_t* dhist = reinterpret_cast<uint32_t*>(smem + (kPreThreads / 32) * kMlpSmemPerWarp);
   uint32_t* hist = dhist + 1024;
   const int r = blockIdx.y;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
   for (int t = threadIdx.x; t < 1024; t += blockDim.x) dhist[t] = 0;
   if (kSharedHist)
     for (int t = threadIdx.x; t < grid.T; t += blockDim.x) hist[t] = 0;
   __syncthreads();
 
+  // per_cta consecutive groups of kPreThreads Gaussians, the histograms
+  // flushed once for all of them
+  for (int grp = 0; grp < per_cta; ++grp) {
+  const int g0 = (blockIdx.x * per_cta + grp) * kPreThreads;
+  const int g = g0 + (int)threadIdx.x;
   bool vis = false;
   int x0 = 0, y0 = 0, x1 = 0, y1 = 0;
   TileSpan span{0, 0, 0, 0, grid.gx, 0};
@@ -209,7 +213,7 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
   // emission MLP of the visible Gaussians, from the warp's staged parameters
   // (no per-Gaussian MLP: the signal is written later by the shared MLP)
   if (mlp != nullptr && __any_sync(0xffffffffu, vis)) {
-    stage_mlp<kVec>(sm_mlp, mlp, P, blockIdx.x * blockDim.x + wid * 32, lane);
+    stage_mlp<kVec>(sm_mlp, mlp, P, g0 + wid * 32, lane);
     __syncwarp();
     if (vis) {
       const float3 rx = make_float3(__ldg(rx_pos + 3 * r), __ldg(rx_pos + 3 * r + 1), __ldg(rx_pos + 3 * r + 2));
@@ -223,6 +227,8 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
       if (kSharedHist) atomicAdd(&hist[tile], 1u);
       else atomicAdd(&counts[(size_t)r * grid.T + tile], 1u);
     });
+  }
+  __syncwarp();   // the warp's staged MLP rows are read before the next group restages them
   }
   __syncthreads();
   if (kSharedHist) {
@@ -297,26 +303,31 @@ cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, 
     if (dev >= 0 && dev < 64) attr_done[dev] = true;
   }
   const bool vec = (((uintptr_t)mlp) & 15u) == 0;
-  dim3 block(kPreThreads), gridd((P + kPreThreads - 1) / kPreThreads, R);
+  // groups of kPreThreads Gaussians per CTA: one while the launch is small
+  // (latency), up to 16 when it fills many waves, so that each CTA's
+  // histogram initialisation and flush serve up to 1,024 Gaussians
+  int per_cta = 1;
+  while (per_cta < 16 && (long long)P * R >= 2LL * per_cta * 148 * kPreThreads * 16) per_cta *= 2;
+  dim3 block(kPreThreads), gridd((P + kPreThreads * per_cta - 1) / (kPreThreads * per_cta), R);
   if (grid.T <= kMaxSharedHistTiles) {
     const size_t smem = kMlpSmemBytes + (size_t)grid.T * sizeof(uint32_t);
     if (vec)
       preprocess_kernel<true, true><<<gridd, block, smem, stream>>>(P, H, W, grid, mod, means3D, mlp, opacities,
                                                                     scales, rotations, views, tx_pos, rx_pos, geo,
-                                                                    radii_out, img);
+                                                                    radii_out, img, per_cta);
     else
       preprocess_kernel<true, false><<<gridd, block, smem, stream>>>(P, H, W, grid, mod, means3D, mlp, opacities,
                                                                      scales, rotations, views, tx_pos, rx_pos, geo,
-                                                                     radii_out, img);
+                                                                     radii_out, img, per_cta);
   } else {
     if (vec)
       preprocess_kernel<false, true><<<gridd, block, kMlpSmemBytes, stream>>>(
           P, H, W, grid, mod, means3D, mlp, opacities, scales, rotations, views, tx_pos, rx_pos, geo, radii_out,
-          img);
+          img, per_cta);
     else
       preprocess_kernel<false, false><<<gridd, block, kMlpSmemBytes, stream>>>(
           P, H, W, grid, mod, means3D, mlp, opacities, scales, rotations, views, tx_pos, rx_pos, geo, radii_out,
-          img);
+          img, per_cta);
   }
   return cudaGetLastError();
 }
