@@ -340,8 +340,10 @@ def run_ours(args):
         "geometry_backward_kernel": vis * (12 + 40 + 24 + 24 + 24) + P_GAUSS * 64,
         "splat_loss_kernels": npix * (8 + 12) + npix * (8 + 12 + 4),
         "gaussian_adam_kernels": P_GAUSS * (11 * 4 * 7 + 8 * 4) + trainer.n_mlp * 4 * 7,
-        "shared_mlp_forward_kernels": P_GAUSS * (12 + 32 * 4 + 2 * 64 * 4 * 2 + 8),
-        "shared_mlp_backward_kernels": P_GAUSS * (32 * 4 + 2 * 64 * 4 * 3 + 8),
+        # fused width-64 MLP: means, radii in; S, signal and both hidden layers' Z out
+        "shared_mlp_forward_kernels": P_GAUSS * (12 + 4 + 4 + 8 + 2 * 64 * 4),
+        # means, radii, S, dL/dsignal and Z in, dL/dx out; then dL/dx in, dL/dmeans out
+        "shared_mlp_backward_kernels": P_GAUSS * (12 + 4 + 4 + 8 + 2 * 64 * 4 + 32 * 4) + P_GAUSS * (32 * 4 + 12 + 12),
     }
     peak, peak_kind = _peaks()
     achieved = alg.get(dom, 0) / (dom_ms / 1000.0) / 1e9

@@ -46,18 +46,6 @@ __device__ __forceinline__ float act_grad(int act, float z) {
   return act == 1 ? (z > 0.0f ? 1.0f : 0.0f) : (act == 2 ? gelu_erf_grad(z) : 1.0f);
 }
 
-// activation and its derivative together (one erf for GELU); same values as act_fwd / act_grad
-__device__ __forceinline__ void act_both(int act, float z, float& a, float& d) {
-  if (act == 2) {
-    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-    a = 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
-    d = cdf + z * (0.39894228040143268f * expf(-0.5f * z * z));
-  } else {
-    a = act_fwd(act, z);
-    d = act_grad(act, z);
-  }
-}
-
 // ---- features ---------------------------------------------------------------
 // x = [mu, sin/cos(2^k pi mu_j) for k < 4, (mu - rx) / d, 1 / d^2, 0]
 __device__ __forceinline__ void pair_features_fp32(const float* __restrict__ means3D, const float* __restrict__ rx_pos,
@@ -261,9 +249,12 @@ mlp_signal_backward_kernel(size_t rows, int Cout, const float* __restrict__ S, c
 // registers and the weights in shared memory (every thread reads the same
 // weight at the same time: broadcast).  Each layer's sums run in the same
 // order as the tiled GEMMs above (inputs ascending from zero, then + bias), so
-// the forward matches them bit for bit.  The adjoint recomputes the forward (no
-// activations go to HBM) and reduces the weight gradients over each tile of
-// 128 rows in shared memory, accumulating per thread across tiles.
+// the forward matches them bit for bit.  The forward also writes each hidden
+// layer's pre-activations Z (fp32, tile-transposed: [layer][tile][64][128], so a
+// warp's float4 stores and loads are contiguous) next to the sigmoid outputs S;
+// the adjoint reads them instead of recomputing the forward GEMMs, and reduces
+// the weight gradients over each tile of 128 rows in shared memory,
+// accumulating per thread across tiles.
 constexpr int kW64 = 64;
 constexpr int kFusedRows = 128;
 
@@ -289,12 +280,10 @@ __device__ __forceinline__ void store_row(float* dst, const float* v) {
 // W [64][K] (row-major, global) -> W^T [K][64] in shared memory.  Each thread
 // takes four consecutive inputs of one output row, consecutive threads
 // consecutive outputs, so the shared-memory writes of a warp are contiguous;
-// every load is independent (all of them in flight at once).  When `rows` is
-// given, the row-major copy is written from the same loads.  blockDim.x must
+// every load is independent (all of them in flight at once).  blockDim.x must
 // be kFusedRows.
 template <int K>
-__device__ __forceinline__ void stage_transposed(float* __restrict__ dst, const float* __restrict__ W,
-                                                 float* __restrict__ rows = nullptr) {
+__device__ __forceinline__ void stage_transposed(float* __restrict__ dst, const float* __restrict__ W) {
   constexpr int kItems = kW64 * (K / 4);
 #pragma unroll
   for (int it = 0; it < (kItems + kFusedRows - 1) / kFusedRows; ++it) {
@@ -306,7 +295,6 @@ __device__ __forceinline__ void stage_transposed(float* __restrict__ dst, const 
       dst[(k + 1) * kW64 + j] = w1;
       dst[(k + 2) * kW64 + j] = w2;
       dst[(k + 3) * kW64 + j] = w3;
-      if (rows) *reinterpret_cast<float4*>(rows + j * K + k) = make_float4(w0, w1, w2, w3);
     }
   }
 }
@@ -359,7 +347,7 @@ template <int kL, int kAct>
 __global__ void __launch_bounds__(kFusedRows)
 mlp64_forward_kernel(int P, size_t rows, const float* __restrict__ means3D, const float* __restrict__ rx_pos,
                      const float* __restrict__ params, const int* __restrict__ radii, float* __restrict__ S,
-                     float2* __restrict__ signal) {
+                     float* __restrict__ Z, float2* __restrict__ signal) {
   using FP = FusedParams<kL>;
   using SM = FusedFwdSmem<kL>;
   extern __shared__ __align__(16) float sm[];
@@ -378,9 +366,11 @@ mlp64_forward_kernel(int P, size_t rows, const float* __restrict__ means3D, cons
   // a column group, so the transposed stores of a lane octet are contiguous
   const int r0 = (t & 15) * 4, c0 = (t >> 4) * 4;
   const size_t ntiles = (rows + kFusedRows - 1) / kFusedRows;
+  const size_t zl = ntiles * (kFusedRows * kW64);   // floats of one layer's Z
   for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const size_t row = tile * kFusedRows + t;
     const bool vis = row < rows && radii[row] > 0;
+    float* Zt = Z + tile * (kFusedRows * kW64);
     __syncthreads();   // the previous tile's reads of XT / HT are done
     {
       float x[kFeat];
@@ -399,14 +389,19 @@ mlp64_forward_kernel(int P, size_t rows, const float* __restrict__ means3D, cons
       for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
     gemm_8x8<kFeat>(XT, kFusedRows, sm + SM::kWt0, kW64, r0, c0, acc);
     if (kL == 2) {
-      // H^T = act(Z0 + b0), then the second layer over it
+      // Z0 = X W0^T + b0 -> HBM, H^T = act(Z0), then the second layer over it
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int c = c0 + (j & 3) + (j >> 2) * 32;
         const float b = sm[SM::kB0 + c];
-        float h[8];
+        float z[8], h[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) h[i] = act_fwd(kAct, acc[i][j] + b);
+        for (int i = 0; i < 8; ++i) {
+          z[i] = acc[i][j] + b;
+          h[i] = act_fwd(kAct, z[i]);
+        }
+        *reinterpret_cast<float4*>(Zt + c * kFusedRows + r0) = make_float4(z[0], z[1], z[2], z[3]);
+        *reinterpret_cast<float4*>(Zt + c * kFusedRows + r0 + 64) = make_float4(z[4], z[5], z[6], z[7]);
         *reinterpret_cast<float4*>(HT + c * kFusedRows + r0) = make_float4(h[0], h[1], h[2], h[3]);
         *reinterpret_cast<float4*>(HT + c * kFusedRows + r0 + 64) = make_float4(h[4], h[5], h[6], h[7]);
       }
@@ -421,13 +416,19 @@ mlp64_forward_kernel(int P, size_t rows, const float* __restrict__ means3D, cons
     // the last hidden layer's activations -> H^T, then the output per row in the
     // GEMMs' order (hidden units ascending)
     const float* bl = sm + (kL == 2 ? SM::kB1 : SM::kB0);
+    float* Zl = Zt + (kL - 1) * zl;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int c = c0 + (j & 3) + (j >> 2) * 32;
       const float b = bl[c];
-      float h[8];
+      float z[8], h[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) h[i] = act_fwd(kAct, acc[i][j] + b);
+      for (int i = 0; i < 8; ++i) {
+        z[i] = acc[i][j] + b;
+        h[i] = act_fwd(kAct, z[i]);
+      }
+      *reinterpret_cast<float4*>(Zl + c * kFusedRows + r0) = make_float4(z[0], z[1], z[2], z[3]);
+      *reinterpret_cast<float4*>(Zl + c * kFusedRows + r0 + 64) = make_float4(z[4], z[5], z[6], z[7]);
       *reinterpret_cast<float4*>(HT + c * kFusedRows + r0) = make_float4(h[0], h[1], h[2], h[3]);
       *reinterpret_cast<float4*>(HT + c * kFusedRows + r0 + 64) = make_float4(h[4], h[5], h[6], h[7]);
     }
@@ -468,20 +469,17 @@ __device__ __forceinline__ void gemm_8x4(const float* __restrict__ AT, int lda, 
   }
 }
 
-// adjoint shared memory (floats): weights W0 [64][32], W0^T, W1 [64][64], W1^T (two
-// layers), b0, b1, wo, bo; tiles X^T [32][128] (forward operand), X [128][36]
-// (rows, for dW0), HT [64][128] (H0^T, then H1^T, then dZ1^T, then dZ0^T), A0 [128][68]
-// (rows, for dW1), G0^T [64][128] (act'(Z0)), D [128][68] (dZ1, then dZ0, rows),
+// adjoint shared memory (floats): weights W0 [64][32], W1 [64][64] (two layers),
+// b0, b1, wo, bo; tiles X [128][36] (rows, for dW0), HT [64][128] (dZ1^T, then
+// dZ0^T), A0 [128][68] (act(Z0) rows, for dW1), D [128][68] (dZ1, then dZ0, rows),
 // dO [128], dwo [64 + 4]
 template <int kL>
 struct FusedTiles {
-  static constexpr int kW0 = 0, kWt0 = kW0 + kW64 * kFeat, kW1 = kWt0 + kFeat * kW64;
-  static constexpr int kWt1 = kW1 + (kL == 2 ? kW64 * kW64 : 0), kB0 = kWt1 + (kL == 2 ? kW64 * kW64 : 0);
+  static constexpr int kW0 = 0, kW1 = kW0 + kW64 * kFeat, kB0 = kW1 + (kL == 2 ? kW64 * kW64 : 0);
   static constexpr int kB1 = kB0 + kW64, kWo = kB1 + kW64, kBo = kWo + kW64;
-  static constexpr int kXT = kBo + 4, kX = kXT + kFeat * kFusedRows, kHT = kX + kFusedRows * kXs;
-  static constexpr int kA0 = kHT + kW64 * kFusedRows, kG0T = kA0 + (kL == 2 ? kFusedRows * kHs : 0);
-  static constexpr int kD = kG0T + (kL == 2 ? kW64 * kFusedRows : 0), kDO = kD + kFusedRows * kHs;
-  static constexpr int kDwo = kDO + kFusedRows, kTotal = kDwo + kW64 + 4;
+  static constexpr int kX = kBo + 4, kHT = kX + kFusedRows * kXs;
+  static constexpr int kA0 = kHT + kW64 * kFusedRows, kD = kA0 + (kL == 2 ? kFusedRows * kHs : 0);
+  static constexpr int kDO = kD + kFusedRows * kHs, kDwo = kDO + kFusedRows, kTotal = kDwo + kW64 + 4;
 };
 
 // acc[4][NI] += sum over the tile's rows of D[r][j0..j0+3] (x) A[r][i0..i0+NI-1];
@@ -533,6 +531,16 @@ __device__ __forceinline__ void store_block4_T(float* T, int r0, int c0, const f
     *reinterpret_cast<float4*>(T + (c0 + j) * kFusedRows + r0 + 64) = make_float4(v[4][j], v[5][j], v[6][j], v[7][j]);
   }
 }
+// T [col][row] (transposed tile, 128 rows, global) -> v[8][4] of the thread's block
+__device__ __forceinline__ void load_block4_T(const float* __restrict__ T, int r0, int c0, float (&v)[8][4]) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float4 a = *reinterpret_cast<const float4*>(T + (c0 + j) * kFusedRows + r0);
+    const float4 b = *reinterpret_cast<const float4*>(T + (c0 + j) * kFusedRows + r0 + 64);
+    v[0][j] = a.x; v[1][j] = a.y; v[2][j] = a.z; v[3][j] = a.w;
+    v[4][j] = b.x; v[5][j] = b.y; v[6][j] = b.z; v[7][j] = b.w;
+  }
+}
 // v[8][4] -> D [row][col] (row tiles, stride kHs)
 __device__ __forceinline__ void store_block4_rows(float* D, int r0, int c0, const float (&v)[8][4]) {
 #pragma unroll
@@ -543,17 +551,17 @@ __device__ __forceinline__ void store_block4_rows(float* D, int r0, int c0, cons
 template <int kL, int kAct>
 __global__ void __launch_bounds__(kAdjThreads, 1)
 mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, const float* __restrict__ rx_pos,
-                      const float* __restrict__ params, const int* __restrict__ radii,
-                      const float* __restrict__ dL_dsignal, float* __restrict__ dX, float* __restrict__ dparams) {
+                      const float* __restrict__ params, const int* __restrict__ radii, const float* __restrict__ S,
+                      const float* __restrict__ Z, const float* __restrict__ dL_dsignal, float* __restrict__ dX,
+                      float* __restrict__ dparams) {
   using FP = FusedParams<kL>;
   using TL = FusedTiles<kL>;
   extern __shared__ __align__(16) float sm[];
   const int t = threadIdx.x, lane = t & 31;
   const bool row_thread = t < kFusedRows;   // one tile row per thread in the per-row phases
-  if (row_thread) {
-    stage_transposed<kFeat>(sm + TL::kWt0, params + FP::kW0, sm + TL::kW0);
-    if (kL == 2) stage_transposed<kW64>(sm + TL::kWt1, params + FP::kW1, sm + TL::kW1);
-  }
+  for (int i = t; i < kW64 * kFeat; i += kAdjThreads) sm[TL::kW0 + i] = params[FP::kW0 + i];
+  if (kL == 2)
+    for (int i = t; i < kW64 * kW64; i += kAdjThreads) sm[TL::kW1 + i] = params[FP::kW1 + i];
   for (int i = t; i < kW64; i += kAdjThreads) {
     sm[TL::kB0 + i] = params[FP::kB0 + i];
     if (kL == 2) sm[TL::kB1 + i] = params[FP::kB1 + i];
@@ -561,11 +569,9 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
   }
   if (t == 0) sm[TL::kBo] = params[FP::kBo];
   for (int i = t; i < kW64 + 4; i += kAdjThreads) sm[TL::kDwo + i] = 0.0f;
-  float* XT = sm + TL::kXT;
   float* Xr = sm + TL::kX;
   float* HT = sm + TL::kHT;
   float* A0 = sm + TL::kA0;
-  float* G0T = sm + TL::kG0T;
   float* D = sm + TL::kD;
   float* sdO = sm + TL::kDO;
   float* dwo = sm + TL::kDwo;
@@ -577,9 +583,11 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
   float g1[4][4] = {}, gb1[4] = {};   // accumulated over tiles
   float g0[4][4] = {}, gb0[4] = {};
   const size_t ntiles = (rows + kFusedRows - 1) / kFusedRows;
+  const size_t zl = ntiles * (kFusedRows * kW64);   // floats of one layer's Z
   for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const size_t row = tile * kFusedRows + t;
     const bool vis = row_thread && row < rows && radii[row] > 0;
+    const float* Zt = Z + tile * (kFusedRows * kW64);
     __syncthreads();   // weights staged / the previous tile's reads done
     if (row_thread) {
       float x[kFeat];
@@ -587,62 +595,9 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
       else
 #pragma unroll
         for (int f = 0; f < kFeat; ++f) x[f] = 0.0f;
-#pragma unroll
-      for (int f = 0; f < kFeat; ++f) XT[f * kFusedRows + t] = x[f];
       store_row<kFeat>(Xr + t * kXs, x);
-    }
-    __syncthreads();
-    // ---- forward recompute (the sums of mlp64_forward_kernel)
-    float acc[8][4];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
-    gemm_8x4<kFeat>(XT, kFusedRows, sm + TL::kWt0, kW64, r0, c0, acc);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const float b = sm[TL::kB0 + c0 + j];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) acc[i][j] += b;
-    }
-    if (kL == 2) {
-      float h[8][4], gd[8][4];
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) act_both(kAct, acc[i][j], h[i][j], gd[i][j]);
-      store_block4_T(HT, r0, c0, h);
-      store_block4_rows(A0, r0, c0, h);
-      store_block4_T(G0T, r0, c0, gd);
-      __syncthreads();
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
-      gemm_8x4<kW64>(HT, kFusedRows, sm + TL::kWt1, kW64, r0, c0, acc);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const float b = sm[TL::kB1 + c0 + j];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) acc[i][j] += b;
-      }
-      __syncthreads();   // HT (H0^T) fully read
-    }
-    // acc = Z of the last hidden layer.  Its activations -> HT, output per row
-    {
-      float h[8][4];
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) h[i][j] = act_fwd(kAct, acc[i][j]);
-      store_block4_T(HT, r0, c0, h);
-    }
-    __syncthreads();
-    if (row_thread) {
-      float o = 0.0f;
-#pragma unroll 8
-      for (int j = 0; j < kW64; ++j) o = fmaf(HT[j * kFusedRows + t], wo[j], o);
-      const float sg = 1.0f / (1.0f + expf(-(o + sm[TL::kBo])));
+      // output layer: dL/do = dL/dsignal * S (1 - S), S from the forward
+      const float sg = vis ? S[row] : 0.0f;
       const float dO = vis ? dL_dsignal[2 * row] * sg * (1.0f - sg) : 0.0f;
       sdO[t] = dO;
       float ds = dO;
@@ -650,7 +605,19 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
       for (int q = 16; q > 0; q >>= 1) ds += __shfl_xor_sync(0xffffffffu, ds, q);
       if (lane == 0) atomicAdd(&dwo[kW64], ds);
     }
-    __syncthreads();   // dO ready; HT (H^T) fully read
+    // the forward's pre-activations of this thread's block: act(Z0) -> A0 rows
+    // (two layers), the last hidden layer's Z -> acc
+    float acc[8][4];
+    if (kL == 2) {
+      load_block4_T(Zt, r0, c0, acc);
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = act_fwd(kAct, acc[i][j]);
+      store_block4_rows(A0, r0, c0, acc);
+    }
+    load_block4_T(Zt + (kL - 1) * zl, r0, c0, acc);
+    __syncthreads();   // dO and A0 ready
     {
       // output-layer weight gradient: this block's rows, then over the 16 row groups (lanes)
       float dOr[8];
@@ -691,12 +658,13 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
       gemm_8x4<kW64>(HT, kFusedRows, sm + TL::kW1, kW64, r0, c0, acc);
+      {
+        float z[8][4];   // Z0 again (this CTA read it a moment ago: L2)
+        load_block4_T(Zt, r0, c0, z);
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const float4 ga = *reinterpret_cast<const float4*>(G0T + (c0 + j) * kFusedRows + r0);
-        const float4 gb = *reinterpret_cast<const float4*>(G0T + (c0 + j) * kFusedRows + r0 + 64);
-        acc[0][j] *= ga.x; acc[1][j] *= ga.y; acc[2][j] *= ga.z; acc[3][j] *= ga.w;
-        acc[4][j] *= gb.x; acc[5][j] *= gb.y; acc[6][j] *= gb.z; acc[7][j] *= gb.w;
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] *= act_grad(kAct, z[i][j]);
       }
       __syncthreads();   // D (dZ1) and HT (dZ1^T) fully read
       store_block4_rows(D, r0, c0, acc);
@@ -766,12 +734,12 @@ static cudaError_t launch_fused(bool fwd, int P, size_t rows, const float* means
   if (fwd) {
     const size_t cap = (size_t)sms * 2;   // persistent, two CTAs per SM (74 KB of shared memory each)
     mlp64_forward_kernel<kL, kAct><<<(unsigned)(ntiles < cap ? ntiles : cap), kFusedRows, smem, s>>>(
-        P, rows, means3D, rx_pos, params, geo.radii, work + L.s, geo.signal);
+        P, rows, means3D, rx_pos, params, geo.radii, work + L.s, work + L.z[1], geo.signal);
     return cudaGetLastError();
   }
   const unsigned grid = (unsigned)(ntiles < (size_t)sms ? ntiles : (size_t)sms);
-  mlp64_backward_kernel<kL, kAct><<<grid, kAdjThreads, smem, s>>>(P, rows, means3D, rx_pos, params, geo.radii,
-                                                                 dL_dsignal, work + L.d0, dparams);
+  mlp64_backward_kernel<kL, kAct><<<grid, kAdjThreads, smem, s>>>(
+      P, rows, means3D, rx_pos, params, geo.radii, work + L.s, work + L.z[1], dL_dsignal, work + L.d0, dparams);
   return cudaGetLastError();
 }
 
@@ -804,9 +772,11 @@ SharedMlpLayout shared_mlp_layout(int layers, int width, int out, size_t rows) {
   L.params = p;
   auto al = [](size_t x) { return (x + 63) / 64 * 64; };   // 256-byte aligned segments
   size_t w = 0;
-  if (shared_mlp_fused(layers, width, out)) {   // the fused kernels keep only S and dL/dx
+  if (shared_mlp_fused(layers, width, out)) {   // the fused kernels keep S, the hidden Z (tiles) and dL/dx
     L.s = w;
     w += al(rows);
+    L.z[1] = w;
+    w += (size_t)layers * ((rows + kFusedRows - 1) / kFusedRows) * kFusedRows * kW64;
     L.d0 = L.d1 = w;
     w += al(rows * kFeat);
     L.work = w;
