@@ -303,6 +303,12 @@ __device__ __forceinline__ void stage_transposed(float* __restrict__ dst, const 
 // consecutive rows' float4s fall on distinct banks.
 constexpr int kXs = kFeat + 4, kHs = kW64 + 4;
 
+// Column swizzle of the 64-wide row tiles (D, A0): row r keeps its float4
+// groups but XORs their index with (r / 4) mod 8.  The 8x4 blocks' row-major
+// stores put rows 4 apart in the lanes of one quarter-warp; without the XOR
+// those rows land on two bank groups (4-way conflicts), with it on eight.
+__device__ __forceinline__ int row_swz(int r) { return ((r >> 2) & 7) << 2; }
+
 // C[8 rows][8 cols] += sum_k AT[k][rows] * BT[k][cols], k ascending from zero:
 // a register-blocked SIMT GEMM step over operands in shared memory (AT rows
 // contiguous, BT columns contiguous).  The thread's rows are r0..r0+3 and
@@ -483,17 +489,19 @@ struct FusedTiles {
 };
 
 // acc[4][NI] += sum over the tile's rows of D[r][j0..j0+3] (x) A[r][i0..i0+NI-1];
-// bsum[4] += sum of D[r][j0..j0+3] when `bias`
+// bsum[4] += sum of D[r][j0..j0+3] when `bias`.  D is a swizzled row tile (row_swz),
+// A one too when its stride is kHs (A0), else plain rows (X)
 template <int NI, int kAs>
 __device__ __forceinline__ void tile_outer(const float* __restrict__ D, const float* __restrict__ A, int j0, int i0,
                                            bool bias, float (&acc)[4][NI], float (&bsum)[4]) {
 #pragma unroll 2
   for (int r = 0; r < kFusedRows; ++r) {
-    const float4 d = *reinterpret_cast<const float4*>(D + r * kHs + j0);
+    const float4 d = *reinterpret_cast<const float4*>(D + r * kHs + (j0 ^ row_swz(r)));
     float a[NI];
 #pragma unroll
     for (int q = 0; q < NI / 4; ++q) {
-      const float4 v = *reinterpret_cast<const float4*>(A + r * kAs + i0 + 4 * q);
+      const int ci = kAs == kHs ? ((i0 + 4 * q) ^ row_swz(r)) : i0 + 4 * q;
+      const float4 v = *reinterpret_cast<const float4*>(A + r * kAs + ci);
       a[4 * q] = v.x; a[4 * q + 1] = v.y; a[4 * q + 2] = v.z; a[4 * q + 3] = v.w;
     }
     const float dd[4] = {d.x, d.y, d.z, d.w};
@@ -541,11 +549,13 @@ __device__ __forceinline__ void load_block4_T(const float* __restrict__ T, int r
     v[4][j] = b.x; v[5][j] = b.y; v[6][j] = b.z; v[7][j] = b.w;
   }
 }
-// v[8][4] -> D [row][col] (row tiles, stride kHs)
+// v[8][4] -> D [row][col] (swizzled row tiles, stride kHs)
 __device__ __forceinline__ void store_block4_rows(float* D, int r0, int c0, const float (&v)[8][4]) {
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
-    *reinterpret_cast<float4*>(D + blk_row(r0, i) * kHs + c0) = make_float4(v[i][0], v[i][1], v[i][2], v[i][3]);
+  for (int i = 0; i < 8; ++i) {
+    const int r = blk_row(r0, i);
+    *reinterpret_cast<float4*>(D + r * kHs + (c0 ^ row_swz(r))) = make_float4(v[i][0], v[i][1], v[i][2], v[i][3]);
+  }
 }
 
 template <int kL, int kAct>
