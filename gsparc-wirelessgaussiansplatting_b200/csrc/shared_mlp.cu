@@ -742,7 +742,16 @@ static cudaError_t launch_fused(bool fwd, int P, size_t rows, const float* means
   }
   const size_t ntiles = (rows + kFusedRows - 1) / kFusedRows;
   if (fwd) {
-    const size_t cap = (size_t)sms * 2;   // persistent, two CTAs per SM (74 KB of shared memory each)
+    // persistent: as many CTAs per SM as fit (74 KB of shared memory each: three)
+    static int per_sm[64][2][3] = {};
+    int occ = dev >= 0 && dev < 64 ? per_sm[dev][kL - 1][kAct] : 0;
+    if (occ == 0) {
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mlp64_forward_kernel<kL, kAct>, kFusedRows, smem);
+      if (e != cudaSuccess) return e;
+      if (occ < 1) occ = 1;
+      if (dev >= 0 && dev < 64) per_sm[dev][kL - 1][kAct] = occ;
+    }
+    const size_t cap = (size_t)sms * occ;
     mlp64_forward_kernel<kL, kAct><<<(unsigned)(ntiles < cap ? ntiles : cap), kFusedRows, smem, s>>>(
         P, rows, means3D, rx_pos, params, geo.radii, work + L.s, work + L.z[1], geo.signal);
     return cudaGetLastError();
