@@ -88,13 +88,11 @@ mlp_features_kernel(int P, const float* __restrict__ means3D, const float* __res
   for (int i = 0; i < kFeat; ++i) x[i] = f[i];
 }
 
-// dL/dmu from dL/dx, summed over receivers (thread per Gaussian).
-__global__ void __launch_bounds__(256)
-mlp_features_backward_kernel(int P, int R, const float* __restrict__ means3D, const float* __restrict__ rx_pos,
-                             const int* __restrict__ radii, const float* __restrict__ dX,
-                             float* __restrict__ dL_dmeans3D) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= P) return;
+// dL/dmu of Gaussian g from dL/dx, summed over receivers in order.  dX is read
+// through L2 (it may have been written earlier in the same kernel).
+__device__ __forceinline__ void features_adjoint(int g, int P, int R, const float* __restrict__ means3D,
+                                                 const float* __restrict__ rx_pos, const int* __restrict__ radii,
+                                                 const float* dX, float* __restrict__ dL_dmeans3D) {
   const float m[3] = {means3D[3 * g], means3D[3 * g + 1], means3D[3 * g + 2]};
   float acc[3] = {0.0f, 0.0f, 0.0f};
   // positional part does not depend on the receiver: sum dX over receivers first
@@ -104,7 +102,9 @@ mlp_features_backward_kernel(int P, int R, const float* __restrict__ means3D, co
   for (int r = 0; r < R; ++r) {
     const size_t row = (size_t)r * P + g;
     if (radii[row] <= 0) continue;
-    const float* dx = dX + row * kFeat;
+    float dx[31];
+#pragma unroll
+    for (int i = 0; i < 31; ++i) dx[i] = __ldcg(dX + row * kFeat + i);
 #pragma unroll
     for (int i = 0; i < 27; ++i) sum_pe[i] += dx[i];
     const float v[3] = {m[0] - rx_pos[3 * r], m[1] - rx_pos[3 * r + 1], m[2] - rx_pos[3 * r + 2]};
@@ -130,6 +130,15 @@ mlp_features_backward_kernel(int P, int R, const float* __restrict__ means3D, co
     }
     dL_dmeans3D[3 * g + j] += gj + acc[j];
   }
+}
+
+// thread per Gaussian
+__global__ void __launch_bounds__(256)
+mlp_features_backward_kernel(int P, int R, const float* __restrict__ means3D, const float* __restrict__ rx_pos,
+                             const int* __restrict__ radii, const float* __restrict__ dX,
+                             float* __restrict__ dL_dmeans3D) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < P) features_adjoint(g, P, R, means3D, rx_pos, radii, dX, dL_dmeans3D);
 }
 
 // ---- tiled SIMT GEMM ----------------------------------------------------------
@@ -558,12 +567,12 @@ __device__ __forceinline__ void store_block4_rows(float* D, int r0, int c0, cons
   }
 }
 
-template <int kL, int kAct>
+template <int kL, int kAct, bool kFeatAdj>
 __global__ void __launch_bounds__(kAdjThreads, 1)
 mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, const float* __restrict__ rx_pos,
                       const float* __restrict__ params, const int* __restrict__ radii, const float* __restrict__ S,
-                      const float* __restrict__ Z, const float* __restrict__ dL_dsignal, float* __restrict__ dX,
-                      float* __restrict__ dparams) {
+                      const float* __restrict__ Z, const float* __restrict__ dL_dsignal, float* dX,
+                      float* __restrict__ dparams, float* __restrict__ dL_dmeans3D) {
   using FP = FusedParams<kL>;
   using TL = FusedTiles<kL>;
   extern __shared__ __align__(16) float sm[];
@@ -698,6 +707,10 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
           *reinterpret_cast<float4*>(dX + rr * kFeat + c0x) = make_float4(dx[i][0], dx[i][1], dx[i][2], dx[i][3]);
       }
     }
+    if (kFeatAdj) {   // one receiver (row = Gaussian): the feature adjoint of the tile here
+      __syncthreads();              // the tile's dL/dx rows are written
+      if (row_thread && row < rows) features_adjoint((int)row, P, 1, means3D, rx_pos, radii, dX, dL_dmeans3D);
+    }
   }
   __syncthreads();
   // this CTA's share -> global
@@ -720,9 +733,10 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
 template <int kL, int kAct>
 static cudaError_t launch_fused(bool fwd, int P, size_t rows, const float* means3D, const float* rx_pos,
                                 const float* params, const GeomView& geo, const SharedMlpLayout& L, float* work,
-                                const float* dL_dsignal, float* dparams, cudaStream_t s) {
+                                const float* dL_dsignal, float* dparams, float* dmeans, cudaStream_t s) {
   const size_t smem = (size_t)(fwd ? FusedFwdSmem<kL>::kTotal : FusedTiles<kL>::kTotal) * sizeof(float);
-  static bool attr_done[2][64] = {};
+  static bool attr_done[3][64] = {};   // forward, adjoint, adjoint with the feature adjoint
+  const int variant = fwd ? 0 : (dmeans ? 2 : 1);
   static int sm_count[64] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -732,13 +746,15 @@ static cudaError_t launch_fused(bool fwd, int P, size_t rows, const float* means
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     if (dev >= 0 && dev < 64) sm_count[dev] = sms;
   }
-  if (dev < 0 || dev >= 64 || !attr_done[fwd][dev]) {
+  if (dev < 0 || dev >= 64 || !attr_done[variant][dev]) {
     e = fwd ? cudaFuncSetAttribute(mlp64_forward_kernel<kL, kAct>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem)
-            : cudaFuncSetAttribute(mlp64_backward_kernel<kL, kAct>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem);
+            : (dmeans ? cudaFuncSetAttribute(mlp64_backward_kernel<kL, kAct, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                      : cudaFuncSetAttribute(mlp64_backward_kernel<kL, kAct, false>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (e != cudaSuccess) return e;
-    if (dev >= 0 && dev < 64) attr_done[fwd][dev] = true;
+    if (dev >= 0 && dev < 64) attr_done[variant][dev] = true;
   }
   const size_t ntiles = (rows + kFusedRows - 1) / kFusedRows;
   if (fwd) {
@@ -757,20 +773,28 @@ static cudaError_t launch_fused(bool fwd, int P, size_t rows, const float* means
     return cudaGetLastError();
   }
   const unsigned grid = (unsigned)(ntiles < (size_t)sms ? ntiles : (size_t)sms);
-  mlp64_backward_kernel<kL, kAct><<<grid, kAdjThreads, smem, s>>>(
-      P, rows, means3D, rx_pos, params, geo.radii, work + L.s, work + L.z[1], dL_dsignal, work + L.d0, dparams);
+  if (dmeans)
+    mlp64_backward_kernel<kL, kAct, true><<<grid, kAdjThreads, smem, s>>>(
+        P, rows, means3D, rx_pos, params, geo.radii, work + L.s, work + L.z[1], dL_dsignal, work + L.d0, dparams, dmeans);
+  else
+    mlp64_backward_kernel<kL, kAct, false><<<grid, kAdjThreads, smem, s>>>(
+        P, rows, means3D, rx_pos, params, geo.radii, work + L.s, work + L.z[1], dL_dsignal, work + L.d0, dparams,
+        nullptr);
   return cudaGetLastError();
 }
 
+// dmeans: dL/dmeans3D when the adjoint also runs the feature adjoint (one receiver), else nullptr
 static cudaError_t launch_fused_dispatch(bool fwd, int layers, int act, int P, size_t rows, const float* means3D,
                                          const float* rx_pos, const float* params, const GeomView& geo,
                                          const SharedMlpLayout& L, float* work, const float* dL_dsignal,
-                                         float* dparams, cudaStream_t s) {
+                                         float* dparams, float* dmeans, cudaStream_t s) {
   if (layers == 1)
-    return act == 1 ? launch_fused<1, 1>(fwd, P, rows, means3D, rx_pos, params, geo, L, work, dL_dsignal, dparams, s)
-                    : launch_fused<1, 2>(fwd, P, rows, means3D, rx_pos, params, geo, L, work, dL_dsignal, dparams, s);
-  return act == 1 ? launch_fused<2, 1>(fwd, P, rows, means3D, rx_pos, params, geo, L, work, dL_dsignal, dparams, s)
-                  : launch_fused<2, 2>(fwd, P, rows, means3D, rx_pos, params, geo, L, work, dL_dsignal, dparams, s);
+    return act == 1
+               ? launch_fused<1, 1>(fwd, P, rows, means3D, rx_pos, params, geo, L, work, dL_dsignal, dparams, dmeans, s)
+               : launch_fused<1, 2>(fwd, P, rows, means3D, rx_pos, params, geo, L, work, dL_dsignal, dparams, dmeans, s);
+  return act == 1
+             ? launch_fused<2, 1>(fwd, P, rows, means3D, rx_pos, params, geo, L, work, dL_dsignal, dparams, dmeans, s)
+             : launch_fused<2, 2>(fwd, P, rows, means3D, rx_pos, params, geo, L, work, dL_dsignal, dparams, dmeans, s);
 }
 
 // ---- layout of parameters and workspace ----------------------------------------
@@ -857,7 +881,7 @@ cudaError_t launch_shared_mlp_forward(int P, int R, int layers, int width, int a
   const SharedMlpLayout L = shared_mlp_layout(layers, width, out, rows);
   if (shared_mlp_fused(layers, width, out))
     return launch_fused_dispatch(true, layers, act, P, rows, means3D, rx_pos, params, geo, L, work, nullptr, nullptr,
-                                 s);
+                                 nullptr, s);
   mlp_features_kernel<<<dim3((P + 255) / 256, R), 256, 0, s>>>(P, means3D, rx_pos, geo.radii, work + L.x0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -886,9 +910,10 @@ cudaError_t launch_shared_mlp_backward(int P, int R, int layers, int width, int 
   cudaError_t e = cudaMemsetAsync(dL_dparams, 0, L.params * sizeof(float), s);
   if (e != cudaSuccess) return e;
   if (shared_mlp_fused(layers, width, out)) {
+    // one receiver: the adjoint finishes each tile's feature adjoint itself (row = Gaussian)
     e = launch_fused_dispatch(false, layers, act, P, rows, means3D, rx_pos, params, geo, L, work, dL_dsignal,
-                              dL_dparams, s);
-    if (e != cudaSuccess) return e;
+                              dL_dparams, R == 1 ? dL_dmeans3D : nullptr, s);
+    if (e != cudaSuccess || R == 1) return e;
     return launch_mlp_features_backward(P, R, means3D, rx_pos, geo.radii, work + L.d0, dL_dmeans3D, s);
   }
   float* dcur = work + L.d1;   // dZ of the current layer

@@ -55,10 +55,11 @@ def _scene(P, R, seed):
 
 
 # width 64 with one or two layers runs the fused kernels (R = 7 puts more than
-# one 128-row tile on some CTAs); the rest runs the tiled GEMM path
+# one 128-row tile on some CTAs; with R = 1 the adjoint also runs the feature
+# adjoint); the rest runs the tiled GEMM path
 @pytest.mark.parametrize("layers,width,act,R", [(2, 64, "relu", 1), (3, 128, "gelu", 3), (2, 64, "relu", 2),
                                                 (2, 64, "relu", 7), (1, 64, "gelu", 2), (2, 64, "gelu", 1),
-                                                (3, 64, "relu", 1)])
+                                                (3, 64, "relu", 1), (1, 64, "gelu", 1)])
 def test_shared_mlp_forward_and_backward_match_torch(layers, width, act, R):
     torch.backends.cuda.matmul.allow_tf32 = False
     P = 3001
