@@ -16,9 +16,11 @@ Adam; every launch one of this library's kernels) with inputs resident in
 HBM; per-step CUDA events on the compute stream, L2 flushed (256 MiB write)
 between steps outside the events.
 e2e: the same step through FusedTrainer.step with the receiver's target
-spectrum, view matrix and position copied from pinned host memory every
-step and the loss and rasterizer status read back to the host, inside the
-timed region.
+spectrum, view matrix and position copied from pinned host memory and the
+loss copied back to pinned host memory every step, inside the step's events;
+the host reads each step's loss and the rasterizer status while the next
+step runs (the last one after the loop), as a training loop that logs every
+loss does.
 cfg2_batched_clustered_autotuned: the clustered batched workload (50,000 Gaussians, 30% in five
 clusters, 64 receivers per step, shared 2x64 ReLU MLP, FP32): the tile shape
 picked by FusedTrainer.autotune_tile from {16x16, 8x32, 32x8} (graph replays
@@ -45,6 +47,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -280,17 +283,27 @@ def run_ours(args):
         j = i % POOL
         return trainer.step(views_d[j:j + 1], rxs_d[j:j + 1], targets_d[j:j + 1])
 
-    loss_h = torch.empty((), dtype=torch.float32).pin_memory()
+    loss_h = torch.empty(2, dtype=torch.float32).pin_memory()
+    loss_done = [torch.cuda.Event(), torch.cuda.Event()]
+    losses = []
 
     def host_step(i):
         # target spectrum, view matrix and receiver position copied from pinned
-        # host memory into the graph's inputs; loss and rasterizer status back
+        # host memory into the graph's inputs, the loss copied back to pinned
+        # memory, all on the stream inside the step's events; the host reads
+        # step i's loss and the rasterizer status while step i + 1 runs (a
+        # training loop that logs every loss), and the last one after the loop
         j = i % POOL
         loss = trainer.step(views_h[j:j + 1], rxs_h[j:j + 1], targets_h[j:j + 1])
-        loss_h.copy_(loss, non_blocking=True)
-        stream.synchronize()
+        loss_h[i & 1].copy_(loss, non_blocking=True)
+        loss_done[i & 1].record(stream)
+        if i > 0:
+            read_loss(i - 1)
+
+    def read_loss(i):
+        loss_done[i & 1].synchronize()
         trainer.plan.check()
-        return float(loss_h)
+        losses.append(float(loss_h[i & 1]))
 
     for i in range(args.warmup):
         dev_step(i)
@@ -301,9 +314,14 @@ def run_ours(args):
             timed(dev_step, max(1, args.steps // 4))
     trainer.plan.check()                      # the capacity held for every timed step
     value = args.steps * world / sec
-    for i in range(min(args.warmup, 3)):
+    n_warm = max(1, min(args.warmup, 3))
+    for i in range(n_warm):
         host_step(i)
+    read_loss(n_warm - 1)
+    losses.clear()
     e2e_sec = timed(host_step, args.steps)
+    read_loss(args.steps - 1)
+    assert len(losses) == args.steps and all(math.isfinite(v) for v in losses)
     e2e = args.steps * world / e2e_sec
     h2d = (90 * 360 + 16 + 3) * 4
     # per-kernel device times from eager runs of the same step (graph replays
