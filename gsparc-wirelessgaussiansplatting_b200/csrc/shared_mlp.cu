@@ -88,8 +88,9 @@ mlp_features_kernel(int P, const float* __restrict__ means3D, const float* __res
   for (int i = 0; i < kFeat; ++i) x[i] = f[i];
 }
 
-// dL/dmu of Gaussian g from dL/dx, summed over receivers in order.  dX is read
-// through L2 (it may have been written earlier in the same kernel).
+// dL/dmu of Gaussian g from dL/dx, summed over receivers in order.  dX rows are
+// read as float4s, through L2 only when kL2 (written earlier in the same kernel).
+template <bool kL2>
 __device__ __forceinline__ void features_adjoint(int g, int P, int R, const float* __restrict__ means3D,
                                                  const float* __restrict__ rx_pos, const int* __restrict__ radii,
                                                  const float* dX, float* __restrict__ dL_dmeans3D) {
@@ -102,9 +103,13 @@ __device__ __forceinline__ void features_adjoint(int g, int P, int R, const floa
   for (int r = 0; r < R; ++r) {
     const size_t row = (size_t)r * P + g;
     if (radii[row] <= 0) continue;
-    float dx[31];
+    float dx[kFeat];
+    const float4* src = reinterpret_cast<const float4*>(dX + row * kFeat);
 #pragma unroll
-    for (int i = 0; i < 31; ++i) dx[i] = __ldcg(dX + row * kFeat + i);
+    for (int q = 0; q < kFeat / 4; ++q) {
+      const float4 v = kL2 ? __ldcg(src + q) : src[q];
+      dx[4 * q] = v.x; dx[4 * q + 1] = v.y; dx[4 * q + 2] = v.z; dx[4 * q + 3] = v.w;
+    }
 #pragma unroll
     for (int i = 0; i < 27; ++i) sum_pe[i] += dx[i];
     const float v[3] = {m[0] - rx_pos[3 * r], m[1] - rx_pos[3 * r + 1], m[2] - rx_pos[3 * r + 2]};
@@ -138,7 +143,7 @@ mlp_features_backward_kernel(int P, int R, const float* __restrict__ means3D, co
                              const int* __restrict__ radii, const float* __restrict__ dX,
                              float* __restrict__ dL_dmeans3D) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g < P) features_adjoint(g, P, R, means3D, rx_pos, radii, dX, dL_dmeans3D);
+  if (g < P) features_adjoint<false>(g, P, R, means3D, rx_pos, radii, dX, dL_dmeans3D);
 }
 
 // ---- tiled SIMT GEMM ----------------------------------------------------------
@@ -709,7 +714,8 @@ mlp64_backward_kernel(int P, size_t rows, const float* __restrict__ means3D, con
     }
     if (kFeatAdj) {   // one receiver (row = Gaussian): the feature adjoint of the tile here
       __syncthreads();              // the tile's dL/dx rows are written
-      if (row_thread && row < rows) features_adjoint((int)row, P, 1, means3D, rx_pos, radii, dX, dL_dmeans3D);
+      if (row_thread && row < rows)
+        features_adjoint<true>((int)row, P, 1, means3D, rx_pos, radii, dX, dL_dmeans3D);
     }
   }
   __syncthreads();
