@@ -88,19 +88,15 @@ mlp_features_kernel(int P, const float* __restrict__ means3D, const float* __res
   for (int i = 0; i < kFeat; ++i) x[i] = f[i];
 }
 
-// dL/dmu of Gaussian g from dL/dx, summed over receivers in order.  dX rows are
+// dL/dmu from dL/dx.  The positional-encoding part does not depend on the
+// receiver, so dX[0..26] is summed over receivers first (sum_pe); the
+// direction and 1/d^2 parts are accumulated per receiver (acc).  dX rows are
 // read as float4s, through L2 only when kL2 (written earlier in the same kernel).
 template <bool kL2>
-__device__ __forceinline__ void features_adjoint(int g, int P, int R, const float* __restrict__ means3D,
+__device__ __forceinline__ void features_partial(int g, int P, int r_lo, int r_hi, const float (&m)[3],
                                                  const float* __restrict__ rx_pos, const int* __restrict__ radii,
-                                                 const float* dX, float* __restrict__ dL_dmeans3D) {
-  const float m[3] = {means3D[3 * g], means3D[3 * g + 1], means3D[3 * g + 2]};
-  float acc[3] = {0.0f, 0.0f, 0.0f};
-  // positional part does not depend on the receiver: sum dX over receivers first
-  float sum_pe[kFeat];
-#pragma unroll
-  for (int i = 0; i < 27; ++i) sum_pe[i] = 0.0f;
-  for (int r = 0; r < R; ++r) {
+                                                 const float* dX, float (&sum_pe)[27], float (&acc)[3]) {
+  for (int r = r_lo; r < r_hi; ++r) {
     const size_t row = (size_t)r * P + g;
     if (radii[row] <= 0) continue;
     float dx[kFeat];
@@ -123,6 +119,11 @@ __device__ __forceinline__ void features_adjoint(int g, int P, int R, const floa
 #pragma unroll
     for (int j = 0; j < 3; ++j) acc[j] += (dx[27 + j] - gu * u[j]) / d + ga * v[j];
   }
+}
+
+// the positional encoding's chain rule, added to dL/dmeans3D[g]
+__device__ __forceinline__ void features_finish(int g, const float (&m)[3], const float (&sum_pe)[27],
+                                                const float (&acc)[3], float* __restrict__ dL_dmeans3D) {
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     float gj = sum_pe[j];
@@ -137,13 +138,46 @@ __device__ __forceinline__ void features_adjoint(int g, int P, int R, const floa
   }
 }
 
-// thread per Gaussian
+// Gaussian g over all R receivers in order (one thread)
+template <bool kL2>
+__device__ __forceinline__ void features_adjoint(int g, int P, int R, const float* __restrict__ means3D,
+                                                 const float* __restrict__ rx_pos, const int* __restrict__ radii,
+                                                 const float* dX, float* __restrict__ dL_dmeans3D) {
+  const float m[3] = {means3D[3 * g], means3D[3 * g + 1], means3D[3 * g + 2]};
+  float sum_pe[27] = {}, acc[3] = {};
+  features_partial<kL2>(g, P, 0, R, m, rx_pos, radii, dX, sum_pe, acc);
+  features_finish(g, m, sum_pe, acc, dL_dmeans3D);
+}
+
+// Several receivers: four lanes per Gaussian, lane q taking receivers
+// [q R / 4, (q + 1) R / 4) in order; the four partial sums are combined as
+// (q0 + q1) + (q2 + q3) (a fixed order: deterministic).
+constexpr int kFeatLanes = 4;
 __global__ void __launch_bounds__(256)
 mlp_features_backward_kernel(int P, int R, const float* __restrict__ means3D, const float* __restrict__ rx_pos,
                              const int* __restrict__ radii, const float* __restrict__ dX,
                              float* __restrict__ dL_dmeans3D) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g < P) features_adjoint<false>(g, P, R, means3D, rx_pos, radii, dX, dL_dmeans3D);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = t / kFeatLanes, q = t % kFeatLanes;
+  const bool live = g < P;
+  float m[3] = {0.0f, 0.0f, 0.0f};
+  if (live) {
+    m[0] = means3D[3 * g];
+    m[1] = means3D[3 * g + 1];
+    m[2] = means3D[3 * g + 2];
+  }
+  float sum_pe[27] = {}, acc[3] = {};
+  if (live)
+    features_partial<false>(g, P, (int)((long long)q * R / kFeatLanes), (int)((long long)(q + 1) * R / kFeatLanes),
+                            m, rx_pos, radii, dX, sum_pe, acc);
+#pragma unroll
+  for (int o = 1; o < kFeatLanes; o <<= 1) {
+#pragma unroll
+    for (int i = 0; i < 27; ++i) sum_pe[i] += __shfl_down_sync(0xffffffffu, sum_pe[i], o, kFeatLanes);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) acc[j] += __shfl_down_sync(0xffffffffu, acc[j], o, kFeatLanes);
+  }
+  if (live && q == 0) features_finish(g, m, sum_pe, acc, dL_dmeans3D);
 }
 
 // ---- tiled SIMT GEMM ----------------------------------------------------------
@@ -869,7 +903,8 @@ SharedMlpLayout shared_mlp_layout_bf16(int layers, size_t rows, int out) {
 
 cudaError_t launch_mlp_features_backward(int P, int R, const float* means3D, const float* rx_pos, const int* radii,
                                          const float* dX, float* dL_dmeans3D, cudaStream_t s) {
-  mlp_features_backward_kernel<<<(P + 255) / 256, 256, 0, s>>>(P, R, means3D, rx_pos, radii, dX, dL_dmeans3D);
+  const unsigned blocks = (unsigned)(((long long)P * kFeatLanes + 255) / 256);
+  mlp_features_backward_kernel<<<blocks, 256, 0, s>>>(P, R, means3D, rx_pos, radii, dX, dL_dmeans3D);
   return cudaGetLastError();
 }
 
@@ -961,9 +996,7 @@ cudaError_t launch_shared_mlp_backward(int P, int R, int layers, int width, int 
     dnext = t;
   }
   // dcur now holds dL/dx of the features
-  mlp_features_backward_kernel<<<(P + 255) / 256, 256, 0, s>>>(P, R, means3D, rx_pos, geo.radii, dcur,
-                                                               dL_dmeans3D);
-  return cudaGetLastError();
+  return launch_mlp_features_backward(P, R, means3D, rx_pos, geo.radii, dcur, dL_dmeans3D, s);
 }
 
 }  // namespace gsparc
