@@ -289,7 +289,8 @@ cudaError_t launch_emission_backward(int P, int R, const float* means3D, const f
   if (P == 0) return cudaSuccess;
   const int warps_per_block = 8;
   int blocks = (P + warps_per_block - 1) / warps_per_block;
-  if (blocks > 148 * 16) blocks = 148 * 16;   // persistent-style grid: 16 CTAs per SM
+  const int cap = device_sm_count() * 16;   // persistent-style grid: 16 CTAs per SM
+  if (blocks > cap) blocks = cap;
   emission_backward_kernel<<<blocks, 32 * warps_per_block, 0, stream>>>(P, R, means3D, mlp, tx_pos, rx_pos, radii,
                                                                         dsig, dL_dmlp, dL_dmeans3D);
   return cudaGetLastError();

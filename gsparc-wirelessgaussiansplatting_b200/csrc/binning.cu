@@ -80,7 +80,7 @@ struct RadixShared {
 // bumps the counter and broadcasts the old value); one column scan over the
 // warps then gives each warp's offset per digit: a stable rank in the tile.
 __device__ __forceinline__ void radix_pass_body(RadixShared& sh, int P, int pass, bool ticketed, GeomView geo,
-                                                ImageHeader* __restrict__ hdr) {
+                                                ImageHeader* __restrict__ hdr, uint32_t spin_limit) {
   auto& s_run = sh.run;
   auto& s_off = sh.off;
   auto& s_wsum = sh.wsum;
@@ -182,7 +182,7 @@ __device__ __forceinline__ void radix_pass_body(RadixShared& sh, int P, int pass
         if (st == 2) finished = true;
       }
       j -= used;
-      if (stalled && ++spins > kLookbackSpins) {
+      if (stalled && ++spins > spin_limit) {
         atomic_or_error(hdr, kErrSortWait);
         break;
       }
@@ -232,23 +232,25 @@ __device__ __forceinline__ void capacity_check(ImageHeader* hdr, unsigned long l
 }
 
 __global__ void __launch_bounds__(kRadixThreads)
-radix_pass_kernel(int P, int pass, GeomView geo, ImageHeader* __restrict__ hdr, unsigned long long capacity) {
+radix_pass_kernel(int P, int pass, GeomView geo, ImageHeader* __restrict__ hdr, unsigned long long capacity,
+                  uint32_t spin_limit) {
   __shared__ RadixShared sh;
   if (pass == 0) capacity_check(hdr, capacity);
-  radix_pass_body(sh, P, pass, true, geo, hdr);
+  radix_pass_body(sh, P, pass, true, geo, hdr, spin_limit);
 }
 
 // All four passes in one cooperative launch (every CTA resident), with a
 // per-receiver barrier between passes: an arrival counter per (receiver,
 // barrier) in the sort state, spun on with a bound (kErrSortWait on give-up).
-__device__ __forceinline__ void receiver_barrier(uint32_t* counter, uint32_t expected, ImageHeader* hdr) {
+__device__ __forceinline__ void receiver_barrier(uint32_t* counter, uint32_t expected, ImageHeader* hdr,
+                                                 uint32_t spin_limit) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     atomicAdd(counter, 1u);
     uint32_t spins = 0;
     while (ld_volatile_u32(counter) < expected) {
-      if (++spins > kLookbackSpins) {
+      if (++spins > spin_limit) {
         atomic_or_error(hdr, kErrSortWait);
         break;
       }
@@ -259,14 +261,15 @@ __device__ __forceinline__ void receiver_barrier(uint32_t* counter, uint32_t exp
 }
 
 __global__ void __launch_bounds__(kRadixThreads)
-radix_sort_coop_kernel(int P, GeomView geo, ImageHeader* __restrict__ hdr, unsigned long long capacity) {
+radix_sort_coop_kernel(int P, GeomView geo, ImageHeader* __restrict__ hdr, unsigned long long capacity,
+                       uint32_t spin_limit) {
   __shared__ RadixShared sh;
   capacity_check(hdr, capacity);
   // barrier counters share the (unused) ticket words of passes 1..3
   uint32_t* bars = geo.sort_state + (size_t)gridDim.y * 1024 + (size_t)blockIdx.y * 4;
   for (int pass = 0; pass < 4; ++pass) {
-    radix_pass_body(sh, P, pass, false, geo, hdr);
-    if (pass < 3) receiver_barrier(bars + pass + 1, gridDim.x, hdr);
+    radix_pass_body(sh, P, pass, false, geo, hdr, spin_limit);
+    if (pass < 3) receiver_barrier(bars + pass + 1, gridDim.x, hdr, spin_limit);
   }
 }
 
@@ -441,14 +444,18 @@ cudaError_t launch_scatter(int P, int R, const TileGrid& grid, const GeomView& g
 
 // One cooperative launch when every CTA of the sort fits on the GPU at once
 // (the launch itself guarantees co-residency), else one launch per pass.
-cudaError_t launch_depth_sort(int P, int R, const GeomView& geo, ImageView img, unsigned long long capacity,
-                              cudaStream_t stream) {
-  if (P == 0 || R == 0) return cudaSuccess;
+namespace {
+// CTAs of the cooperative sort that fit on the current device at once (-1:
+// no cooperative launch), looked up once per device.
+cudaError_t coop_sort_capacity(int* dev_out, long long* cap) {
   static long long coop_capacity[64] = {0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (dev >= 0 && dev < 64 && coop_capacity[dev] == 0) {
+  *dev_out = dev;
+  *cap = -1;
+  if (dev < 0 || dev >= 64) return cudaSuccess;
+  if (coop_capacity[dev] == 0) {
     int per_sm = 0, sms = 0, coop = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, radix_sort_coop_kernel, kRadixThreads, 0)) !=
         cudaSuccess)
@@ -457,9 +464,31 @@ cudaError_t launch_depth_sort(int P, int R, const GeomView& geo, ImageView img, 
     if ((e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev)) != cudaSuccess) return e;
     coop_capacity[dev] = coop ? (long long)per_sm * sms : -1;
   }
+  *cap = coop_capacity[dev];
+  return cudaSuccess;
+}
+}  // namespace
+
+int depth_sort_launches(int P, int R) {
+  if (P <= 0 || R <= 0) return 0;
+  int dev = 0;
+  long long cap = -1;
+  if (coop_sort_capacity(&dev, &cap) != cudaSuccess) return -1;
+  const long long ctas = (long long)sort_tiles((size_t)P) * R;
+  return (cap > 0 && ctas <= cap) ? 1 : 4;
+}
+
+cudaError_t launch_depth_sort(int P, int R, const GeomView& geo, ImageView img, unsigned long long capacity,
+                              cudaStream_t stream) {
+  if (P == 0 || R == 0) return cudaSuccess;
+  int dev = 0;
+  long long cap = -1;
+  cudaError_t e = coop_sort_capacity(&dev, &cap);
+  if (e != cudaSuccess) return e;
   const dim3 grid((unsigned)sort_tiles((size_t)P), R);
   const long long ctas = (long long)grid.x * grid.y;
-  if (dev >= 0 && dev < 64 && coop_capacity[dev] > 0 && ctas <= coop_capacity[dev]) {
+  const uint32_t spin_limit = wait_polls(kLookbackSpins);
+  if (cap > 0 && ctas <= cap) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = dim3(kRadixThreads);
@@ -471,10 +500,10 @@ cudaError_t launch_depth_sort(int P, int R, const GeomView& geo, ImageView img, 
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     ImageHeader* hdr = img.hdr;
-    return cudaLaunchKernelEx(&cfg, radix_sort_coop_kernel, P, geo, hdr, capacity);
+    return cudaLaunchKernelEx(&cfg, radix_sort_coop_kernel, P, geo, hdr, capacity, spin_limit);
   }
   for (int pass = 0; pass < 4; ++pass) {
-    radix_pass_kernel<<<grid, kRadixThreads, 0, stream>>>(P, pass, geo, img.hdr, capacity);
+    radix_pass_kernel<<<grid, kRadixThreads, 0, stream>>>(P, pass, geo, img.hdr, capacity, spin_limit);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

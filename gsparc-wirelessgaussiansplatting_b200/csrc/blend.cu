@@ -469,7 +469,7 @@ blend_backward_kernel(int P, int H, int W, TileGrid grid, int RT, int span, unsi
 
 // 64-thread CTAs (four per tile) while the launch has fewer tiles than two
 // per SM; full-tile CTAs otherwise.
-static bool use_split_tiles(int R, const TileGrid& grid) { return (long long)R * grid.T < 2 * 148; }
+static bool use_split_tiles(int R, const TileGrid& grid) { return (long long)R * grid.T < 2LL * device_sm_count(); }
 
 cudaError_t launch_blend_forward(int P, int R, int H, int W, const TileGrid& grid, const GeomView& geo,
                                  const ImageView& img, const BinningView& bin, float* out_real,
@@ -535,7 +535,7 @@ cudaError_t launch_blend_backward(int P, int R, int H, int W, const TileGrid& gr
   const long long items = capacity / kBwdChunk + RT;
   if (items > 0x7fffffffLL) return cudaErrorInvalidValue;
   int span = 1;   // the largest power of two up to 32 that leaves about 64 items per SM
-  while (span < 32 && items >= 2LL * span * 148 * 64) span *= 2;
+  while (span < 32 && items >= 2LL * span * device_sm_count() * 64) span *= 2;
   long long grid_items = items;
   if (span > 1) {
     blend_item_scan_kernel<<<1, 1024, 0, stream>>>(RT, span, img.chunk_base, img.item_base);

@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -47,7 +48,7 @@ bool valid_tile(int th, int tw) {
 enum KernelId {
   KID_PREPROCESS, KID_CHECK, KID_SCATTER, KID_DEPTH_SORT, KID_PLACE, KID_BLEND_FWD, KID_BLEND_BWD,
   KID_GEOM_BWD, KID_MLP_BWD, KID_SSIM_FWD, KID_SSIM_BWD, KID_MARK_VISIBLE, KID_ADAM, KID_LOSS, KID_ACTIVATE, KID_SHARED_MLP, KID_SHARED_MLP_BWD,
-  KID_BLEND_MC_FWD, KID_BLEND_MC_BWD, KID_EVAL, KID_DENSIFY,
+  KID_BLEND_MC_FWD, KID_BLEND_MC_BWD, KID_EVAL, KID_DENSIFY, KID_MLP_FEAT_BWD,
   KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
@@ -56,7 +57,7 @@ const char* const kKernelNames[KID_COUNT] = {
     "emission_backward_kernel", "ssim_forward_kernel", "ssim_backward_kernel", "mark_visible_kernel",
     "gaussian_adam_kernels", "splat_loss_kernels", "gaussian_activate_kernel", "shared_mlp_forward_kernels",
     "shared_mlp_backward_kernels", "blend_channels_forward_kernel", "blend_channels_backward_kernel",
-    "eval_metrics_kernel", "densify_kernels"};
+    "eval_metrics_kernel", "densify_kernels", "mlp_features_backward_kernel"};
 
 struct PendingTiming {
   int id;
@@ -102,7 +103,15 @@ struct Timed {
 
 }  // namespace
 
+namespace {
+std::atomic<long long> g_wait_limit{-1};   // < 0: every wait uses its own default bound
+}  // namespace
+
 namespace gsparc {
+uint32_t wait_polls(uint32_t dflt) {
+  const long long lim = g_wait_limit.load(std::memory_order_relaxed);
+  return (lim < 0 || lim >= (long long)dflt) ? dflt : (uint32_t)lim;
+}
 // error reporting shared with entry points defined in other files
 int report_invalid(const char* what) { return invalid(what); }
 int report_cuda(cudaError_t e, const char* where) { return cuda_fail(e, where); }
@@ -479,12 +488,20 @@ int gsparc_shared_mlp_backward(int P, int R, int layers, int width, int act, int
     return invalid("null pointer");
   GeomView geo;
   carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
-  Timed t(KID_SHARED_MLP_BWD, s);
   if (precision == GSPARC_MLP_BF16) {
-    GS_CHECK(launch_shared_mlp_bf16(false, P, R, layers, act, out, means3D, rx_pos, params, geo, workspace, dL_dsignal,
-                                    dL_dparams, dL_dmeans3D, (ImageHeader*)image_state, s),
-             "shared mlp backward (bf16)");
+    {   // the tensor-core adjoint and the feature adjoint, timed apart
+      Timed t(KID_SHARED_MLP_BWD, s);
+      GS_CHECK(launch_shared_mlp_bf16(false, P, R, layers, act, out, means3D, rx_pos, params, geo, workspace,
+                                      dL_dsignal, dL_dparams, nullptr, (ImageHeader*)image_state, s),
+               "shared mlp backward (bf16)");
+    }
+    Timed t(KID_MLP_FEAT_BWD, s);
+    GS_CHECK(launch_mlp_features_backward(P, R, means3D, rx_pos, geo.radii,
+                                          workspace + shared_mlp_layout_bf16(layers, (size_t)P * R, out).d0,
+                                          dL_dmeans3D, s),
+             "shared mlp feature adjoint (bf16)");
   } else {
+    Timed t(KID_SHARED_MLP_BWD, s);
     GS_CHECK(launch_shared_mlp_backward(P, R, layers, width, act, out, means3D, rx_pos, params, geo, workspace,
                                         dL_dsignal, dL_dparams, dL_dmeans3D, s),
              "shared mlp backward");
@@ -717,6 +734,13 @@ int gsparc_timing_enable(int on) {
 }
 
 int gsparc_timing_kernel_count(void) { return KID_COUNT; }
+
+int gsparc_depth_sort_launches(int P, int R) { return depth_sort_launches(P, R); }
+
+int gsparc_set_wait_limit(long long polls) {
+  g_wait_limit.store(polls < 0 ? -1 : polls, std::memory_order_relaxed);
+  return GSPARC_OK;
+}
 
 const char* gsparc_timing_kernel_name(int id) { return (id >= 0 && id < KID_COUNT) ? kKernelNames[id] : ""; }
 

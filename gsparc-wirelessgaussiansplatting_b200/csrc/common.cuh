@@ -30,6 +30,20 @@ constexpr int kMlpHidden = 32;
 constexpr int kMlpOut = 2;               // (real, imag)
 constexpr int kMlpFloats = kMlpIn * kMlpHidden + kMlpHidden + kMlpOut * kMlpHidden + kMlpOut;
 
+// Streaming multiprocessors of the current device (148 on a B200), looked up
+// once per device; grid-size heuristics scale with it.
+inline int device_sm_count() {
+  static int cache[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cache[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return 148;
+    cache[dev] = n;
+  }
+  return cache[dev];
+}
+
 // error word bits (image state header)
 constexpr uint32_t kErrCapacity = 1u << 0;   // K exceeded the binning capacity
 constexpr uint32_t kErrSegment = 1u << 1;    // a tile segment exceeded the sort limit

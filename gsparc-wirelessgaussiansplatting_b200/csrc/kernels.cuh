@@ -7,6 +7,10 @@ namespace gsparc {
 
 // Record the detail text of a failed call and return its status (capi.cu).
 int report_invalid(const char* what);
+// Poll bound of the library's device-side waits: `dflt` unless the host set a
+// limit with gsparc_set_wait_limit (the smaller of the two; 0 = give up at the
+// first wait that is not already satisfied).
+uint32_t wait_polls(uint32_t dflt);
 int report_cuda(cudaError_t e, const char* where);
 
 // Preprocess, tile counts and (last CTA) the segment scan: ranges, cursors,
@@ -31,6 +35,7 @@ constexpr int kMaxBinningP = 1 << 20;
 
 // Depth order of every receiver's Gaussians; also records the binning
 // capacity in the header and flags K > capacity.
+int depth_sort_launches(int P, int R);
 cudaError_t launch_depth_sort(int P, int R, const GeomView& geo, ImageView img, unsigned long long capacity,
                               cudaStream_t stream);
 

@@ -234,7 +234,7 @@ cudaError_t launch_gaussian_adam(int P, long long mlp_floats, int conf_floats, f
   const size_t n = conf_floats > 0 ? (L.conf - L.mlp) + (size_t)conf_floats : n_mlp;
   const int nb_g = (P + 255) / 256;
   int nb_m = (int)((n / 4 + 255) / 256);
-  if (nb_m > 148 * 8) nb_m = 148 * 8;
+  if (nb_m > device_sm_count() * 8) nb_m = device_sm_count() * 8;
   if (nb_m < 1) nb_m = 1;
   train_adam_kernel<<<nb_g + nb_m, 256, 0, stream>>>(P, L, nb_g, n, n_mlp, params, grads, m, v, step, lr6, beta1,
                                                      beta2, eps, lo3, hi3, act_scales, act_rots, act_opac);

@@ -307,7 +307,7 @@ cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, 
   // (latency), up to 16 when it fills many waves, so that each CTA's
   // histogram initialisation and flush serve up to 1,024 Gaussians
   int per_cta = 1;
-  while (per_cta < 16 && (long long)P * R >= 2LL * per_cta * 148 * kPreThreads * 16) per_cta *= 2;
+  while (per_cta < 16 && (long long)P * R >= 2LL * per_cta * device_sm_count() * kPreThreads * 16) per_cta *= 2;
   dim3 block(kPreThreads), gridd((P + kPreThreads * per_cta - 1) / (kPreThreads * per_cta), R);
   if (grid.T <= kMaxSharedHistTiles) {
     const size_t smem = kMlpSmemBytes + (size_t)grid.T * sizeof(uint32_t);

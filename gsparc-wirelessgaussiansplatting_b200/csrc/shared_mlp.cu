@@ -971,7 +971,7 @@ cudaError_t launch_shared_mlp_backward(int P, int R, int layers, int width, int 
     // tile into dW with one atomic per element; chunks stay >= 128 rows.
     {
       const unsigned gxy = (unsigned)(((o + kBM - 1) / kBM) * ((in + kBN - 1) / kBN));
-      const long long want_z = std::max<long long>(1, (4 * 148) / gxy);
+      const long long want_z = std::max<long long>(1, (4LL * device_sm_count()) / gxy);
       long long kchunk = (rows + want_z - 1) / want_z;
       kchunk = std::max<long long>(128, (kchunk + kBK - 1) / kBK * kBK);
       const unsigned zsplit = (unsigned)((rows + kchunk - 1) / kchunk);

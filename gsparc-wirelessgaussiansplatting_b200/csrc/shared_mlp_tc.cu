@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(128 * kFwdGroups, 1)
 mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                         const float* __restrict__ rx_pos, const float* __restrict__ params,
                         const int* __restrict__ radii, __nv_bfloat16* __restrict__ zb, float* __restrict__ S,
-                        float2* __restrict__ signal, ImageHeader* __restrict__ hdr) {
+                        float2* __restrict__ signal, ImageHeader* __restrict__ hdr, uint32_t polls) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar[kFwdGroups];
   __shared__ uint32_t tbase;
@@ -306,7 +306,7 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                        tc::smem_desc(b0 + kk * 2 * kLbo, kLbo, sbo), idesc, kk > 0 ? 1u : 0u);
         tc::commit(&mbar[grp]);
       }
-      const bool got = tc::mbar_wait(&mbar[grp], phase, kPolls);
+      const bool got = tc::mbar_wait(&mbar[grp], phase, polls);
       phase ^= 1u;
       tc::fence_after_sync();
       if (!tc::named_all(bar_id, 128, got)) {
@@ -368,7 +368,7 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                        tc::smem_desc(b0 + kk * 2 * kLbo, kLbo, kSboH), idesc, kk > 0 ? 1u : 0u);
         tc::commit(&mbar[grp]);
       }
-      const bool got = tc::mbar_wait(&mbar[grp], phase, kPolls);
+      const bool got = tc::mbar_wait(&mbar[grp], phase, polls);
       phase ^= 1u;
       tc::fence_after_sync();
       if (!tc::named_all(bar_id, 128, got)) {
@@ -389,7 +389,12 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
       }
     }
   }
-  if (!ok && t == 0 && hdr) atomic_or_error(hdr, kErrMlpWait);
+  if (!ok && t == 0) {
+    if (hdr) atomic_or_error(hdr, kErrMlpWait);
+    // drain: the MMAs this group's leader committed last (the phase the group
+    // gave up on) complete before the tensor memory is freed
+    tc::mbar_wait(&mbar[grp], phase ^ 1u, kPolls);
+  }
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tbase, kFwdGroups * kH);
@@ -414,11 +419,13 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                          const float* __restrict__ rx_pos, const float* __restrict__ params,
                          const int* __restrict__ radii, const __nv_bfloat16* __restrict__ zb,
                          const float* __restrict__ S, const float* __restrict__ dL_dsignal,
-                         float* __restrict__ dX0, float* __restrict__ dparams, ImageHeader* __restrict__ hdr) {
+                         float* __restrict__ dX0, float* __restrict__ dparams, ImageHeader* __restrict__ hdr,
+                         uint32_t polls) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar_ready[kBwdGroups];
   __shared__ __align__(8) uint64_t bar_done[kBwdGroups];
   __shared__ __align__(8) uint64_t bar_free;
+  __shared__ __align__(8) uint64_t bar_drain;
   __shared__ uint32_t tbase;
   __shared__ int s_fail;
   // one output: dw_out[128], db_out; kOut outputs: db_out[kOut], db_0[128]
@@ -487,6 +494,7 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
       tc::mbar_init(&bar_done[q], 1);
     }
     tc::mbar_init(&bar_free, 128);
+    tc::mbar_init(&bar_drain, 1);
     s_fail = 0;
   }
   if (warp == 0) tc::tmem_alloc(&tbase, 512);
@@ -526,7 +534,7 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
           const int in = l == 0 ? kFin : kH;
           for (int q = 0; q < kBwdGroups; ++q) {
             if (base + q >= ntiles) break;
-            if (!tc::mbar_wait(&bar_ready[q], ph_ready[q], kPolls)) {
+            if (!tc::mbar_wait(&bar_ready[q], ph_ready[q], polls)) {
               ok = false;
               break;
             }
@@ -556,7 +564,7 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
             }
             // dA = dZ_l W_l (or dO W_out) into the scratch, once its previous reader has drained it
             if (n_da > 0) {
-              if (!tc::mbar_wait(&bar_free, (n_da - 1) & 1u, kPolls)) {
+              if (!tc::mbar_wait(&bar_free, (n_da - 1) & 1u, polls)) {
                 ok = false;
                 break;
               }
@@ -711,7 +719,7 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         // hand dZ_l (or dO) and A_{l-1} to the MMA warp
         tc::fence_async_smem();
         tc::mbar_arrive(&bar_ready[grp]);
-        const bool got = tc::mbar_wait(&bar_done[grp], ph_done, kPolls);
+        const bool got = tc::mbar_wait(&bar_done[grp], ph_done, polls);
         ph_done ^= 1u;
         tc::fence_after_sync();
         if (!tc::named_all(bar_id, 128, got)) {
@@ -803,6 +811,12 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
     }
   }
   if (s_fail && tid == 0 && hdr) atomic_or_error(hdr, kErrMlpWait);
+  if (s_fail && grp == kBwdGroups && lane == 0) {
+    // drain: every MMA the issuing thread started completes before the
+    // tensor memory is freed
+    tc::commit(&bar_drain);
+    tc::mbar_wait(&bar_drain, 0, kPolls);
+  }
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tmem, 512);
@@ -854,11 +868,11 @@ static cudaError_t launch_bf16_layers(bool fwd, int P, size_t rows, const float*
   if (fwd)
     mlp_bf16_forward_kernel<L, A, O><<<grid, 128 * kFwdGroups, smem, s>>>(P, rows, means3D, rx_pos, params,
                                                                           geo.radii, zb, work + Lt.s, geo.signal,
-                                                                          hdr);
+                                                                          hdr, wait_polls(kPolls));
   else
     mlp_bf16_backward_kernel<L, A, O><<<grid, kBwdThreads, smem, s>>>(P, rows, means3D, rx_pos, params, geo.radii,
                                                                       zb, work + Lt.s, dL_dsignal, work + Lt.d0,
-                                                                      dparams, hdr);
+                                                                      dparams, hdr, wait_polls(kPolls));
   return cudaGetLastError();
 }
 
@@ -896,7 +910,7 @@ cudaError_t launch_shared_mlp_bf16(bool fwd, int P, int R, int layers, int act, 
     case 3: e = launch_bf16_act<3>(fwd, P, rows, act, out, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
     default: return cudaErrorInvalidValue;
   }
-  if (e != cudaSuccess || fwd) return e;
+  if (e != cudaSuccess || fwd || dL_dmeans3D == nullptr) return e;
   return launch_mlp_features_backward(P, R, means3D, rx_pos, geo.radii, work + Lt.d0, dL_dmeans3D, s);
 }
 

@@ -19,6 +19,7 @@
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (with that device current) and caches it; make that
 //    first call before any stream capture.
+#include <initializer_list>
 #include <mutex>
 
 #include "common.cuh"
@@ -27,6 +28,8 @@
 namespace {
 
 constexpr size_t kStaticSsimMaxPixels = size_t(1) << 20;
+static_assert(kStaticSsimMaxPixels == GSPARC_SSIM_STATIC_MAX_PIXELS,
+              "the header's GSPARC_SSIM_STATIC_MAX_PIXELS must equal the scratch array's pixel limit");
 
 // file-scope device scratch: dm/dmu1 | dm/dsigma1^2 | dm/dsigma12
 static __device__ __align__(256) float g_ssim_static_scratch[3 * kStaticSsimMaxPixels];
@@ -59,10 +62,15 @@ extern "C" int gsparc_ssim_static_scratch(int B, int CH, int H, int W, float C1,
                                           float* dL_dimg1, void* stream) {
   using namespace gsparc;
   if (B < 0 || CH < 0 || H < 0 || W < 0) return report_invalid("sizes");
-  const size_t n = (size_t)B * CH * H * W;
-  if (n == 0) return GSPARC_OK;
-  if (n > kStaticSsimMaxPixels)
-    return report_invalid("B*CH*H*W exceeds the 1048576 pixels of gsparc_ssim_static_scratch's static scratch");
+  if (B == 0 || CH == 0 || H == 0 || W == 0) return GSPARC_OK;
+  // the running product is checked after every factor, so it never exceeds
+  // 2^20 * 2^31 and cannot wrap
+  size_t n = 1;
+  for (int f : {B, CH, H, W}) {
+    n *= (size_t)f;
+    if (n > kStaticSsimMaxPixels)
+      return report_invalid("B*CH*H*W exceeds the 1048576 pixels of gsparc_ssim_static_scratch's static scratch");
+  }
   if (!img1 || !img2 || !dL_dmap || !ssim_map || !dL_dimg1) return report_invalid("null pointer");
   float* scratch = nullptr;
   cudaError_t e = static_scratch(&scratch);

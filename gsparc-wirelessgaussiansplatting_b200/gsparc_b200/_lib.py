@@ -88,6 +88,8 @@ _SIGS = {
     "gsparc_timing_kernel_count": (_c_int, []),
     "gsparc_timing_kernel_name": (ctypes.c_char_p, [_c_int]),
     "gsparc_timing_read": (_c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_c_ll), _c_int, _c_int]),
+    "gsparc_depth_sort_launches": (_c_int, [_c_int, _c_int]),
+    "gsparc_set_wait_limit": (_c_int, [_c_ll]),
 }
 
 _lib = None

@@ -453,6 +453,27 @@ GSPARC_API const char* gsparc_timing_kernel_name(int id);
  * n entries, either may be NULL).  reset != 0 clears the totals. */
 GSPARC_API int gsparc_timing_read(double* total_ms, long long* launches, int n, int reset);
 
+/* Kernel launches one depth sort of P Gaussians for R receivers makes on the
+ * current device: 1 when all its CTAs fit at once (one cooperative launch),
+ * else 4 (one per 8-bit pass); 0 for an empty sort, -1 on a CUDA error.  For
+ * counting launches (the timing above counts calls). */
+GSPARC_API int gsparc_depth_sort_launches(int P, int R);
+
+/* ---- bounded device waits (failure detection; no counterpart in the
+ * reference, which has no inter-CTA waits) ------------------------------- */
+
+/* Every wait of one CTA on another CTA or on the tensor cores inside this
+ * library is bounded: the depth sort's look-back and per-receiver barrier,
+ * and the tensor-core MLP kernels' mbarrier waits.  A wait that runs out sets
+ * kErrSortWait (bit 3) or kErrMlpWait (bit 4) in the image state's error word
+ * (gsparc_read_status), the kernel drains its own tensor-core work in flight,
+ * frees its tensor memory and returns; later stages skip their work.
+ * polls >= 0 caps every such wait at `polls` polls (0: give up at the first
+ * wait that is not already satisfied) for the launches that follow; polls < 0
+ * restores each wait's default bound.  Process-wide; for tests of the give-up
+ * path. */
+GSPARC_API int gsparc_set_wait_limit(long long polls);
+
 #ifdef __cplusplus
 }
 #endif

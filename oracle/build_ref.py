@@ -1,8 +1,8 @@
 """Build recipe for the reference extensions, compiled from their own sources
 as checkers (TEST INFRASTRUCTURE ONLY).
 
-Compiles, from the sources under /root/reference (read in place, never
-copied), with this repository's recipe rather than the reference's setup.py:
+Compiles, from the sources of the reference checkout (GSPARC_REFERENCE_ROOT,
+default /root/reference; read in place, never copied), with this repository's recipe rather than the reference's setup.py:
   * cuda_kernel_rasterize/{rasterize_points.cu, ext.cpp,
     cuda_wireless_rasterizer/{rasterizer_impl,forward,backward}.cu}
     -> oracle/_ref/raster/gsparc_ref_rasterizer*.so
@@ -14,7 +14,7 @@ oracle/ref_build_prelude.h is force-included to turn glibc's _Float32
 constants into plain float literals (nvcc rejects the former in device
 code).  Outputs go to oracle/_ref/ only (git-ignored; travels to the GPU box).
 
-Run:  python oracle/build_ref.py     (needs /root/reference; no GPU needed)
+Run:  python oracle/build_ref.py     (needs the reference checkout; no GPU needed)
 Load: oracle.build_ref.load_ref()    (on a GPU box, from the prebuilt .so)
 """
 from __future__ import annotations
@@ -25,7 +25,8 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = "/root/reference"
+# where the reference checkout lives (read only, never copied)
+REF_ROOT = os.environ.get("GSPARC_REFERENCE_ROOT", "/root/reference")
 OUT = os.path.join(HERE, "_ref")
 ARCH = ["-gencode=arch=compute_100a,code=sm_100a"]
 
@@ -67,6 +68,12 @@ def _load_so(name, sub):
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     return mod
+
+
+def reference_present() -> bool:
+    """Whether the reference checkout's sources are here (only in the build container)."""
+    raster, ssim = _sources()
+    return all(os.path.exists(p) for p in raster + ssim)
 
 
 def load_ref():

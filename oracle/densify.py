@@ -57,9 +57,12 @@ KEYS = ("centre", "log_scale", "rotation", "opacity", "mlp")
 
 
 def densify_and_prune(state, m1, m2, accum, denom, max_grad, min_opacity, extent, max_screen_size=None,
-                      scene_min=None, scene_max=None, percent_dense=0.01, seed=0):
+                      scene_min=None, scene_max=None, percent_dense=0.01, seed=0, split_samples=None):
     """state / m1 / m2: dicts of per-Gaussian arrays (KEYS; "mlp" [P,194] or
-    absent); returns the new (state, m1, m2) with float64 values."""
+    absent); returns the new (state, m1, m2) with float64 values.
+    ``split_samples`` [2n, 3], if given, replaces the split's offsets
+    stds * z (the draws of torch.normal(0, stds) at gaussian.py:471, in its
+    row order: copy-major, then selected Gaussian)."""
     keys = [k for k in KEYS if k in state]
     st = {k: np.asarray(state[k], dtype=np.float64).copy() for k in keys}
     a1 = {k: np.asarray(m1[k], dtype=np.float64).copy() for k in keys}
@@ -91,10 +94,16 @@ def densify_and_prune(state, m1, m2, accum, denom, max_grad, min_opacity, extent
     sel = (padded >= max_grad) & (scaling().max(axis=1) > percent_dense * extent)
     idx = np.nonzero(sel)[0]
     s = scaling()[idx]
-    z = np.array([[[normal(seed, int(g), k, d) for d in range(3)] for g in idx] for k in range(2)]).reshape(-1, 3)
     stds = np.concatenate([s, s])
+    if split_samples is None:
+        z = np.array([[[normal(seed, int(g), k, d) for d in range(3)] for g in idx]
+                      for k in range(2)]).reshape(-1, 3)
+        offs = stds * z
+    else:
+        offs = np.asarray(split_samples, dtype=np.float64).reshape(-1, 3)
+        assert offs.shape[0] == 2 * len(idx), (offs.shape, len(idx))
     rots = np.concatenate([build_rotation(st["rotation"][idx])] * 2)
-    new = {"centre": np.einsum("nij,nj->ni", rots, stds * z) + np.concatenate([st["centre"][idx]] * 2),
+    new = {"centre": np.einsum("nij,nj->ni", rots, offs) + np.concatenate([st["centre"][idx]] * 2),
            "log_scale": np.log(stds / 1.2)}
     for k in keys:
         if k not in new:

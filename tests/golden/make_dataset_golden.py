@@ -5,7 +5,7 @@ reference checkout on a few receiver positions and gateway orientations and
 saves the results to dataset_views_golden.npz.  Run from the repository
 root in a container with the reference checked out:
 
-    python tests/golden/make_dataset_golden.py /root/reference
+    python tests/golden/make_dataset_golden.py [REFERENCE_ROOT]
 
 preprocess_data imports imageio (for the PNG spectra of another dataset
 type) at module level; the method used here does not touch it, so an empty
@@ -49,4 +49,6 @@ def main(ref_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from oracle.build_ref import REF_ROOT
+    main(sys.argv[1] if len(sys.argv) > 1 else REF_ROOT)

@@ -3,7 +3,8 @@ conv2d SSIM (utils.py:81-124 -- the function fused-ssim/tests/test.py:24-54
 checks the fused kernel against) and differentiating it with torch autograd
 on the CPU.
 
-Run in a container that has the reference checked out at /root/reference:
+Run in a container that has the reference checked out (GSPARC_REFERENCE_ROOT,
+default as in oracle/build_ref.py):
     python tests/golden/make_golden.py
 The reference's utils.py imports ``plyfile`` (for an unrelated PLY reader);
 that package is not installed here, so an empty stand-in module is put in
@@ -19,7 +20,8 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference"
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.build_ref import REF_ROOT as REF  # noqa: E402
 
 # (name, shape, kind, seed)
 CASES = [

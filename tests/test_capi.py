@@ -149,3 +149,15 @@ def test_adam_step_rejects_partial_activation_outputs():
     st = L.gsparc_gaussian_adam_step(10, 1940, 161, d, d, d, d, d, d, 0.9, 0.999, 1e-15, d, d, d, None, None, None)
     assert st == 1
     assert b"all three" in L.gsparc_last_error_detail()
+
+
+def test_static_ssim_rejects_sizes_whose_product_wraps():
+    """B = CH = H = W = 65536 multiplies to 2^64, i.e. 0 in 64 bits; the
+    allocation-free SSIM entry point must reject it (each factor is checked
+    against the limit as the product grows) rather than report success."""
+    L = _lib.lib()
+    d = ctypes.c_void_p(16)     # never dereferenced: the size check fails first
+    for dims in ((65536, 65536, 65536, 65536), (1 << 20, 1 << 20, 1 << 20, 16), (1, 1, 1 << 20, 2)):
+        assert L.gsparc_ssim_static_scratch(*dims, 1e-4, 9e-4, d, d, d, d, d, None) == 1, dims
+        assert b"1048576" in L.gsparc_last_error_detail()
+    assert L.gsparc_ssim_static_scratch(0, 65536, 65536, 65536, 1e-4, 9e-4, d, d, d, d, d, None) == 0

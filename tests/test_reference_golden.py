@@ -203,3 +203,80 @@ def test_gpu_fused_ssim_vs_reference():
     np.testing.assert_allclose(m.cpu().numpy(), z["ssim/map"], rtol=0, atol=1e-5)
     for got, key in ((d1, "ssim/dm_dmu1"), (d2, "ssim/dm_dsigma1_sq"), (d3, "ssim/dm_dsigma12")):
         np.testing.assert_allclose(got.cpu().numpy(), z[key], rtol=0, atol=1e-5 * np.abs(z[key]).max())
+
+
+# ------------------------------------------------------ bench-size cases (GPU)
+
+FIX_LARGE = os.path.join(HERE, "golden", "raster_ref_golden_large.npz")
+
+
+def _load_large(name):
+    z = np.load(FIX_LARGE)
+    return {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith(name + "/")}
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(FIX_LARGE), reason="bench-size reference fixture not recorded yet")
+@pytest.mark.parametrize("name", ["cfg1", "cfg2r"])
+def test_gpu_bench_size_bit_exact_and_gradients_vs_reference(name):
+    """The 20,000-Gaussian training scene and one receiver of the 50,000-
+    Gaussian clustered scene against the reference extension: sorted keys,
+    point list, tile ranges, radii, preprocess outputs, contributor counts,
+    final T and spectra bit for bit (SHA-256 of each array, recorded by
+    make_ref_golden.py --large); the reference-mode gradients within 1e-4
+    relative 2-norm, the difference's norm estimated by the stored count-
+    sketches (a linear map; its norm estimate is good to a few per cent)."""
+    import torch
+    import wireless_rasterizer as wr
+    from gsparc_b200 import raster
+    from tests._helpers import reference_keys
+    m = _mod()
+    c = [c for c in m.LARGE_CASES if c[0] == name][0]
+    x = m.case_inputs(c[1], c[2], c[3], c[4])
+    g = _load_large(name)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    args = (t(x["means"]), t(x["mlp"]), t(x["opac"]), t(x["scales"]), t(x["rots"]), H, W, 1.0, t(x["view"]),
+            torch.eye(4, device="cuda"), t(x["tx"]), t(x["rx"]))
+    K, o_r, o_i, radii, gb, bb, ib = wr.rasterize_gaussians(*args)
+    P = x["means"].shape[0]
+    assert K == int(g["num_rendered"])
+    np.testing.assert_array_equal(radii.cpu().numpy(), g["radii"])
+    st = raster.ForwardState(P, 1, H, W, (16, 16), K, K, gb, ib, bb)
+    v = {k: val.cpu().numpy() for k, val in raster.state_views(st).items()}
+    np.testing.assert_array_equal(v["ranges"][0].astype(np.uint32), g["ranges"])
+    vis = g["radii"] > 0
+    pl = v["point_list"].astype(np.uint32)
+    ours = {
+        "values": pl, "keys": reference_keys(pl, v["ranges"][0].astype(np.uint32), v["depth"][0]),
+        "radii": radii.cpu().numpy(),
+        "depth": np.where(vis, v["depth"][0], 0).astype(np.float32),
+        "means2D": np.where(vis[:, None], v["means2D"][0], 0).astype(np.float32),
+        "conic_opacity": np.where(vis[:, None], v["conic_opacity"][0], 0).astype(np.float32),
+        "signal": np.where(vis[:, None], v["signal"][0], 0).astype(np.float32),
+        "n_contrib": v["n_contrib"][0].astype(np.uint32).reshape(H, W),
+        "final_T": v["final_T"][0].astype(np.float32).reshape(H, W),
+        "out_real": o_r.cpu().numpy(), "out_imag": o_i.cpu().numpy()}
+    for k in m.DIGESTED:
+        assert m.digest(ours[k]) == str(g["sha256_" + k]), k
+    gr, gi = m.case_dL()
+    out = wr.rasterize_gaussians_backward(args[0], args[1], radii, o_r, o_i, args[2], args[3], args[4], 1.0, args[8],
+                                          args[9], t(gr), t(gi), args[10], args[11], gb, K, bb, ib)
+    names = ["dL_dmeans2D", "dL_dmeans3D", "dL_dmlp", "dL_dopacity", "dL_dcov3D", "dL_dscales", "dL_drotations"]
+    for nm, got in zip(names, out):
+        if nm not in m.GRADS:
+            continue
+        diff = np.linalg.norm(m.sketch(got.cpu().numpy()) - g["sketch_" + nm])
+        assert diff <= 1e-4 * float(g["norm_" + nm]) + 1e-12, (nm, diff / float(g["norm_" + nm]))
+
+
+def test_sketch_estimates_difference_norms():
+    """The count-sketch behind the bench-size gradient check is linear and
+    estimates 2-norms to a few per cent at these sizes."""
+    m = _mod()
+    rng = np.random.default_rng(0)
+    a = rng.normal(size=150000).astype(np.float32)
+    b = a + 1e-5 * rng.normal(size=a.size).astype(np.float32)
+    est = np.linalg.norm(m.sketch(a) - m.sketch(b))
+    true = np.linalg.norm(a.astype(np.float64) - b.astype(np.float64))
+    assert abs(est / true - 1.0) < 0.1
+    assert abs(np.linalg.norm(m.sketch(a)) / np.linalg.norm(a.astype(np.float64)) - 1.0) < 0.1
