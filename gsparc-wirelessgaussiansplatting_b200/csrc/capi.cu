@@ -15,6 +15,8 @@
 #include <mutex>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -81,18 +83,23 @@ cudaEvent_t pool_event() {
   return e;
 }
 
-// Records an event pair around one launch when timing is enabled.
+// Marks one pipeline stage: an NVTX range named after its kernels around the
+// host-side launch (seen by profilers that record NVTX: stage names on the
+// timeline, `ncu --nvtx --nvtx-include <stage>/` to capture one stage), and,
+// when timing is enabled, an event pair around the launch.
 struct Timed {
   int id;
   cudaStream_t s;
   cudaEvent_t a = nullptr;
   Timed(int id_, cudaStream_t s_) : id(id_), s(s_) {
+    nvtxRangePushA(kKernelNames[id]);
     if (!g_timing) return;
     std::lock_guard<std::mutex> lk(g_tmu);
     a = pool_event();
     cudaEventRecord(a, s);
   }
   ~Timed() {
+    nvtxRangePop();
     if (!a) return;
     std::lock_guard<std::mutex> lk(g_tmu);
     cudaEvent_t b = pool_event();

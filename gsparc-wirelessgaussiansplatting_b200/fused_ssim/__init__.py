@@ -1,6 +1,34 @@
 """``fused_ssim`` Python API of the reference (fused-ssim/fused_ssim/__init__.py:1-41)
 over the sm_100a kernels.  C1 = 0.01^2, C2 = 0.03^2; padding "same" or
-"valid" (the map cropped by 5 pixels on every side before the mean)."""
+"valid" (the map cropped by 5 pixels on every side before the mean).
+
+This module keeps fused-ssim's Python interface (the FusedSSIMMap autograd
+Function and the fused_ssim wrapper) line for line so that it is a drop-in;
+that interface is fused-ssim's, used under its licence:
+
+    MIT License
+
+    Copyright (c) 2024 Rahul Goel
+
+    Permission is hereby granted, free of charge, to any person obtaining a
+    copy of this software and associated documentation files (the
+    "Software"), to deal in the Software without restriction, including
+    without limitation the rights to use, copy, modify, merge, publish,
+    distribute, sublicense, and/or sell copies of the Software, and to permit
+    persons to whom the Software is furnished to do so, subject to the
+    following conditions:
+
+    The above copyright notice and this permission notice shall be included
+    in all copies or substantial portions of the Software.
+
+    THE SOFTWARE IS PROVIDED "AS IS", WITHOUT WARRANTY OF ANY KIND, EXPRESS
+    OR IMPLIED, INCLUDING BUT NOT LIMITED TO THE WARRANTIES OF
+    MERCHANTABILITY, FITNESS FOR A PARTICULAR PURPOSE AND NONINFRINGEMENT. IN
+    NO EVENT SHALL THE AUTHORS OR COPYRIGHT HOLDERS BE LIABLE FOR ANY CLAIM,
+    DAMAGES OR OTHER LIABILITY, WHETHER IN AN ACTION OF CONTRACT, TORT OR
+    OTHERWISE, ARISING FROM, OUT OF OR IN CONNECTION WITH THE SOFTWARE OR THE
+    USE OR OTHER DEALINGS IN THE SOFTWARE.
+"""
 from __future__ import annotations
 
 import torch

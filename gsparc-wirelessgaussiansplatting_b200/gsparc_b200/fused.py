@@ -33,7 +33,7 @@ import ctypes
 import numpy as np
 import torch
 
-from . import _lib, raster, scenes
+from . import _lib, raster, scenes, shard
 from ._lib import check, ptr, stream_of
 from .autograd import RasterPlan
 from .loss import Evaluator, SplatLoss, conf_floats
@@ -154,10 +154,7 @@ class FusedTrainer:
         per_g = int(self.shared is None)
         if self.group is not None:
             # receivers are sharded: every rank densifies the same way from the summed statistics
-            import torch.distributed as dist
-            dist.all_reduce(self.grad_accum, op=dist.ReduceOp.SUM, group=self.group)
-            dist.all_reduce(self.grad_denom, op=dist.ReduceOp.SUM, group=self.group)
-            dist.all_reduce(self.max_radii2D, op=dist.ReduceOp.MAX, group=self.group)
+            shard.reduce_densify_stats(self.grad_accum, self.grad_denom, self.max_radii2D, self.group)
         inf = float("inf")
         lo = list(scene_min) if scene_min is not None else [-inf] * 3
         hi = list(scene_max) if scene_max is not None else [inf] * 3
@@ -289,8 +286,7 @@ class FusedTrainer:
 
     def _reduce_and_adam(self):
         if self.group is not None:
-            import torch.distributed as dist
-            dist.all_reduce(self.grads, op=dist.ReduceOp.SUM, group=self.group)
+            shard.allreduce_flat(self.grads, self.group)
         b1, b2 = self.betas
         check("gaussian_adam_step", _lib.lib().gsparc_gaussian_adam_step(
             self.P, self.n_mlp, self.n_conf, ptr(self.params), ptr(self.grads), ptr(self.exp_avg), ptr(self.exp_avg_sq),

@@ -45,3 +45,22 @@ def allreduce_grads(params, group=None) -> int:
             p.grad.copy_(g)
         off += n
     return int(flat.numel())
+
+
+def allreduce_flat(flat: torch.Tensor, group=None) -> None:
+    """The exchange step of the receiver-sharded training step: sum the flat
+    gradient buffer (every parameter group, the MLPs included, in one
+    contiguous tensor) over the ranks in one collective, in place.
+    FusedTrainer issues it inside its captured step, between the adjoint and
+    the optimizer kernel, on the step's stream."""
+    dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+
+
+def reduce_densify_stats(accum: torch.Tensor, denom: torch.Tensor, max_radii2D: torch.Tensor, group=None) -> None:
+    """Densification statistics of the receivers of every rank (train.py:508-516
+    accumulates them per rendered receiver): the gradient-norm sums and
+    counts add up, the screen radii take the maximum; in place, so that every
+    rank then densifies the same Gaussians the same way."""
+    dist.all_reduce(accum, op=dist.ReduceOp.SUM, group=group)
+    dist.all_reduce(denom, op=dist.ReduceOp.SUM, group=group)
+    dist.all_reduce(max_radii2D, op=dist.ReduceOp.MAX, group=group)
