@@ -894,7 +894,8 @@ SharedMlpLayout shared_mlp_layout_bf16(int layers, size_t rows, int out) {
   L.s = w;   // first: the sigmoid outputs [rows][out] (the amplitudes for out > 1)
   w += a(rows * (size_t)out);
   L.z[1] = w;
-  w += a((size_t)layers * rows * 128 / 2);   // BF16 pre-activations, two per float
+  // BF16 pre-activations, two per float, for whole 128-row tiles (tile-transposed)
+  w += a((size_t)layers * ((rows + 127) / 128 * 128) * 128 / 2);
   L.d0 = w;
   w += a(rows * kFeat);
   L.work = w;

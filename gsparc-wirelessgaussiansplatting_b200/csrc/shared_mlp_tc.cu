@@ -148,6 +148,16 @@ __device__ __forceinline__ void row_pair(size_t row0, int t, int P, int& r, int&
   g = gg;
 }
 
+// Stored pre-activations, tile-transposed so that a warp's 16-byte accesses to
+// one 8-column chunk of its 32 rows cover 512 contiguous bytes: layer l, row
+// tile, chunk k (columns 8k..8k+7), row t of the tile at element
+//   l * zrows * 128 + tile * 128 * 128 + k * 128 * 8 + t * 8,
+// zrows = the row count rounded up to whole tiles (the allocation's size).
+__device__ __forceinline__ size_t z_row_base(size_t zrows, int l, size_t tile, int t) {
+  return (size_t)l * zrows * kH + tile * (size_t)kRows * kH + (size_t)t * 8;
+}
+constexpr int kZChunk = kRows * 8;   // elements between a row's consecutive 8-column chunks
+
 // Features of one pair (as mlp_features_kernel), zero for culled pairs.  The
 // positional encoding's higher octaves come from the first by the double-angle
 // identities: the arguments are exact power-of-two multiples of the first, so
@@ -280,6 +290,7 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   uint32_t phase = 0;
   bool ok = true;
   const size_t ntiles = (rows + kRows - 1) / kRows;
+  const size_t zrows = ntiles * kRows;   // pre-activation rows, whole tiles
   for (size_t tile = (size_t)blockIdx.x * kFwdGroups + grp; tile < ntiles; tile += (size_t)gridDim.x * kFwdGroups) {
     const size_t row0 = tile * kRows, row = row0 + t;
     const bool valid = row < rows;
@@ -313,7 +324,7 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         ok = false;
         break;
       }
-      __nv_bfloat16* z_out = zb + (size_t)l * rows * kH;
+      __nv_bfloat16* z_out = zb + z_row_base(zrows, l, tile, t);
 #pragma unroll 1
       for (int c0 = 0; c0 < kH; c0 += 32) {
         float v[32];
@@ -326,7 +337,7 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
           for (int i = 0; i < 4; ++i) z2[i] = fadd2(make_float2(v[q * 8 + 2 * i], v[q * 8 + 2 * i + 1]), b2[q * 4 + i]);
           const uint4 zp = make_uint4(pack2(z2[0].x, z2[0].y), pack2(z2[1].x, z2[1].y), pack2(z2[2].x, z2[2].y),
                                       pack2(z2[3].x, z2[3].y));
-          if (valid) *reinterpret_cast<uint4*>(z_out + row * kH + c0 + q * 8) = zp;
+          if (valid) *reinterpret_cast<uint4*>(z_out + (size_t)((c0 + q * 8) / 8) * kZChunk) = zp;
           // the next layer (and the adjoint) see the BF16-rounded pre-activation
           float zr[8], a[8];
           unpack8(zp, zr);
@@ -514,6 +525,7 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   const uint32_t dwo_col = col;                       // kOut outputs: dW_out^T
   const uint32_t scratch = col + (kMulti ? kOut : 0);  // 3 layers: 336 (+ 0) or 320 + 64 = 384; + 128 <= 512
   const size_t ntiles = (rows + kRows - 1) / kRows;
+  const size_t zrows = ntiles * kRows;   // pre-activation rows, whole tiles
   const size_t tile_stride = (size_t)gridDim.x * kBwdGroups;
   // steps per tile, from the top: the output step (kOut outputs), then hidden layers L-1 .. 0
   constexpr int kTop = kMulti ? kLayers : kLayers - 1;
@@ -602,13 +614,12 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
       if (t == 0) {
         // into L2 ahead of use: this tile's remaining pre-activation slabs (one
         // contiguous 32 KB range per layer), then the next tile's first inputs
-        const uint32_t n = (uint32_t)(rows - row0 < (size_t)kRows ? rows - row0 : (size_t)kRows);
-        for (int l = 0; l + 1 < kLayers; ++l) tc::prefetch_l2(zb + (size_t)l * rows * kH + row0 * kH, n * kH * 2);
+        for (int l = 0; l + 1 < kLayers; ++l) tc::prefetch_l2(zb + z_row_base(zrows, l, tile, 0), kRows * kH * 2);
         const size_t nt = tile + tile_stride;
         if (nt < ntiles) {
           const size_t r1 = nt * kRows;
           const uint32_t n1 = (uint32_t)(rows - r1 < (size_t)kRows ? rows - r1 : (size_t)kRows);
-          tc::prefetch_l2(zb + (size_t)(kLayers - 1) * rows * kH + r1 * kH, n1 * kH * 2);
+          tc::prefetch_l2(zb + z_row_base(zrows, kLayers - 1, nt, 0), kRows * kH * 2);
           tc::prefetch_l2(S + r1 * kOut, n1 * 4 * kOut);
           tc::prefetch_l2(radii + r1, n1 * 4);
           tc::prefetch_l2(dL_dsignal + (kMulti ? r1 * kOut : 2 * r1), n1 * (kMulti ? 4 * kOut : 8));
@@ -642,12 +653,14 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         // output layer: dO, its weight gradient (reduced over the warp's rows), dZ of the last hidden layer
         const float s = valid ? S[row] : 0.0f;
         const float dO = vis ? dL_dsignal[2 * row] * s * (1.0f - s) : 0.0f;
-        const uint4* zl = reinterpret_cast<const uint4*>(zb + (size_t)(kLayers - 1) * rows * kH + row * kH);
+        const __nv_bfloat16* zl = zb + z_row_base(zrows, kLayers - 1, tile, t);
 #pragma unroll 1
         for (int c0 = 0; c0 < kH; c0 += 32) {
           uint4 zq[4];   // a 32-column chunk of the row in flight at once
 #pragma unroll
-          for (int q = 0; q < 4; ++q) zq[q] = valid ? zl[c0 / 8 + q] : make_uint4(0u, 0u, 0u, 0u);
+          for (int q = 0; q < 4; ++q)
+            zq[q] = valid ? *reinterpret_cast<const uint4*>(zl + (size_t)(c0 / 8 + q) * kZChunk)
+                          : make_uint4(0u, 0u, 0u, 0u);
           float red[32];
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
@@ -693,11 +706,11 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
             *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kFin + 8, kLbo, kSboA)) = make_uint4(0u, 0u, 0u, 0u);
           }
         } else {
-          const __nv_bfloat16* zp = zb + (size_t)(l - 1) * rows * kH + row * kH;
+          const __nv_bfloat16* zp = zb + z_row_base(zrows, l - 1, tile, t);
 #pragma unroll
           for (int c0 = 0; c0 < kH; c0 += 8) {
             float z[8], a[8];
-            if (valid) unpack8(*reinterpret_cast<const uint4*>(zp + c0), z);
+            if (valid) unpack8(*reinterpret_cast<const uint4*>(zp + (size_t)(c0 / 8) * kZChunk), z);
             else
 #pragma unroll
               for (int i = 0; i < 8; ++i) z[i] = 0.0f;

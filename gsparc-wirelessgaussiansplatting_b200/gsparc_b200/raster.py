@@ -365,9 +365,9 @@ def ssim_forward(img1, img2, C1, C2, train=True):
     if a.dim() != 4 or a.shape != b.shape:
         raise ValueError("img1 and img2 must both be [B,CH,H,W] with the same shape")
     B, CH, H, W = a.shape
-    mp = torch.zeros_like(a)
+    mp = torch.empty_like(a)          # the kernel writes every pixel of each output
     if train:
-        d1, d2, d3 = torch.zeros_like(a), torch.zeros_like(a), torch.zeros_like(a)
+        d1, d2, d3 = torch.empty_like(a), torch.empty_like(a), torch.empty_like(a)
     else:
         d1 = d2 = d3 = torch.empty(0, device=a.device)
     check("ssim_forward", _lib.lib().gsparc_ssim_forward(
@@ -384,7 +384,7 @@ def ssim_backward(img1, img2, dL_dmap, dm_dmu1, dm_dsigma1_sq, dm_dsigma12, C1, 
     d2 = _dev_f32(dm_dsigma1_sq, "dm_dsigma1_sq", a.device)
     d3 = _dev_f32(dm_dsigma12, "dm_dsigma12", a.device)
     B, CH, H, W = a.shape
-    out = torch.zeros_like(a)
+    out = torch.empty_like(a)         # written at every pixel
     check("ssim_backward", _lib.lib().gsparc_ssim_backward(
         B, CH, H, W, float(C1), float(C2), ptr(a), ptr(b), ptr(g), ptr(d1), ptr(d2), ptr(d3), ptr(out),
         stream_of(a.device)))

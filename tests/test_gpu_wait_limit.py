@@ -117,7 +117,8 @@ def test_bf16_mlp_waits_give_up_then_recover():
     # restored: clean and equal to the calls before
     radii, st = fwd()
     assert _status(st)[0] == 0
-    assert torch.equal(raster.state_views(st)["signal"], sig0)
+    vis = radii > 0      # culled pairs' signal entries are never written
+    assert torch.equal(raster.state_views(st)["signal"][vis], sig0[vis])
     dp1, dm1 = bwd(st, radii, dsig)
     assert _status(st)[0] == 0
     for a, b in ((dp1, dp0), (dm1, dm0)):
