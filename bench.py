@@ -318,13 +318,16 @@ class _Timer:
         return float(tt)
 
 
-def _launches_per_step(kt_results, n_steps, P, R):
+def _launches_per_step(kt_results, n_steps, P, R, capacity, tiles=138, sms=148):
     """Kernel launches per step from the library's per-call timing counts:
     the loss is two launches per call, the depth sort 1 or 4 (the library
-    says which), every other timed call one launch."""
+    says which), the blend adjoint two when a one-CTA scan first numbers its
+    multi-chunk work items (capacity / 64 + R x tiles >= 2 x 64 x SMs), every
+    other timed call one launch."""
     from gsparc_b200 import _lib
     sort_n = int(_lib.lib().gsparc_depth_sort_launches(int(P), int(R)))
-    per_call = {"splat_loss_kernels": 2, "depth_sort_kernels": sort_n}
+    per_call = {"splat_loss_kernels": 2, "depth_sort_kernels": sort_n,
+                "blend_backward_kernel": 2 if capacity // 64 + R * tiles >= 2 * 64 * sms else 1}
     tot = sum(c * per_call.get(k, 1) for k, (_, c) in kt_results.items())
     return tot // max(n_steps, 1)
 
@@ -499,7 +502,8 @@ def run_ours(args):
             bf.step_eager(b[0], b[1], tx, b[2])
         torch.cuda.synchronize()
     ktimes = {k: v for k, v in kt.results().items() if v[1] > 0}
-    launches = _launches_per_step(ktimes, n_eager, P_CFG3, R_CFG3)
+    launches = _launches_per_step(ktimes, n_eager, P_CFG3, R_CFG3, cap3 * R_CFG3,
+                                  sms=torch.cuda.get_device_properties(dev).multi_processor_count)
     kms = {k: v[0] / n_eager for k, v in sorted(ktimes.items())}
     dom = max(ktimes, key=lambda k: ktimes[k][0])
     rows3 = P_CFG3 * R_CFG3
@@ -685,6 +689,22 @@ def _side_lines(args, dev, timed):
     return out
 
 
+def run_check_ranks():
+    """Launcher check without GPUs: join a gloo process group on 127.0.0.1,
+    print this rank's place in it, leave."""
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        dist.init_process_group("gloo")
+        dist.barrier()
+        print(json.dumps({"rank": dist.get_rank(), "world": dist.get_world_size()}), flush=True)
+        dist.barrier()
+        dist.destroy_process_group()
+    else:
+        print(json.dumps({"rank": 0, "world": 1}), flush=True)
+    return 0
+
+
 def run_eager(args):
     """Eager steps of one FusedTrainer configuration for profiler captures."""
     import numpy as np
@@ -739,11 +759,15 @@ def main():
     ap.add_argument("--mlp", choices=["ref", "relu64", "gelu128", "ch64"], default="ref")
     ap.add_argument("--precision", choices=["fp32", "bf16"], default="fp32")
     ap.add_argument("--times", action="store_true")
+    ap.add_argument("--check-ranks", action="store_true",
+                    help="start the ranks as for --gpus N, have each join a gloo group and print its rank, and exit")
     args = ap.parse_args()
     if args.eager_steps > 0:
         return run_eager(args)
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         return _launch_ranks(args)
+    if args.check_ranks:
+        return run_check_ranks()
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
