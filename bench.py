@@ -690,14 +690,18 @@ def _side_lines(args, dev, timed):
 
 
 def run_check_ranks():
-    """Launcher check without GPUs: join a gloo process group on 127.0.0.1,
-    print this rank's place in it, leave."""
+    """Launcher check without GPUs: join a gloo process group on 127.0.0.1;
+    rank 0 prints every rank's place in it (one line per rank, gathered, so
+    the ranks' output never interleaves), then all leave."""
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if world > 1:
         dist.init_process_group("gloo")
-        dist.barrier()
-        print(json.dumps({"rank": dist.get_rank(), "world": dist.get_world_size()}), flush=True)
+        places = [None] * dist.get_world_size()
+        dist.all_gather_object(places, {"rank": dist.get_rank(), "world": dist.get_world_size()})
+        if dist.get_rank() == 0:
+            for p in places:
+                print(json.dumps(p), flush=True)
         dist.barrier()
         dist.destroy_process_group()
     else:

@@ -318,8 +318,8 @@ scatter_kernel(int P, TileGrid grid, GeomView geo, uint32_t* __restrict__ cursor
 // ---- segment placement ------------------------------------------------------
 // One CTA per segment.  A segment's ranks are unique values below P, so:
 //  * bitmap (P <= kBitmapMaxP, and the segment is not tiny next to P): set
-//    one bit per rank, prefix-popcount the words per group of 8, and every
-//    rank's position is its group prefix + the popcounts before it;
+//    one bit per rank, prefix-popcount the words per group of 8, then walk
+//    the words in order, each set bit writing its id at the next position;
 //  * short segments (n <= kPlaceSmall) otherwise: bitonic network over the
 //    32-bit ranks in shared memory.
 // The Gaussian id of rank q is the depth order's entry q.
@@ -401,27 +401,32 @@ segment_place_kernel(int P, int T, const uint2* __restrict__ ranges, const Image
     off += c;
   }
   __syncthreads();
-  for (int i0 = threadIdx.x; i0 < n; i0 += 8 * kPlaceThreads) {
-    uint32_t q[8], pos[8], id[8];
+  // walk the bitmap in rank order: thread i of a round takes word w = round
+  // base + i, so the 8 lanes of a group hold its 8 words; a word's first
+  // position is its group's prefix plus the popcounts of the lanes before it
+  // (a shuffle scan within the 8 lanes), and its set bits take the positions
+  // after it in bit order.  A warp writes one contiguous run of the segment.
+  const int lane = threadIdx.x & 31;
+  for (int base = 0; base < words; base += kPlaceThreads) {
+    const int w = base + (int)threadIdx.x;
+    uint32_t bits = w < words ? bm[w] : 0u;
+    const uint32_t c = __popc(bits);
+    uint32_t incl = c;
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int i = i0 + u * kPlaceThreads;
-      q[u] = i < n ? sr[i] : 0xffffffffu;
+    for (int d = 1; d < 8; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d, 8);
+      if ((lane & 7) >= d) incl += o;
     }
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      pos[u] = 0xffffffffu;
-      if (q[u] < (uint32_t)P) {
-        const int w = (int)(q[u] >> 5);
-        uint32_t p = pre[w >> 3];
-        for (int v = w & ~7; v < w; ++v) p += __popc(bm[v]);
-        pos[u] = p + __popc(bm[w] & ((1u << (q[u] & 31u)) - 1u));
+    if (w < words) {
+      uint32_t pos = pre[w >> 3] + incl - c;
+      const uint32_t* idw = ids + ((size_t)w << 5);
+      while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1u;
+        if (pos < (uint32_t)n) out[pos] = idw[b];
+        ++pos;
       }
-      id[u] = id_of(q[u]);
     }
-#pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (pos[u] < (uint32_t)n) out[pos[u]] = id[u];
   }
 }
 

@@ -462,6 +462,8 @@ int gsparc_shared_mlp_forward(int P, int R, int layers, int width, int act, int 
   if (st != GSPARC_OK) return st;
   if (P == 0) return GSPARC_OK;
   if (!means3D || !rx_pos || !params || !geom_state || !workspace) return invalid("null pointer");
+  if (precision == GSPARC_MLP_BF16 && ((uintptr_t)workspace & 255u) != 0)
+    return invalid("the BF16 path needs a 256-byte aligned workspace");
   cudaStream_t s = (cudaStream_t)stream;
   GeomView geo;
   carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
@@ -493,6 +495,8 @@ int gsparc_shared_mlp_backward(int P, int R, int layers, int width, int act, int
   }
   if (!means3D || !rx_pos || !params || !geom_state || !workspace || !dL_dsignal || !dL_dmeans3D)
     return invalid("null pointer");
+  if (precision == GSPARC_MLP_BF16 && ((uintptr_t)workspace & 255u) != 0)
+    return invalid("the BF16 path needs a 256-byte aligned workspace");
   GeomView geo;
   carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
   if (precision == GSPARC_MLP_BF16) {
@@ -513,6 +517,13 @@ int gsparc_shared_mlp_backward(int P, int R, int layers, int width, int act, int
                                         dL_dsignal, dL_dparams, dL_dmeans3D, s),
              "shared mlp backward");
   }
+  return GSPARC_OK;
+}
+
+int gsparc_shared_mlp_bf16_act_table(int act, uint16_t* out, void* stream) {
+  if (act != GSPARC_ACT_RELU && act != GSPARC_ACT_GELU) return invalid("act");
+  if (!out) return invalid("null pointer");
+  GS_CHECK(launch_bf16_act_table(act, out, (cudaStream_t)stream), "bf16 activation table");
   return GSPARC_OK;
 }
 

@@ -132,6 +132,8 @@ cudaError_t launch_shared_mlp_bf16(bool fwd, int P, int R, int layers, int act, 
                                    cudaStream_t s);
 cudaError_t launch_mlp_features_backward(int P, int R, const float* means3D, const float* rx_pos, const int* radii,
                                          const float* dX, float* dL_dmeans3D, cudaStream_t s);
+// the BF16 path's activation (forward and adjoint) and derivative for every BF16 input
+cudaError_t launch_bf16_act_table(int act, uint16_t* out, cudaStream_t s);
 
 cudaError_t launch_shared_mlp_forward(int P, int R, int layers, int width, int act, int out, const float* means3D,
                                       const float* rx_pos, const float* params, const GeomView& geo, float* work,

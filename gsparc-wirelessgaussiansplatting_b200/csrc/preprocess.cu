@@ -101,10 +101,13 @@ __device__ __forceinline__ float2 emission_mlp_row(const float* __restrict__ sm,
   return make_float2(o[0], o[1]);
 }
 
-// Dynamic shared memory: the warps' MLP staging areas, the 4 x 256 digit
-// counters of the depth keys (the radix sort's histograms), then
-// (kSharedHist) one counter per tile.
-template <bool kSharedHist, bool kVec>
+// Dynamic shared memory: the warps' MLP staging areas (per-Gaussian MLP
+// only), the 4 x 256 digit counters of the depth keys (the radix sort's
+// histograms), then (kSharedHist) one counter per tile.  kMlp: 0 no
+// per-Gaussian MLP (the shared MLP writes the signal later; without the
+// 50 KB staging area four times as many CTAs fit on an SM), 1 staged with
+// float4 loads, 2 staged with scalar loads.
+template <bool kSharedHist, int kMlp>
 __global__ void __launch_bounds__(kPreThreads)
 preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
                   const float* __restrict__ means3D, const float* __restrict__ mlp,
@@ -116,7 +119,7 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   float* sm_mlp = smem + wid * kMlpSmemPerWarp;
-  uint32_t* dhist = reinterpret_cast<uint32_t*>(smem + (kPreThreads / 32) * kMlpSmemPerWarp);
+  uint32_t* dhist = reinterpret_cast<uint32_t*>(smem + (kMlp ? (kPreThreads / 32) * kMlpSmemPerWarp : 0));
   uint32_t* hist = dhist + 1024;
   const int r = blockIdx.y;
   for (int t = threadIdx.x; t < 1024; t += blockDim.x) dhist[t] = 0;
@@ -212,8 +215,8 @@ preprocess_kernel(int P, int H, int W, TileGrid grid, float mod,
   }
   // emission MLP of the visible Gaussians, from the warp's staged parameters
   // (no per-Gaussian MLP: the signal is written later by the shared MLP)
-  if (mlp != nullptr && __any_sync(0xffffffffu, vis)) {
-    stage_mlp<kVec>(sm_mlp, mlp, P, g0 + wid * 32, lane);
+  if (kMlp != 0 && __any_sync(0xffffffffu, vis)) {
+    stage_mlp<kMlp == 1>(sm_mlp, mlp, P, g0 + wid * 32, lane);
     __syncwarp();
     if (vis) {
       const float3 rx = make_float3(__ldg(rx_pos + 3 * r), __ldg(rx_pos + 3 * r + 1), __ldg(rx_pos + 3 * r + 2));
@@ -269,18 +272,33 @@ __global__ void mark_visible_kernel(int P, const float* __restrict__ means3D,
   present[g] = rr <= 0.04f ? 0 : 1;
 }
 
-// MLP staging (50,432 B) + digit counters (4 KB)
-constexpr size_t kMlpSmemBytes = (kPreThreads / 32) * kMlpSmemPerWarp * sizeof(float) + 1024 * sizeof(uint32_t);
+// MLP staging (50,432 B), digit counters (4 KB)
+constexpr size_t kMlpStageBytes = (kPreThreads / 32) * kMlpSmemPerWarp * sizeof(float);
+constexpr size_t kDigitSmemBytes = 1024 * sizeof(uint32_t);
 // dynamic shared memory ceiling: 227 KB per CTA less 1 KB kept for the
 // kernel's static shared memory (the last CTA's scan)
 constexpr int kPreDynSmemMax = 226 * 1024;
-constexpr int kMaxSharedHistTiles = (int)((kPreDynSmemMax - kMlpSmemBytes) / sizeof(uint32_t));
 
-template <bool kSharedHist, bool kVec>
-static cudaError_t set_preprocess_smem(int dev) {
-  (void)dev;
-  return cudaFuncSetAttribute(preprocess_kernel<kSharedHist, kVec>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <bool kSharedHist, int kMlp>
+static cudaError_t set_preprocess_smem() {
+  return cudaFuncSetAttribute(preprocess_kernel<kSharedHist, kMlp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kPreDynSmemMax);
+}
+
+template <int kMlp>
+static void preprocess_launch(bool shared_hist, dim3 gridd, size_t smem, cudaStream_t stream, int P, int H, int W,
+                              const TileGrid& grid, float mod, const float* means3D, const float* mlp,
+                              const float* opacities, const float* scales, const float* rotations,
+                              const float* views, const float* tx_pos, const float* rx_pos, const GeomView& geo,
+                              int* radii_out, const ImageView& img, int per_cta) {
+  if (shared_hist)
+    preprocess_kernel<true, kMlp><<<gridd, kPreThreads, smem, stream>>>(
+        P, H, W, grid, mod, means3D, mlp, opacities, scales, rotations, views, tx_pos, rx_pos, geo, radii_out, img,
+        per_cta);
+  else
+    preprocess_kernel<false, kMlp><<<gridd, kPreThreads, smem, stream>>>(
+        P, H, W, grid, mod, means3D, mlp, opacities, scales, rotations, views, tx_pos, rx_pos, geo, radii_out, img,
+        per_cta);
 }
 
 cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, float mod,
@@ -296,39 +314,33 @@ cudaError_t launch_preprocess(int P, int R, int H, int W, const TileGrid& grid, 
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64 || !attr_done[dev]) {
-    if ((e = set_preprocess_smem<true, true>(dev)) != cudaSuccess) return e;
-    if ((e = set_preprocess_smem<true, false>(dev)) != cudaSuccess) return e;
-    if ((e = set_preprocess_smem<false, true>(dev)) != cudaSuccess) return e;
-    if ((e = set_preprocess_smem<false, false>(dev)) != cudaSuccess) return e;
+    if ((e = set_preprocess_smem<true, 0>()) != cudaSuccess) return e;
+    if ((e = set_preprocess_smem<true, 1>()) != cudaSuccess) return e;
+    if ((e = set_preprocess_smem<true, 2>()) != cudaSuccess) return e;
+    if ((e = set_preprocess_smem<false, 0>()) != cudaSuccess) return e;
+    if ((e = set_preprocess_smem<false, 1>()) != cudaSuccess) return e;
+    if ((e = set_preprocess_smem<false, 2>()) != cudaSuccess) return e;
     if (dev >= 0 && dev < 64) attr_done[dev] = true;
   }
-  const bool vec = (((uintptr_t)mlp) & 15u) == 0;
+  const int mode = mlp == nullptr ? 0 : ((((uintptr_t)mlp) & 15u) == 0 ? 1 : 2);
   // groups of kPreThreads Gaussians per CTA: one while the launch is small
   // (latency), up to 16 when it fills many waves, so that each CTA's
   // histogram initialisation and flush serve up to 1,024 Gaussians
   int per_cta = 1;
   while (per_cta < 16 && (long long)P * R >= 2LL * per_cta * device_sm_count() * kPreThreads * 16) per_cta *= 2;
-  dim3 block(kPreThreads), gridd((P + kPreThreads * per_cta - 1) / (kPreThreads * per_cta), R);
-  if (grid.T <= kMaxSharedHistTiles) {
-    const size_t smem = kMlpSmemBytes + (size_t)grid.T * sizeof(uint32_t);
-    if (vec)
-      preprocess_kernel<true, true><<<gridd, block, smem, stream>>>(P, H, W, grid, mod, means3D, mlp, opacities,
-                                                                    scales, rotations, views, tx_pos, rx_pos, geo,
-                                                                    radii_out, img, per_cta);
-    else
-      preprocess_kernel<true, false><<<gridd, block, smem, stream>>>(P, H, W, grid, mod, means3D, mlp, opacities,
-                                                                     scales, rotations, views, tx_pos, rx_pos, geo,
-                                                                     radii_out, img, per_cta);
-  } else {
-    if (vec)
-      preprocess_kernel<false, true><<<gridd, block, kMlpSmemBytes, stream>>>(
-          P, H, W, grid, mod, means3D, mlp, opacities, scales, rotations, views, tx_pos, rx_pos, geo, radii_out,
-          img, per_cta);
-    else
-      preprocess_kernel<false, false><<<gridd, block, kMlpSmemBytes, stream>>>(
-          P, H, W, grid, mod, means3D, mlp, opacities, scales, rotations, views, tx_pos, rx_pos, geo, radii_out,
-          img, per_cta);
-  }
+  const dim3 gridd((P + kPreThreads * per_cta - 1) / (kPreThreads * per_cta), R);
+  const size_t base = (mode ? kMlpStageBytes : 0) + kDigitSmemBytes;
+  const bool shared_hist = base + (size_t)grid.T * sizeof(uint32_t) <= (size_t)kPreDynSmemMax;
+  const size_t smem = base + (shared_hist ? (size_t)grid.T * sizeof(uint32_t) : 0);
+  if (mode == 0)
+    preprocess_launch<0>(shared_hist, gridd, smem, stream, P, H, W, grid, mod, means3D, mlp, opacities, scales,
+                         rotations, views, tx_pos, rx_pos, geo, radii_out, img, per_cta);
+  else if (mode == 1)
+    preprocess_launch<1>(shared_hist, gridd, smem, stream, P, H, W, grid, mod, means3D, mlp, opacities, scales,
+                         rotations, views, tx_pos, rx_pos, geo, radii_out, img, per_cta);
+  else
+    preprocess_launch<2>(shared_hist, gridd, smem, stream, P, H, W, grid, mod, means3D, mlp, opacities, scales,
+                         rotations, views, tx_pos, rx_pos, geo, radii_out, img, per_cta);
   return cudaGetLastError();
 }
 

@@ -1,28 +1,35 @@
 // Shared emission MLP in BF16 on the 5th-generation tensor cores (tcgen05).
 //
 // Same network as shared_mlp.cu (features, hidden layers of width 128,
-// sigmoid of one output, or of 64 outputs whose layer is one more MMA) with
-// BF16 operands and FP32 accumulation in tensor memory.  Two fused persistent kernels over tiles of 128 (receiver, Gaussian)
-// rows, one row per thread of a 128-thread warpgroup:
+// sigmoid of one output, or of 64 outputs) with BF16 operands and FP32
+// accumulation in tensor memory; every layer, the output layer included, is
+// an MMA (one output is padded to an N = 16 MMA).  The epilogues between the
+// MMAs -- activation, its derivative, the adjoint's product with it -- run in
+// packed BF16 arithmetic (two elements per instruction, no conversions:
+// the operands the next MMA reads and the stored pre-activations are BF16
+// anyway).  Two fused persistent kernels over tiles of 128 (receiver,
+// Gaussian) rows, one row per thread of a 128-thread warpgroup:
 //
 //   forward:  four warpgroups per CTA, each with its own tile in flight and
 //             its own 128 TMEM columns; per layer the group's leader issues
 //             the MMA, the group runs the +bias/activation epilogue.  The
 //             weights are staged in shared memory once per CTA; only the BF16
 //             pre-activations (for the adjoint) and the signal go to HBM.
-//   backward: two compute warpgroups, each with its own tile, and one MMA
-//             warp that issues every MMA of the CTA (so all accumulation into
-//             the shared weight-gradient columns is in issue order).  Per tile
-//             and hidden layer l (last first):
+//   backward: two compute groups of 256 threads (two per row, 64 columns
+//             each), each group with its own tile, and one MMA warp that issues
+//             every MMA of the CTA (so all accumulation into the shared
+//             weight-gradient columns is in issue order).  Per tile,
+//             first the output step
+//               dW_out^T += A_{L-1}^T dO,   dA_{L-1} = dO W_out
+//             then per hidden layer l (last first):
 //               dW_l | db_l += dZ_l^T [A_{l-1} | 1]   (M = 128 outputs, K = the
 //                              128 rows; accumulated in TMEM over all tiles)
 //               dA_{l-1}     = dZ_l W_l              (M = 128 rows; one
 //                              shared scratch accumulator)
 //             A_{l-1} = act(Z_{l-1}) and act'(Z_{l-1}) come from one pass over
-//             the stored pre-activations (one CDF evaluation per element;
-//             act' is held in registers as FP16 until dA arrives); the output
-//             layer's gradient is reduced on the CUDA cores.  At the end the
-//             CTA adds its TMEM accumulators to the global gradient.
+//             the stored pre-activations (act' is held in registers as BF16
+//             pairs until dA arrives).  At the end the CTA adds its TMEM
+//             accumulators to the global gradient.
 //
 // Operands use the no-swizzle core-matrix layouts of tcgen05.cuh.  A buffer
 // written row-per-thread in the K-major layout of a [rows x cols] matrix is
@@ -45,77 +52,33 @@ constexpr int kH = 128;        // hidden width of the BF16 path
 constexpr int kFin = 32;       // features
 constexpr int kRows = 128;     // rows per tile (= MMA M)
 constexpr int kFwdGroups = 4;  // forward: warpgroups (tiles in flight) per CTA
-constexpr int kBwdGroups = 2;  // backward: compute warpgroups per CTA (+ one MMA warp)
-constexpr int kBwdThreads = kBwdGroups * 128 + 32;
+constexpr int kBwdGroups = 2;  // backward: compute groups (tiles in flight) per CTA (+ one MMA warp)
+constexpr int kBwdHalves = 2;  // backward: threads per row, each with kH / kBwdHalves columns
+constexpr int kBwdGroupThreads = 128 * kBwdHalves;
+static_assert(kBwdGroupThreads * 64 == kRows * kH, "one 128-byte line of a tile's slab per thread");
+constexpr int kBwdThreads = kBwdGroups * kBwdGroupThreads + 32;
 constexpr uint32_t kLbo = 128; // core matrices along K are adjacent
 constexpr uint32_t kSboX = (kFin / 8) * 128u;         // [rows x 32] K-major
 constexpr uint32_t kSboH = (kH / 8) * 128u;           // [rows x 128] K-major
-constexpr uint32_t kSboA = ((kH + 16) / 8) * 128u;    // [rows x 144] K-major (activations | ones)
+// The adjoint's activation tile [128 rows x 144] (activations | ones) is laid
+// out like one stored pre-activation slab -- 8-column chunk k, row t at byte
+// k * 2048 + t * 16 -- so a slab lands in it with one bulk copy and is
+// activated in place.  As an MN-major operand (N = columns, K = rows) the core
+// matrices step 128 bytes along K and 2048 along N.
+constexpr uint32_t kChunkA = kRows * 16;   // bytes per 8-column chunk
+__host__ __device__ constexpr uint32_t slab_off(int r, int c) {
+  return (uint32_t)(c / 8) * kChunkA + (uint32_t)r * 16u + (uint32_t)(c % 8) * 2u;
+}
 constexpr uint32_t kPolls = 1u << 24;
+// N of the output layer's MMA: one output is padded to the smallest N (16)
+constexpr int out_mma_width(int out) { return out < 16 ? 16 : out; }
+// Adjoint TMEM plan: the weight-gradient accumulators with their ones (bias)
+// columns, dW_out^T and the 128-column dA scratch must fit 512 columns; when
+// they do not, the first layer's bias gradient is summed on the CUDA cores.
+constexpr bool bwd_bias0_on_cuda_cores(int layers, int out) {
+  return (kFin + 16) + (layers - 1) * (kH + 16) + out_mma_width(out) + kH > 512;
+}
 constexpr float kPiF = 3.14159265358979323846f;
-
-// GELU of two pre-activations at once (FP32x2) for the forward, where no
-// density term is needed: Phi from Abramowitz & Stegun 7.1.28,
-//   erf(x) = 1 - (1 + a1 x + a2 x^2 + ... + a6 x^6)^-16,  x >= 0, |error| <= 3e-7,
-// one approximate reciprocal per element and four squarings, no exponential.
-__device__ __forceinline__ float rcp_approx(float x) {
-  float r;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r;
-}
-__device__ __forceinline__ float2 gelu2(float2 z) {
-  const float2 x = make_float2(fabsf(z.x) * 0.70710678118654752f, fabsf(z.y) * 0.70710678118654752f);
-  float2 p = ffma2(x, make_float2(4.30638e-5f, 4.30638e-5f), make_float2(2.765672e-4f, 2.765672e-4f));
-  p = ffma2(p, x, make_float2(1.520143e-4f, 1.520143e-4f));
-  p = ffma2(p, x, make_float2(9.2705272e-3f, 9.2705272e-3f));
-  p = ffma2(p, x, make_float2(4.22820123e-2f, 4.22820123e-2f));
-  p = ffma2(p, x, make_float2(7.05230784e-2f, 7.05230784e-2f));
-  p = ffma2(p, x, make_float2(1.0f, 1.0f));
-  float2 r = make_float2(rcp_approx(p.x), rcp_approx(p.y));
-  r = fmul2(r, r);
-  r = fmul2(r, r);
-  r = fmul2(r, r);
-  r = fmul2(r, r);   // 1 - erf(x)
-  // Phi(z) = 1 - r / 2 (z >= 0) or r / 2 (z < 0) = 1/2 + h (r - 1), h = -+1/2
-  const float2 h = make_float2(copysignf(0.5f, -z.x), copysignf(0.5f, -z.y));
-  const float2 ph = ffma2(h, fadd2(r, make_float2(-1.0f, -1.0f)), make_float2(0.5f, 0.5f));
-  return fmul2(z, ph);
-}
-__device__ __forceinline__ float ex2_approx(float x) {
-  float r;
-  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r;
-}
-// Activation and derivative of two elements from one evaluation (FP32x2), for
-// the adjoint.  GELU's normal CDF Phi(z) = (1 + erf(z / sqrt 2)) / 2 by
-// Abramowitz & Stegun 7.1.26 (Hastings' rational approximation, |error of
-// erf| <= 1.5e-7, three orders below the BF16 rounding the results go through):
-//   erf(x) = 1 - t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2),
-//   t = 1 / (1 + p x), x >= 0, odd extension for x < 0,
-// whose exponential is also the density term of GELU':
-//   a = z Phi(z),  d = Phi(z) + z phi(z),  phi(z) = exp(-z^2 / 2) / sqrt(2 pi).
-__device__ __forceinline__ void act_and_grad2(int act, float2 z, float2& a, float2& d) {
-  if (act == 1) {
-    a = make_float2(fmaxf(z.x, 0.0f), fmaxf(z.y, 0.0f));
-    d = make_float2(z.x > 0.0f ? 1.0f : 0.0f, z.y > 0.0f ? 1.0f : 0.0f);
-    return;
-  }
-  const float2 x = make_float2(fabsf(z.x) * 0.70710678118654752f, fabsf(z.y) * 0.70710678118654752f);
-  const float2 arg = fmul2(fmul2(z, z), make_float2(-0.72134752044448170f, -0.72134752044448170f));  // -z^2/2 log2 e
-  const float2 ez = make_float2(ex2_approx(arg.x), ex2_approx(arg.y));
-  const float2 den = ffma2(make_float2(0.3275911f, 0.3275911f), x, make_float2(1.0f, 1.0f));
-  const float2 tt = make_float2(rcp_approx(den.x), rcp_approx(den.y));
-  // -(a1 + t (a2 + t (a3 + t (a4 + t a5)))): negated so erf = 1 + t p' e^{-x^2} is one FMA
-  float2 p = ffma2(tt, make_float2(-1.061405429f, -1.061405429f), make_float2(1.453152027f, 1.453152027f));
-  p = ffma2(tt, p, make_float2(-1.421413741f, -1.421413741f));
-  p = ffma2(tt, p, make_float2(0.284496736f, 0.284496736f));
-  p = ffma2(tt, p, make_float2(-0.254829592f, -0.254829592f));
-  const float2 e = ffma2(fmul2(tt, p), ez, make_float2(1.0f, 1.0f));   // erf(|z| / sqrt 2)
-  const float2 h = make_float2(copysignf(0.5f, z.x), copysignf(0.5f, z.y));
-  const float2 ph = ffma2(h, e, make_float2(0.5f, 0.5f));
-  a = fmul2(z, ph);
-  d = ffma2(fmul2(z, make_float2(0.39894228040143268f, 0.39894228040143268f)), ez, ph);
-}
 
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
   const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -124,15 +87,69 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
 __device__ __forceinline__ uint4 pack8(const float* v) {
   return make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
 }
-__device__ __forceinline__ void unpack8(uint4 u, float* v) {
-  const uint32_t w[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&w[i]);
-    const float2 f = __bfloat1622float2(h);
-    v[2 * i] = f.x;
-    v[2 * i + 1] = f.y;
+
+// ---- packed BF16 epilogue arithmetic (two elements per 32-bit register) ----
+__device__ __forceinline__ uint32_t bf2_mul(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+__device__ __forceinline__ uint32_t bf2_max(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("max.bf16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+__device__ __forceinline__ float tanh_approx(float x) {
+  float r;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+// the two BF16 halves of a packed pair as floats (exact)
+__device__ __forceinline__ float2 bf2_unpack(uint32_t z) {
+  return make_float2(__uint_as_float(z << 16), __uint_as_float(z & 0xFFFF0000u));
+}
+constexpr uint32_t kBfOne = 0x3F803F80u;   // BF16 1.0 in both halves
+
+// GELU of BF16 pre-activations in the tanh form
+//   a = h (1 + t),  h = z / 2,  t = tanh v,  v = z (c1 + c3 z^2),
+// i.e. Phi(z) ~ (1 + t) / 2, evaluated in FP32 with the hardware tanh and
+// rounded to BF16 once.  c1 = 0.80078125 and c3 = 0.034423828125 are fitted to
+// the erf GELU z Phi(z): max |a - z Phi(z)| = 3.6e-4 over [-8, 8] (the classic
+// sqrt(2/pi), 0.044715 sqrt(2/pi) give 4.7e-4), below the BF16 spacing of the
+// activations it feeds.  The adjoint's derivative is the form's own:
+//   a' = (1 + t) / 2 + h (1 - t^2) (c1 + 3 c3 z^2),
+// in FP32 (1 - t^2 needs FP32 where t is within a BF16 step of +-1).  One
+// special-function evaluation (the tanh) per element in both kernels.
+constexpr float kGeluC1 = 0.80078125f, kGeluC3 = 0.034423828125f;
+__device__ __forceinline__ uint32_t act_fwd2(int act, uint32_t zb) {
+  if (act == 1) return bf2_max(zb, 0u);
+  const float2 z = bf2_unpack(zb);
+  const float2 zz = fmul2(z, z);
+  const float2 v = fmul2(z, ffma2(zz, make_float2(kGeluC3, kGeluC3), make_float2(kGeluC1, kGeluC1)));
+  const float2 t = make_float2(tanh_approx(v.x), tanh_approx(v.y));
+  const float2 h = fmul2(z, make_float2(0.5f, 0.5f));
+  const float2 a = ffma2(h, t, h);
+  return pack2(a.x, a.y);
+}
+// act (the forward's, bit for bit) and act' of a pair, both rounded to BF16
+__device__ __forceinline__ void act_bwd2(int act, uint32_t zb, uint32_t& a2, uint32_t& d2) {
+  if (act == 1) {
+    a2 = bf2_max(zb, 0u);
+    d2 = __vcmpgts2(zb, 0u) & kBfOne;   // 1 where the BF16 half is > 0 (as a signed 16-bit integer)
+    return;
   }
+  const float2 z = bf2_unpack(zb);
+  const float2 zz = fmul2(z, z);
+  const float2 v = fmul2(z, ffma2(zz, make_float2(kGeluC3, kGeluC3), make_float2(kGeluC1, kGeluC1)));
+  const float2 t = make_float2(tanh_approx(v.x), tanh_approx(v.y));
+  const float2 h = fmul2(z, make_float2(0.5f, 0.5f));
+  const float2 a = ffma2(h, t, h);
+  const float2 s = ffma2(make_float2(-t.x, -t.y), t, make_float2(1.0f, 1.0f));   // 1 - t^2
+  const float2 w = ffma2(zz, make_float2(3.0f * kGeluC3, 3.0f * kGeluC3), make_float2(kGeluC1, kGeluC1));
+  // (h s) first: s is exactly 0 where t saturates, so w (~z^2) cannot make inf * 0
+  const float2 d = ffma2(fmul2(h, s), w, ffma2(t, make_float2(0.5f, 0.5f), make_float2(0.5f, 0.5f)));
+  a2 = pack2(a.x, a.y);
+  d2 = pack2(d.x, d.y);
 }
 
 // (receiver, Gaussian) of row row0 + t, with one 64-bit division per tile.
@@ -207,6 +224,21 @@ __device__ __forceinline__ float warp_transpose_sum32(float (&v)[32], int lane) 
   return v[0];
 }
 
+// Sum 16 per-lane values over the warp: returns, in lane j < 16, the sum of value j.
+__device__ __forceinline__ float warp_transpose_sum16(float (&v)[16], int lane) {
+#pragma unroll
+  for (int half = 8; half >= 1; half >>= 1) {
+    const bool upper = lane & half;
+#pragma unroll
+    for (int i = 0; i < half; ++i) {
+      const float send = upper ? v[i] : v[i + half];
+      const float keep = upper ? v[i + half] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, half);
+    }
+  }
+  return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 16);
+}
+
 // Warpgroup-local ordering of generic shared-memory writes and TMEM reads
 // before the group's leader issues MMAs that read / overwrite them.
 __device__ __forceinline__ void group_publish(uint32_t bar_id) {
@@ -221,14 +253,16 @@ __device__ __forceinline__ void group_publish(uint32_t bar_id) {
 // ---- forward ------------------------------------------------------------------
 // dynamic smem: W_l K-major [128 x in_l] bf16 (the B operand: n = output,
 // k = input), then per warpgroup an activation tile H [128 x 128] K-major bf16
-// whose first 8 KB also hold the feature tile X [128 x 32]; biases and the
-// output row in fp32.
+// whose first 8 KB also hold the feature tile X [128 x 32]; the hidden biases
+// and the output biases in fp32; W_out K-major [kOutMma x 128] bf16 (rows past
+// the real outputs zero).
 template <int kLayers, int act, int kOut>
 __global__ void __launch_bounds__(128 * kFwdGroups, 1)
 mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                         const float* __restrict__ rx_pos, const float* __restrict__ params,
                         const int* __restrict__ radii, __nv_bfloat16* __restrict__ zb, float* __restrict__ S,
                         float2* __restrict__ signal, ImageHeader* __restrict__ hdr, uint32_t polls) {
+  constexpr int kOutMma = out_mma_width(kOut);
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar[kFwdGroups];
   __shared__ uint32_t tbase;
@@ -241,10 +275,9 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   }
   unsigned char* Hs = smem + off + (size_t)grp * kRows * kH * 2;
   off += (size_t)kFwdGroups * kRows * kH * 2;
-  float* bias = reinterpret_cast<float*>(smem + off);   // [kLayers][128], then w_out[128] + b_out (one
-  float* wout = bias + kLayers * kH;                    // output) or b_out[kOut] (kOut outputs)
+  float* bias = reinterpret_cast<float*>(smem + off);   // [kLayers][128], then b_out[kOut]
+  float* bout = bias + kLayers * kH;
   off += (size_t)(kLayers * kH + kH + 4) * sizeof(float);
-  // kOut > 1: the output layer as an MMA, W_out K-major [kOut x 128] bf16
   unsigned char* Wo = smem + (off + 127) / 128 * 128;
 
   size_t poff = 0;
@@ -263,20 +296,14 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
     for (int j = tid; j < kH; j += blockDim.x) bias[l * kH + j] = params[poff + j];
     poff += kH;
   }
-  float bout = 0.0f;
-  if constexpr (kOut == 1) {
-    for (int j = tid; j < kH; j += blockDim.x) wout[j] = params[poff + j];
-    bout = params[poff + kH];
-  } else {
-    for (int c = tid; c < kOut * (kH / 8); c += blockDim.x) {
-      const int n = c / (kH / 8), kc = c % (kH / 8);
-      float v[8];
+  for (int c = tid; c < kOutMma * (kH / 8); c += blockDim.x) {
+    const int n = c / (kH / 8), kc = c % (kH / 8);
+    float v[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) v[i] = params[poff + (size_t)n * kH + kc * 8 + i];
-      *reinterpret_cast<uint4*>(Wo + tc::kmajor_off(n, kc * 8, kLbo, kSboH)) = pack8(v);
-    }
-    for (int j = tid; j < kOut; j += blockDim.x) wout[j] = params[poff + (size_t)kOut * kH + j];
+    for (int i = 0; i < 8; ++i) v[i] = n < kOut ? params[poff + (size_t)n * kH + kc * 8 + i] : 0.0f;
+    *reinterpret_cast<uint4*>(Wo + tc::kmajor_off(n, kc * 8, kLbo, kSboH)) = pack8(v);
   }
+  for (int j = tid; j < kOut; j += blockDim.x) bout[j] = params[poff + (size_t)kOut * kH + j];
   if (tid == 0)
     for (int q = 0; q < kFwdGroups; ++q) tc::mbar_init(&mbar[q], 1);
   if (warp == 0) tc::tmem_alloc(&tbase, kFwdGroups * kH);
@@ -291,9 +318,22 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   bool ok = true;
   const size_t ntiles = (rows + kRows - 1) / kRows;
   const size_t zrows = ntiles * kRows;   // pre-activation rows, whole tiles
-  for (size_t tile = (size_t)blockIdx.x * kFwdGroups + grp; tile < ntiles; tile += (size_t)gridDim.x * kFwdGroups) {
+  const size_t fwd_stride = (size_t)gridDim.x * kFwdGroups;
+  for (size_t tile = (size_t)blockIdx.x * kFwdGroups + grp; tile < ntiles; tile += fwd_stride) {
     const size_t row0 = tile * kRows, row = row0 + t;
     const bool valid = row < rows;
+    if (t == 0 && tile + fwd_stride < ntiles) {
+      // the next tile's radii and Gaussian centres into L2 (its rows are
+      // consecutive Gaussians of at most two receivers)
+      const size_t r1 = (tile + fwd_stride) * kRows;
+      const uint32_t n1 = (uint32_t)(rows - r1 < (size_t)kRows ? rows - r1 : (size_t)kRows);
+      tc::prefetch_l2(radii + r1, n1 * 4);
+      // centres [gs, ge) of the tile's first receiver, gs rounded down to a
+      // 16-byte boundary, ge <= P (the range stays inside the buffer)
+      const size_t g1 = r1 % (size_t)P, gs = g1 & ~(size_t)3;
+      const size_t ge = (size_t)P - g1 < (size_t)n1 ? (size_t)P : g1 + n1;
+      tc::prefetch_l2(means3D + 3 * gs, (uint32_t)((ge - gs) * 12));
+    }
     const bool vis = valid && radii[row] > 0;
     {
       int r, g;
@@ -304,14 +344,15 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
       for (int kc = 0; kc < kFin / 8; ++kc)
         *reinterpret_cast<uint4*>(Hs + tc::kmajor_off(t, kc * 8, kLbo, kSboX)) = pack8(x + kc * 8);
     }
-    float o = bout;
-    for (int l = 0; l < kLayers; ++l) {
+    // hidden layers, then the output layer (l == kLayers)
+    for (int l = 0; l <= kLayers; ++l) {
+      const bool out_layer = l == kLayers;
       const int in = l == 0 ? kFin : kH;
       group_publish(bar_id);
       if (t == 0) {
         const uint32_t sbo = (uint32_t)(in / 8) * 128u;
-        const uint32_t a0 = tc::smem_u32(Hs), b0 = tc::smem_u32(Ws[l]);
-        const uint32_t idesc = tc::idesc_bf16(kRows, kH, false, false);
+        const uint32_t a0 = tc::smem_u32(Hs), b0 = tc::smem_u32(out_layer ? Wo : Ws[l]);
+        const uint32_t idesc = tc::idesc_bf16(kRows, out_layer ? kOutMma : kH, false, false);
         for (int kk = 0; kk < in / 16; ++kk)
           tc::mma_bf16(tmem, tc::smem_desc(a0 + kk * 2 * kLbo, kLbo, sbo),
                        tc::smem_desc(b0 + kk * 2 * kLbo, kLbo, sbo), idesc, kk > 0 ? 1u : 0u);
@@ -324,74 +365,47 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         ok = false;
         break;
       }
+      if (out_layer) break;
+      // z = acc + b rounded to BF16 (stored for the adjoint), a = act(z) in BF16
+      // -> the next layer's operand tile
       __nv_bfloat16* z_out = zb + z_row_base(zrows, l, tile, t);
+      const float* bl = bias + l * kH;
 #pragma unroll 1
       for (int c0 = 0; c0 < kH; c0 += 32) {
         float v[32];
         tc::tmem_ld32(tmem + lane_base + c0, v);
-        const float2* b2 = reinterpret_cast<const float2*>(bias + l * kH + c0);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          float2 z2[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) z2[i] = fadd2(make_float2(v[q * 8 + 2 * i], v[q * 8 + 2 * i + 1]), b2[q * 4 + i]);
-          const uint4 zp = make_uint4(pack2(z2[0].x, z2[0].y), pack2(z2[1].x, z2[1].y), pack2(z2[2].x, z2[2].y),
-                                      pack2(z2[3].x, z2[3].y));
+          const float4 b0 = *reinterpret_cast<const float4*>(bl + c0 + q * 8);
+          const float4 b1 = *reinterpret_cast<const float4*>(bl + c0 + q * 8 + 4);
+          const float2 z0 = fadd2(make_float2(v[q * 8 + 0], v[q * 8 + 1]), make_float2(b0.x, b0.y));
+          const float2 z1 = fadd2(make_float2(v[q * 8 + 2], v[q * 8 + 3]), make_float2(b0.z, b0.w));
+          const float2 z2 = fadd2(make_float2(v[q * 8 + 4], v[q * 8 + 5]), make_float2(b1.x, b1.y));
+          const float2 z3 = fadd2(make_float2(v[q * 8 + 6], v[q * 8 + 7]), make_float2(b1.z, b1.w));
+          const uint4 zp = make_uint4(pack2(z0.x, z0.y), pack2(z1.x, z1.y), pack2(z2.x, z2.y), pack2(z3.x, z3.y));
           if (valid) *reinterpret_cast<uint4*>(z_out + (size_t)((c0 + q * 8) / 8) * kZChunk) = zp;
-          // the next layer (and the adjoint) see the BF16-rounded pre-activation
-          float zr[8], a[8];
-          unpack8(zp, zr);
-          if (act == 1) {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) a[i] = fmaxf(zr[i], 0.0f);
-          } else {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              const float2 g = gelu2(make_float2(zr[2 * i], zr[2 * i + 1]));
-              a[2 * i] = g.x;
-              a[2 * i + 1] = g.y;
-            }
-          }
-          if (l + 1 < kLayers || kOut > 1) {
-            *reinterpret_cast<uint4*>(Hs + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = pack8(a);
-          } else {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) o += wout[c0 + q * 8 + i] * a[i];
-          }
+          const uint4 ap = make_uint4(act_fwd2(act, zp.x), act_fwd2(act, zp.y), act_fwd2(act, zp.z),
+                                      act_fwd2(act, zp.w));
+          *reinterpret_cast<uint4*>(Hs + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = ap;
         }
       }
     }
     if (!ok) break;
+    // output layer [128 rows x kOutMma] in the group's TMEM columns: sigmoid(acc + b_out)
     if constexpr (kOut == 1) {
+      const float o = tc::tmem_ld1(tmem + lane_base);
       if (valid) {
-        const float s = 1.0f / (1.0f + expf(-o));
+        const float s = 1.0f / (1.0f + expf(-(o + bout[0])));
         S[row] = s;
         if (vis) signal[row] = make_float2(s, 0.0f);
       }
     } else {
-      // output layer: [128 rows x kOut] = A_{L-1} W_out^T into the group's TMEM columns
-      group_publish(bar_id);
-      if (t == 0) {
-        const uint32_t a0 = tc::smem_u32(Hs), b0 = tc::smem_u32(Wo);
-        const uint32_t idesc = tc::idesc_bf16(kRows, kOut, false, false);
-        for (int kk = 0; kk < kH / 16; ++kk)
-          tc::mma_bf16(tmem, tc::smem_desc(a0 + kk * 2 * kLbo, kLbo, kSboH),
-                       tc::smem_desc(b0 + kk * 2 * kLbo, kLbo, kSboH), idesc, kk > 0 ? 1u : 0u);
-        tc::commit(&mbar[grp]);
-      }
-      const bool got = tc::mbar_wait(&mbar[grp], phase, polls);
-      phase ^= 1u;
-      tc::fence_after_sync();
-      if (!tc::named_all(bar_id, 128, got)) {
-        ok = false;
-        break;
-      }
 #pragma unroll 1
       for (int c0 = 0; c0 < kOut; c0 += 32) {
         float v[32];
         tc::tmem_ld32(tmem + lane_base + c0, v);
 #pragma unroll
-        for (int i = 0; i < 32; ++i) v[i] = 1.0f / (1.0f + expf(-(v[i] + wout[c0 + i])));
+        for (int i = 0; i < 32; ++i) v[i] = 1.0f / (1.0f + expf(-(v[i] + bout[c0 + i])));
         if (valid)
 #pragma unroll
           for (int q = 0; q < 8; ++q)
@@ -415,15 +429,15 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
 // dynamic smem: W_l as the MN-major B operand of dA = dZ W ([n = in_l] x
 // [k = 128 outputs]) for every layer; per compute warpgroup dZ [128 rows x 128]
 // and A [128 rows x 144] (activations, then a ones column and 15 zero columns),
-// both K-major by row; the output row in fp32 (one output) or W_out as the
-// MN-major B operand of dA = dO W_out ([n = 128] x [k = kOut]) (kOut outputs).
-// TMEM columns: dW_l accumulators of (in_l + 16) columns each (last layer
-// first; with kOut outputs the first layer's bias is summed on the CUDA cores
-// and its accumulator is in_0 wide), then dW_out^T (kOut columns, lanes =
-// hidden units; kOut outputs only), then one 128-column scratch accumulator
-// for dA.  With kOut outputs every tile starts with an output step: dW_out^T +=
-// A_{L-1}^T dO and dA_{L-1} = dO W_out on the tensor cores, dO staged as a
-// K-major row tile in the dZ buffer.
+// both K-major by row; W_out as the MN-major B operand of dA = dO W_out
+// ([n = 128] x [k = kOutMma]; rows past the real outputs zero).
+// TMEM columns: dW_l accumulators of in_l (+ 16) columns each (last layer
+// first; the ones columns give db_l, except for the first layer when the
+// columns run short -- 3 hidden layers and 64 outputs -- whose bias is then
+// summed on the CUDA cores), then dW_out^T (kOutMma columns, lanes = hidden
+// units), then one 128-column scratch accumulator for dA.  Every tile starts
+// with the output step: dW_out^T += A_{L-1}^T dO and dA_{L-1} = dO W_out,
+// dO staged as a K-major row tile in the dZ buffer.
 template <int kLayers, int act, int kOut>
 __global__ void __launch_bounds__(kBwdThreads, 1)
 mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
@@ -432,21 +446,27 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                          const float* __restrict__ S, const float* __restrict__ dL_dsignal,
                          float* __restrict__ dX0, float* __restrict__ dparams, ImageHeader* __restrict__ hdr,
                          uint32_t polls) {
+  constexpr int kOutMma = out_mma_width(kOut);
+  constexpr bool kBias0Cuda = bwd_bias0_on_cuda_cores(kLayers, kOut);
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar_ready[kBwdGroups];
   __shared__ __align__(8) uint64_t bar_done[kBwdGroups];
   __shared__ __align__(8) uint64_t bar_free;
   __shared__ __align__(8) uint64_t bar_drain;
+  __shared__ __align__(8) uint64_t bar_z[kBwdGroups];   // a pre-activation slab has landed
+  __shared__ __align__(8) uint64_t bar_afree[kBwdGroups];  // a step's MMAs reading the activation tile are done
   __shared__ uint32_t tbase;
   __shared__ int s_fail;
-  // one output: dw_out[128], db_out; kOut outputs: db_out[kOut], db_0[128]
-  constexpr int kRed = kOut == 1 ? kH + 1 : kOut + kH;
+  // db_out[kOut], then (kBias0Cuda) db_0[128]
+  constexpr int kRed = kOut + (kBias0Cuda ? kH : 0);
   __shared__ float s_red[kRed];
-  constexpr bool kMulti = kOut > 1;
-  constexpr uint32_t kSboO = (uint32_t)(kOut / 8) * 128u;   // [rows x kOut] K-major / W_out MN-major
+  constexpr uint32_t kSboO = (uint32_t)(kOutMma / 8) * 128u;   // [rows x kOutMma] K-major / W_out MN-major
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int grp = tid >> 7;   // compute warpgroup 0..kBwdGroups-1; kBwdGroups = the MMA warp
-  const int t = tid & 127;
+  const int grp = tid / kBwdGroupThreads;   // compute group 0..kBwdGroups-1; kBwdGroups = the MMA warp
+  const int t = tid % kBwdGroupThreads;
+  const int r = t & 127;                    // the thread's row of the tile (its TMEM lane)
+  const int hf = t >> 7;                    // which half of the row's columns (uniform per warp)
+  constexpr int kHc = kH / kBwdHalves;      // columns per thread
   constexpr size_t kGroupBytes = (size_t)kRows * kH * 2 + (size_t)kRows * (kH + 16) * 2;
   unsigned char* Wb[kLayers];
   size_t off = 0;
@@ -456,17 +476,18 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   }
   unsigned char* const groups = smem + off;
   off += kBwdGroups * kGroupBytes;
-  float* wout = reinterpret_cast<float*>(smem + off);   // one output: w_out[128]
-  off += (size_t)kH * sizeof(float);
-  unsigned char* const Wo = smem + off;                 // kOut outputs: W_out MN-major
+  unsigned char* const Wo = smem + off;
 
+  // offsets in the flat parameters of W_l and b_l (l == kLayers: the output
+  // layer), recomputed where needed rather than held in registers
+  auto woff = [](int l) -> size_t {
+    return l == 0 ? 0 : (size_t)(kFin * kH + kH) + (size_t)(l - 1) * (kH * kH + kH);
+  };
+  auto boff = [&](int l) -> size_t { return woff(l) + (size_t)kH * (l == kLayers ? kOut : (l == 0 ? kFin : kH)); };
   // W_l [out][in] -> MN-major B operand (n = in, k = out), once per CTA
-  size_t poff = 0;
-  size_t woff[kLayers + 1], boff[kLayers + 1];
   for (int l = 0; l < kLayers; ++l) {
     const int in = l == 0 ? kFin : kH;
-    woff[l] = poff;
-    const float* W = params + poff;
+    const float* W = params + woff(l);
     for (int c = tid; c < kH * (in / 8); c += blockDim.x) {
       const int k = c / (in / 8), nc = c % (in / 8);   // k = output row of W, nc = group of 8 inputs
       float v[8];
@@ -474,37 +495,31 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
       for (int i = 0; i < 8; ++i) v[i] = W[(size_t)k * in + nc * 8 + i];
       *reinterpret_cast<uint4*>(Wb[l] + tc::mnmajor_off(nc * 8, k, kLbo, kSboH)) = pack8(v);
     }
-    poff += (size_t)kH * in;
-    boff[l] = poff;
-    poff += kH;
   }
-  woff[kLayers] = poff;
-  boff[kLayers] = poff + (size_t)kOut * kH;
-  if constexpr (kMulti) {
-    for (int c = tid; c < kOut * (kH / 8); c += blockDim.x) {
-      const int k = c / (kH / 8), nc = c % (kH / 8);   // k = output row of W_out, nc = group of 8 hidden units
-      float v[8];
+  const size_t poff = woff(kLayers);
+  for (int c = tid; c < kOutMma * (kH / 8); c += blockDim.x) {
+    const int k = c / (kH / 8), nc = c % (kH / 8);   // k = output row of W_out, nc = group of 8 hidden units
+    float v[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) v[i] = params[poff + (size_t)k * kH + nc * 8 + i];
-      *reinterpret_cast<uint4*>(Wo + tc::mnmajor_off(nc * 8, k, kLbo, kSboO)) = pack8(v);
-    }
-  } else {
-    for (int j = tid; j < kH; j += blockDim.x) wout[j] = params[woff[kLayers] + j];
+    for (int i = 0; i < 8; ++i) v[i] = k < kOut ? params[poff + (size_t)k * kH + nc * 8 + i] : 0.0f;
+    *reinterpret_cast<uint4*>(Wo + tc::mnmajor_off(nc * 8, k, kLbo, kSboO)) = pack8(v);
   }
   for (int j = tid; j < kRed; j += blockDim.x) s_red[j] = 0.0f;
   unsigned char* const dZ = groups + (size_t)(grp < kBwdGroups ? grp : 0) * kGroupBytes;
   unsigned char* const Ab = dZ + (size_t)kRows * kH * 2;
-  if (grp < kBwdGroups) {   // the constant ones column (db) of the activation tile
+  if (grp < kBwdGroups && hf == 0) {   // the constant ones column (db) of the activation tile
     const uint4 one = make_uint4(pack2(1.0f, 0.0f), 0u, 0u, 0u);
-    *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kH, kLbo, kSboA)) = one;
-    *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kH + 8, kLbo, kSboA)) = make_uint4(0u, 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(Ab + slab_off(r, kH)) = one;
+    *reinterpret_cast<uint4*>(Ab + slab_off(r, kH + 8)) = make_uint4(0u, 0u, 0u, 0u);
   }
   if (tid == 0) {
     for (int q = 0; q < kBwdGroups; ++q) {
-      tc::mbar_init(&bar_ready[q], 128);
+      tc::mbar_init(&bar_ready[q], kBwdGroupThreads);
       tc::mbar_init(&bar_done[q], 1);
+      tc::mbar_init(&bar_z[q], 1);
+      tc::mbar_init(&bar_afree[q], 1);
     }
-    tc::mbar_init(&bar_free, 128);
+    tc::mbar_init(&bar_free, kBwdGroupThreads);
     tc::mbar_init(&bar_drain, 1);
     s_fail = 0;
   }
@@ -514,21 +529,14 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = tbase;
-  // the first layer's accumulator has the ones columns unless kOut outputs need the room
-  auto dw_width = [](int l) { return (l == 0 ? kFin : kH) + ((l == 0 && kMulti) ? 0 : 16); };
-  uint32_t dwcol[kLayers];
-  uint32_t col = 0;
-  for (int l = kLayers - 1; l >= 0; --l) {
-    dwcol[l] = col;
-    col += dw_width(l);
-  }
-  const uint32_t dwo_col = col;                       // kOut outputs: dW_out^T
-  const uint32_t scratch = col + (kMulti ? kOut : 0);  // 3 layers: 336 (+ 0) or 320 + 64 = 384; + 128 <= 512
+  // TMEM columns: dW_l (last layer first), dW_out^T, the dA scratch
+  auto dw_width = [](int l) { return (l == 0 ? kFin : kH) + ((l == 0 && kBias0Cuda) ? 0 : 16); };
+  auto dwcol = [](int l) -> uint32_t { return (uint32_t)(kLayers - 1 - l) * (kH + 16); };
+  constexpr uint32_t dwo_col = (uint32_t)(kLayers - 1) * (kH + 16) + kFin + (kBias0Cuda ? 0 : 16);
+  constexpr uint32_t scratch = dwo_col + kOutMma;   // + 128 <= 512 (bwd_bias0_on_cuda_cores)
   const size_t ntiles = (rows + kRows - 1) / kRows;
   const size_t zrows = ntiles * kRows;   // pre-activation rows, whole tiles
   const size_t tile_stride = (size_t)gridDim.x * kBwdGroups;
-  // steps per tile, from the top: the output step (kOut outputs), then hidden layers L-1 .. 0
-  constexpr int kTop = kMulti ? kLayers : kLayers - 1;
 
   if (grp == kBwdGroups) {
     // ---- MMA warp: one thread issues every MMA of the CTA, in the order
@@ -541,9 +549,11 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
       uint32_t n_da = 0;
       bool ok = true;
       for (size_t base = (size_t)blockIdx.x * kBwdGroups; base < ntiles && ok; base += tile_stride) {
-        for (int l = kTop; l >= 0 && ok; --l) {
-          const bool out_step = kMulti && l == kLayers;
+#pragma unroll 1
+        for (int l = kLayers; l >= 0 && ok; --l) {
+          const bool out_step = l == kLayers;
           const int in = l == 0 ? kFin : kH;
+#pragma unroll 1
           for (int q = 0; q < kBwdGroups; ++q) {
             if (base + q >= ntiles) break;
             if (!tc::mbar_wait(&bar_ready[q], ph_ready[q], polls)) {
@@ -557,23 +567,27 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
             if (out_step) {
               // dW_out^T += A_{L-1}^T dO: A operand A^T (M = hidden units, K = rows) and B operand
               // dO^T (N = outputs, K = rows), MN-major views of the row tiles
-              const uint32_t id_o = tc::idesc_bf16(kH, kOut, true, true);
+              const uint32_t id_o = tc::idesc_bf16(kH, kOutMma, true, true);
+#pragma unroll 1
               for (int kk = 0; kk < kRows / 16; ++kk)
-                tc::mma_bf16(tmem + dwo_col, tc::smem_desc(aq + kk * 2 * kSboA, kSboA, 128u),
+                tc::mma_bf16(tmem + dwo_col, tc::smem_desc(aq + kk * 256u, 128u, kChunkA),
                              tc::smem_desc(zq + kk * 2 * kSboO, kSboO, 128u), id_o,
                              (!first[kLayers] || kk > 0) ? 1u : 0u);
               first[kLayers] = false;
             } else {
               // dW_l | db_l += dZ^T [A | 1]: A operand dZ^T (M = outputs, K = rows) and
               // B operand [A | 1]^T (N = in (+ 16), K = rows), both MN-major views of the
-              // row-major tiles (core-matrix stride 128 B along M/N, one row group along K)
+              // row tiles
               const uint32_t id_w = tc::idesc_bf16(kH, dw_width(l), true, true);
+#pragma unroll 1
               for (int kk = 0; kk < kRows / 16; ++kk)
-                tc::mma_bf16(tmem + dwcol[l], tc::smem_desc(zq + kk * 2 * kSboH, kSboH, 128u),
-                             tc::smem_desc(aq + kk * 2 * kSboA, kSboA, 128u), id_w,
+                tc::mma_bf16(tmem + dwcol(l), tc::smem_desc(zq + kk * 2 * kSboH, kSboH, 128u),
+                             tc::smem_desc(aq + kk * 256u, 128u, kChunkA), id_w,
                              (!first[l] || kk > 0) ? 1u : 0u);
               first[l] = false;
             }
+            // the activation tile is read: the group may stage the next slab into it
+            tc::commit(&bar_afree[q]);
             // dA = dZ_l W_l (or dO W_out) into the scratch, once its previous reader has drained it
             if (n_da > 0) {
               if (!tc::mbar_wait(&bar_free, (n_da - 1) & 1u, polls)) {
@@ -585,12 +599,14 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
             if (out_step) {
               const uint32_t id_x = tc::idesc_bf16(kRows, kH, false, true);
               const uint32_t wo = tc::smem_u32(Wo);
-              for (int kk = 0; kk < kOut / 16; ++kk)
+#pragma unroll 1
+              for (int kk = 0; kk < kOutMma / 16; ++kk)
                 tc::mma_bf16(tmem + scratch, tc::smem_desc(zq + kk * 2 * kLbo, kLbo, kSboO),
                              tc::smem_desc(wo + kk * 2 * kLbo, kLbo, kSboO), id_x, kk > 0 ? 1u : 0u);
             } else {
               const uint32_t id_x = tc::idesc_bf16(kRows, in, false, true);
               const uint32_t wb = tc::smem_u32(Wb[l]);
+#pragma unroll 1
               for (int kk = 0; kk < kH / 16; ++kk)
                 tc::mma_bf16(tmem + scratch, tc::smem_desc(zq + kk * 2 * kLbo, kLbo, kSboH),
                              tc::smem_desc(wb + kk * 2 * kLbo, kLbo, kSboH), id_x, kk > 0 ? 1u : 0u);
@@ -603,33 +619,53 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
       if (!ok) s_fail = 1;
     }
   } else {
-    // ---- compute warpgroup
+    // ---- compute group: thread (r, hf) handles row r, columns [hf kHc, hf kHc + kHc)
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
     const uint32_t bar_id = 1u + (uint32_t)grp;
-    uint32_t ph_done = 0;
-    bool ok = true;
-    for (size_t tile = (size_t)blockIdx.x * kBwdGroups + grp; tile < ntiles && ok; tile += tile_stride) {
-      const size_t row0 = tile * kRows, row = row0 + t;
-      const bool valid = row < rows;
+    const int cb = hf * kHc;
+    uint32_t ph_done = 0, ph_z = 0;
+    bool ok = true, z_pending = false;
+    // one pre-activation slab (layer l of a tile, 32 KB) -> the activation
+    // tile, by the group's first thread once the MMAs reading the tile are done
+    auto stage_slab = [&](int l, size_t tl) {
       if (t == 0) {
-        // into L2 ahead of use: this tile's remaining pre-activation slabs (one
-        // contiguous 32 KB range per layer), then the next tile's first inputs
-        for (int l = 0; l + 1 < kLayers; ++l) tc::prefetch_l2(zb + z_row_base(zrows, l, tile, 0), kRows * kH * 2);
-        const size_t nt = tile + tile_stride;
-        if (nt < ntiles) {
-          const size_t r1 = nt * kRows;
-          const uint32_t n1 = (uint32_t)(rows - r1 < (size_t)kRows ? rows - r1 : (size_t)kRows);
-          tc::prefetch_l2(zb + z_row_base(zrows, kLayers - 1, nt, 0), kRows * kH * 2);
-          tc::prefetch_l2(S + r1 * kOut, n1 * 4 * kOut);
-          tc::prefetch_l2(radii + r1, n1 * 4);
-          tc::prefetch_l2(dL_dsignal + (kMulti ? r1 * kOut : 2 * r1), n1 * (kMulti ? 4 * kOut : 8));
-        }
+        tc::mbar_arrive_expect_tx(&bar_z[grp], kRows * kH * 2);
+        tc::bulk_load(Ab, zb + z_row_base(zrows, l, tl, 0), kRows * kH * 2, &bar_z[grp]);
+        z_pending = true;
+      }
+    };
+    if ((size_t)blockIdx.x * kBwdGroups + grp < ntiles) stage_slab(kLayers - 1, (size_t)blockIdx.x * kBwdGroups + grp);
+    for (size_t tile = (size_t)blockIdx.x * kBwdGroups + grp; tile < ntiles && ok; tile += tile_stride) {
+      const size_t row0 = tile * kRows, row = row0 + r;
+      const bool valid = row < rows;
+      if (t == 0 && tile + tile_stride < ntiles) {
+        // the next tile's pre-activation slabs, outputs, radii and incoming gradients into L2
+        for (int l = kLayers - 1; l >= 0; --l)
+          tc::prefetch_l2(zb + z_row_base(zrows, l, tile + tile_stride, 0), kRows * kH * 2);
+        const size_t r1 = (tile + tile_stride) * kRows;
+        const uint32_t n1 = (uint32_t)(rows - r1 < (size_t)kRows ? rows - r1 : (size_t)kRows);
+        tc::prefetch_l2(S + r1 * kOut, n1 * 4 * kOut);
+        tc::prefetch_l2(radii + r1, n1 * 4);
+        tc::prefetch_l2(dL_dsignal + (kOut > 1 ? r1 * kOut : 2 * r1), n1 * (kOut > 1 ? 4 * kOut : 8));
       }
       const bool vis = valid && radii[row] > 0;
-      if constexpr (kMulti) {
-        // dO = dL/dfeatures * s (1 - s) -> the dO row tile (BF16) in the dZ buffer; db_out
+      // dO = dL/dsignal * s (1 - s) -> the dO row tile (BF16) in the dZ buffer; db_out sums it in FP32
+      if constexpr (kOut == 1) {
+        if (hf == 0) {
+          const float s = valid ? S[row] : 0.0f;
+          const float dO = vis ? dL_dsignal[2 * row] * s * (1.0f - s) : 0.0f;
+          *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(r, 0, kLbo, kSboO)) =
+              make_uint4(pack2(dO, 0.0f), 0u, 0u, 0u);
+          *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(r, 8, kLbo, kSboO)) = make_uint4(0u, 0u, 0u, 0u);
+          float dsum = dO;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+          if (lane == 0) atomicAdd(&s_red[0], dsum);
+        }
+      } else {
+        constexpr int kOc = kOut / kBwdHalves;   // outputs per thread (a multiple of 32)
 #pragma unroll 1
-        for (int c0 = 0; c0 < kOut; c0 += 32) {
+        for (int c0 = hf * kOc; c0 < hf * kOc + kOc; c0 += 32) {
           float d[32];
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
@@ -645,141 +681,127 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
           }
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboO)) = pack8(d + q * 8);
+            *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(r, c0 + q * 8, kLbo, kSboO)) = pack8(d + q * 8);
           const float sum = warp_transpose_sum32(d, lane);
           atomicAdd(&s_red[c0 + lane], sum);
         }
-      } else {
-        // output layer: dO, its weight gradient (reduced over the warp's rows), dZ of the last hidden layer
-        const float s = valid ? S[row] : 0.0f;
-        const float dO = vis ? dL_dsignal[2 * row] * s * (1.0f - s) : 0.0f;
-        const __nv_bfloat16* zl = zb + z_row_base(zrows, kLayers - 1, tile, t);
-#pragma unroll 1
-        for (int c0 = 0; c0 < kH; c0 += 32) {
-          uint4 zq[4];   // a 32-column chunk of the row in flight at once
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            zq[q] = valid ? *reinterpret_cast<const uint4*>(zl + (size_t)(c0 / 8 + q) * kZChunk)
-                          : make_uint4(0u, 0u, 0u, 0u);
-          float red[32];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            float z[8], dz[8];
-            unpack8(zq[q], z);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-              if (i & 1) continue;
-              float2 a, d;
-              act_and_grad2(act, make_float2(z[i], z[i + 1]), a, d);
-              red[q * 8 + i] = dO * a.x;
-              red[q * 8 + i + 1] = dO * a.y;
-              dz[i] = dO * wout[c0 + q * 8 + i] * d.x;
-              dz[i + 1] = dO * wout[c0 + q * 8 + i + 1] * d.y;
-            }
-            *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = pack8(dz);
-          }
-          const float sum = warp_transpose_sum32(red, lane);
-          atomicAdd(&s_red[c0 + lane], sum);
-        }
-        float dsum = dO;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
-        if (lane == 0) atomicAdd(&s_red[kH], dsum);
       }
-      for (int l = kTop; l >= 0; --l) {
-        // act'(Z_{l-1}) of this row, kept for dZ_{l-1} after the MMAs as FP16 pairs
-        // (nine warps leave 168 registers a thread; the FP16 rounding, 2^-11
-        // relative, sits below the BF16 rounding of dZ that follows)
-        __half2 ad[kH / 2];
+#pragma unroll 1
+      for (int l = kLayers; l >= 0; --l) {
+        // act'(Z_{l-1}) of this row's columns as BF16 pairs, kept for dZ_{l-1}
+        // after the MMAs
+        uint32_t ad[kHc / 2];
         // A_{l-1}: features (l == 0) or act(Z_{l-1}); the ones column sits at `in`
         if (l == 0) {
-          int r, g;
-          row_pair(row0, t, P, r, g);
-          float x[kFin];
-          pair_features(means3D, rx_pos, g, r, vis, x);
+          if (hf == 0) {
+            int rr, g;
+            row_pair(row0, r, P, rr, g);
+            float x[kFin];
+            pair_features(means3D, rx_pos, g, rr, vis, x);
 #pragma unroll
-          for (int kc = 0; kc < kFin / 8; ++kc)
-            *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kc * 8, kLbo, kSboA)) = pack8(x + kc * 8);
-          if constexpr (!kMulti) {
-            *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kFin, kLbo, kSboA)) =
-                make_uint4(pack2(1.0f, 0.0f), 0u, 0u, 0u);
-            *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, kFin + 8, kLbo, kSboA)) = make_uint4(0u, 0u, 0u, 0u);
+            for (int kc = 0; kc < kFin / 8; ++kc)
+              *reinterpret_cast<uint4*>(Ab + slab_off(r, kc * 8)) = pack8(x + kc * 8);
+          } else if constexpr (!kBias0Cuda) {
+            *reinterpret_cast<uint4*>(Ab + slab_off(r, kFin)) = make_uint4(pack2(1.0f, 0.0f), 0u, 0u, 0u);
+            *reinterpret_cast<uint4*>(Ab + slab_off(r, kFin + 8)) = make_uint4(0u, 0u, 0u, 0u);
           }
         } else {
-          const __nv_bfloat16* zp = zb + z_row_base(zrows, l - 1, tile, t);
+          // Z_{l-1} of the tile, staged in the activation tile by a bulk copy:
+          // activate it in place (rows past the end read as zero)
+          const bool zgot = tc::mbar_wait(&bar_z[grp], ph_z, polls);
+          if (zgot) {
+            ph_z ^= 1u;
+            z_pending = false;
+          }
+          if (!tc::named_all(bar_id, kBwdGroupThreads, zgot)) {
+            ok = false;
+            break;
+          }
 #pragma unroll
-          for (int c0 = 0; c0 < kH; c0 += 8) {
-            float z[8], a[8];
-            if (valid) unpack8(*reinterpret_cast<const uint4*>(zp + (size_t)(c0 / 8) * kZChunk), z);
-            else
+          for (int k = 0; k < kHc / 8; ++k) {
+            uint4* cell = reinterpret_cast<uint4*>(Ab + slab_off(r, cb + 8 * k));
+            const uint4 zq = valid ? *cell : make_uint4(0u, 0u, 0u, 0u);
+            const uint32_t zk[4] = {zq.x, zq.y, zq.z, zq.w};
+            uint32_t a[4];
 #pragma unroll
-              for (int i = 0; i < 8; ++i) z[i] = 0.0f;
-            float d[8];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              float2 a2, d2;
-              act_and_grad2(act, make_float2(z[2 * i], z[2 * i + 1]), a2, d2);
-              a[2 * i] = a2.x;
-              a[2 * i + 1] = a2.y;
-              d[2 * i] = d2.x;
-              d[2 * i + 1] = d2.y;
-            }
-#pragma unroll
-            for (int i = 0; i < 4; ++i) ad[c0 / 2 + i] = __floats2half2_rn(d[2 * i], d[2 * i + 1]);
-            *reinterpret_cast<uint4*>(Ab + tc::kmajor_off(t, c0, kLbo, kSboA)) = pack8(a);
+            for (int j = 0; j < 4; ++j) act_bwd2(act, zk[j], a[j], ad[4 * k + j]);
+            *cell = make_uint4(a[0], a[1], a[2], a[3]);
           }
         }
         // hand dZ_l (or dO) and A_{l-1} to the MMA warp
         tc::fence_async_smem();
         tc::mbar_arrive(&bar_ready[grp]);
+        // once the weight-gradient MMA has read the activation tile (before dA is
+        // computed), the group's first thread stages the slab the next step
+        // activates into it
+        bool afree = true;
+        if (t == 0 && (l >= 2 || (l == 0 && tile + tile_stride < ntiles))) {
+          afree = tc::mbar_wait(&bar_afree[grp], ph_done, polls);
+          if (afree) {
+            if (l >= 2) stage_slab(l - 2, tile);
+            else stage_slab(kLayers - 1, tile + tile_stride);
+          }
+        }
         const bool got = tc::mbar_wait(&bar_done[grp], ph_done, polls);
         ph_done ^= 1u;
         tc::fence_after_sync();
-        if (!tc::named_all(bar_id, 128, got)) {
+        if (!tc::named_all(bar_id, kBwdGroupThreads, got && afree)) {
           ok = false;
           break;
         }
         if (l == 0) {
-          float v[32];
-          tc::tmem_ld32(tmem + lane_base + scratch, v);
-          tc::fence_before_sync();
-          tc::mbar_arrive(&bar_free);
-          if (valid)
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-              *reinterpret_cast<float4*>(dX0 + row * kFin + q * 4) =
-                  make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-        } else {
-          // dZ_{l-1} = dA_{l-1} * act'(Z_{l-1}); the MMAs that read dZ_l (or dO) are done
-#pragma unroll
-          for (int c0 = 0; c0 < kH; c0 += 32) {
+          if (hf == 0) {
             float v[32];
-            tc::tmem_ld32(tmem + lane_base + scratch + c0, v);
-            if (c0 + 32 == kH) {
+            tc::tmem_ld32(tmem + lane_base + scratch, v);
+            tc::fence_before_sync();
+            tc::mbar_arrive(&bar_free);
+            if (valid)
+#pragma unroll
+              for (int q = 0; q < 8; ++q)
+                *reinterpret_cast<float4*>(dX0 + row * kFin + q * 4) =
+                    make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          } else {
+            tc::fence_before_sync();
+            tc::mbar_arrive(&bar_free);
+          }
+        } else {
+          // dZ_{l-1} = BF16(dA_{l-1}) * act'(Z_{l-1}) in BF16, 16 columns at a time; the MMAs
+          // that read dZ_l (or dO) are done
+#pragma unroll
+          for (int c = 0; c < kHc / 16; ++c) {
+            const int c0 = cb + 16 * c;
+            float v[16];
+            tc::tmem_ld16(tmem + lane_base + scratch + c0, v);
+            if (c + 1 == kHc / 16) {
               tc::fence_before_sync();
               tc::mbar_arrive(&bar_free);
             }
+            uint32_t p[8];
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              const float2 d = __half22float2(ad[c0 / 2 + i]);
-              v[2 * i] *= d.x;
-              v[2 * i + 1] *= d.y;
-            }
+            for (int i = 0; i < 8; ++i) p[i] = bf2_mul(pack2(v[2 * i], v[2 * i + 1]), ad[8 * c + i]);
+            *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(r, c0, kLbo, kSboH)) = make_uint4(p[0], p[1], p[2], p[3]);
+            *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(r, c0 + 8, kLbo, kSboH)) =
+                make_uint4(p[4], p[5], p[6], p[7]);
+            if (kBias0Cuda && l == 1) {
+              // db_0 sums the BF16 dZ_0 the MMAs see (16 columns: half a warp transpose)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const uint4 p = pack8(v + q * 8);
-              *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(t, c0 + q * 8, kLbo, kSboH)) = p;
-              if (kMulti && l == 1) unpack8(p, v + q * 8);   // db_0 sums the BF16 dZ_0 the MMAs see
-            }
-            if (kMulti && l == 1) {
-              const float sum = warp_transpose_sum32(v, lane);
-              atomicAdd(&s_red[kOut + c0 + lane], sum);
+              for (int i = 0; i < 8; ++i) {
+                const float2 f = bf2_unpack(p[i]);
+                v[2 * i] = f.x;
+                v[2 * i + 1] = f.y;
+              }
+              const float sum = warp_transpose_sum16(v, lane);
+              if (lane < 16) atomicAdd(&s_red[kOut + c0 + lane], sum);
             }
           }
         }
       }
     }
-    if (!ok && t == 0) s_fail = 1;
+    if (!ok && t == 0) {
+      s_fail = 1;
+      // a slab copy still in flight lands before the CTA's shared memory goes away
+      if (z_pending) tc::mbar_wait(&bar_z[grp], ph_z, kPolls);
+    }
   }
   __syncthreads();
   tc::fence_after_sync();
@@ -787,40 +809,42 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   // (layer, 32-column chunk) items are split over the compute warpgroups
   if (!s_fail && grp < kBwdGroups) {
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+    const int part = grp * kBwdHalves + hf, nparts = kBwdGroups * kBwdHalves;
     int item = 0;
     for (int l = 0; l < kLayers; ++l) {
       const int in = l == 0 ? kFin : kH;
-      const int ncols = (l == 0 && kMulti) ? in : in + 1;   // weights, then the bias column
+      const int ncols = (l == 0 && kBias0Cuda) ? in : in + 1;   // weights, then the bias column
 #pragma unroll 1
       for (int c0 = 0; c0 < ncols; c0 += 32, ++item) {
-        if (item % kBwdGroups != grp) continue;
+        if (item % nparts != part) continue;
         float v[32];
-        tc::tmem_ld32(tmem + lane_base + dwcol[l] + c0, v);
+        tc::tmem_ld32(tmem + lane_base + dwcol(l) + c0, v);
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
           const int n = c0 + i;
-          if (n < in) atomicAdd(&dparams[woff[l] + (size_t)t * in + n], v[i]);
-          else if (n == in && n < ncols) atomicAdd(&dparams[boff[l] + t], v[i]);
+          if (n < in) atomicAdd(&dparams[woff(l) + (size_t)r * in + n], v[i]);
+          else if (n == in && n < ncols) atomicAdd(&dparams[boff(l) + r], v[i]);
         }
       }
     }
-    if constexpr (kMulti) {
-      // dW_out^T: lane = hidden unit t, column = output
+    // dW_out^T: lane = hidden unit t, column = output
+    if constexpr (kOut == 1) {
+      if (item % nparts == part) atomicAdd(&dparams[woff(kLayers) + r], tc::tmem_ld1(tmem + lane_base + dwo_col));
+      ++item;
+    } else {
 #pragma unroll 1
       for (int c0 = 0; c0 < kOut; c0 += 32, ++item) {
-        if (item % kBwdGroups != grp) continue;
+        if (item % nparts != part) continue;
         float v[32];
         tc::tmem_ld32(tmem + lane_base + dwo_col + c0, v);
 #pragma unroll
-        for (int i = 0; i < 32; ++i) atomicAdd(&dparams[woff[kLayers] + (size_t)(c0 + i) * kH + t], v[i]);
+        for (int i = 0; i < 32; ++i) atomicAdd(&dparams[woff(kLayers) + (size_t)(c0 + i) * kH + r], v[i]);
       }
-      if (grp == 0) {
-        for (int j = t; j < kOut; j += 128) atomicAdd(&dparams[boff[kLayers] + j], s_red[j]);
-        for (int j = t; j < kH; j += 128) atomicAdd(&dparams[boff[0] + j], s_red[kOut + j]);
-      }
-    } else {
-      if (grp == 0)
-        for (int j = t; j <= kH; j += 128) atomicAdd(&dparams[j < kH ? woff[kLayers] + j : boff[kLayers]], s_red[j]);
+    }
+    if (grp == 0) {
+      for (int j = t; j < kOut; j += kBwdGroupThreads) atomicAdd(&dparams[boff(kLayers) + j], s_red[j]);
+      if constexpr (kBias0Cuda)
+        for (int j = t; j < kH; j += kBwdGroupThreads) atomicAdd(&dparams[boff(0) + j], s_red[kOut + j]);
     }
   }
   if (s_fail && tid == 0 && hdr) atomic_or_error(hdr, kErrMlpWait);
@@ -835,17 +859,46 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   if (warp == 0) tc::tmem_dealloc(tmem, 512);
 }
 
+// ---- the epilogue's activation as a table ----------------------------------
+// Every BF16 input z (bit pattern i), through the kernels' own packed
+// arithmetic: out [3][2][65536] = {act (forward), act (adjoint), act'} x
+// {low lane, high lane}; thread i puts z = i in the low lane and z = 65535 - i
+// in the high lane of the same register, so both lanes of every input are
+// produced and can be compared.
+__global__ void bf16_act_table_kernel(int act, uint16_t* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 65536u) return;
+  const uint32_t j = 65535u - i;
+  const uint32_t z = i | (j << 16);
+  // the forward's call and the adjoint's
+  const uint32_t af = act == 1 ? act_fwd2(1, z) : act_fwd2(2, z);
+  uint32_t a, d;
+  if (act == 1) act_bwd2(1, z, a, d);
+  else act_bwd2(2, z, a, d);
+  const uint32_t v[3] = {af, a, d};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    out[(size_t)(2 * k) * 65536 + i] = (uint16_t)(v[k] & 0xFFFFu);
+    out[(size_t)(2 * k + 1) * 65536 + j] = (uint16_t)(v[k] >> 16);
+  }
+}
+
+cudaError_t launch_bf16_act_table(int act, uint16_t* out, cudaStream_t s) {
+  bf16_act_table_kernel<<<256, 256, 0, s>>>(act, out);
+  return cudaGetLastError();
+}
+
 // ---- launchers ------------------------------------------------------------------
 
 size_t mlp_bf16_forward_smem(int layers, int out) {
   const size_t base = (size_t)kH * kFin * 2 + (size_t)(layers - 1) * kH * kH * 2 +
                       (size_t)kFwdGroups * kRows * kH * 2 + (size_t)(layers * kH + kH + 4) * sizeof(float);
-  return out > 1 ? (base + 127) / 128 * 128 + (size_t)out * kH * 2 : base;
+  return (base + 127) / 128 * 128 + (size_t)out_mma_width(out) * kH * 2;
 }
 size_t mlp_bf16_backward_smem(int layers, int out) {
   return (size_t)kFin * kH * 2 + (size_t)(layers - 1) * kH * kH * 2 +
-         (size_t)kBwdGroups * ((size_t)kRows * kH * 2 + (size_t)kRows * (kH + 16) * 2) + (size_t)kH * sizeof(float) +
-         (out > 1 ? (size_t)out * kH * 2 : 0);
+         (size_t)kBwdGroups * ((size_t)kRows * kH * 2 + (size_t)kRows * (kH + 16) * 2) +
+         (size_t)out_mma_width(out) * kH * 2;
 }
 
 template <int L, int A, int O>

@@ -66,6 +66,7 @@ _SIGS = {
     "gsparc_shared_mlp_workspace_floats": (_c_size, [_c_int] * 6),
     "gsparc_shared_mlp_forward": (_c_int, [_c_int] * 7 + [_vp] * 7),
     "gsparc_shared_mlp_backward": (_c_int, [_c_int] * 7 + [_vp] * 10),
+    "gsparc_shared_mlp_bf16_act_table": (_c_int, [_c_int, _vp, _vp]),
     "gsparc_splat_loss_scratch_floats": (_c_size, [_c_int, _c_int, _c_int, _c_int]),
     "gsparc_splat_loss": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_float, _c_float, _c_float, _c_float,
                                    _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -115,3 +115,19 @@ class SharedMLP:
             int(P), int(R), *self._spec(), ptr(means3D), ptr(rx_pos), ptr(params), ptr(geom),
             ptr(image) if image is not None else None, ptr(work), ptr(dsignal), ptr(dparams), ptr(dmeans3D),
             stream_of(dev)))
+
+
+def bf16_act_table(act, device="cuda"):
+    """The BF16 path's activation for every BF16 input, as its kernels
+    evaluate it: (a_forward, a_adjoint, a') float32 tensors of 65,536 entries,
+    entry i for the input whose BF16 bit pattern is i, each from the low lane
+    of a packed pair; raises if the high lane ever differs."""
+    out = torch.empty(6 * 65536, dtype=torch.int16, device=device)
+    check("shared_mlp_bf16_act_table",
+          _lib.lib().gsparc_shared_mlp_bf16_act_table(ACTS[act], ptr(out), stream_of(torch.device(device))))
+    t = out.view(3, 2, 65536)
+    if not torch.equal(t[:, 0], t[:, 1]):
+        raise RuntimeError("packed BF16 activation: the two lanes disagree")
+    bits = t[:, 0].to(torch.int32) << 16
+    f = bits.view(torch.float32)
+    return f[0].clone(), f[1].clone(), f[2].clone()

@@ -239,8 +239,8 @@ GSPARC_API int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float
  * backward pass emission_mlps = dL_demission_mlps = NULL and follow
  * gsparc_rasterize_backward with gsparc_shared_mlp_backward.
  * params: flat fp32, per layer W [out, in] row-major then b [out].
- * workspace: gsparc_shared_mlp_workspace_floats floats; the forward keeps
- * what the backward needs there.
+ * workspace: gsparc_shared_mlp_workspace_floats floats (256-byte aligned for
+ * GSPARC_MLP_BF16); the forward keeps what the backward needs there.
  * out: 1 (the signal of gsparc_rasterize_render), or up to 64 amplitude
  * channels for gsparc_rasterize_render_channels: then the first R*P*out floats
  * of the workspace hold features [R,P,out] = sigmoid(outputs) after the forward
@@ -248,9 +248,11 @@ GSPARC_API int gsparc_ssim_backward(int B, int CH, int H, int W, float C1, float
  * precision GSPARC_MLP_FP32: SIMT FP32 layers (any width 8..256, 1-6
  * layers; width 64 with one output and 1-2 layers runs fused kernels).
  * GSPARC_MLP_BF16: BF16 operands on the tcgen05 tensor cores with FP32
- * accumulation (width 128, 1-3 layers, one output); the forward and the
- * backward are one fused kernel each.  image_state (optional) receives the error bit
- * of a bounded tensor-core wait that gave up. */
+ * accumulation (width 128, 1-3 layers, 1 or 64 outputs); the forward and the
+ * backward are one fused kernel each, their epilogues in packed BF16
+ * arithmetic (GELU in the tanh form with BF16 coefficients fitted to the erf
+ * GELU; gsparc_shared_mlp_bf16_act_table lists it).  image_state (optional)
+ * receives the error bit of a bounded tensor-core wait that gave up. */
 #define GSPARC_ACT_RELU 1
 #define GSPARC_ACT_GELU 2
 #define GSPARC_MLP_FP32 0
@@ -273,6 +275,13 @@ GSPARC_API int gsparc_shared_mlp_backward(int P, int R, int layers, int width, i
                                           const float* params, const void* geom_state, void* image_state,
                                           float* workspace, const float* dL_dsignal, float* dL_dparams,
                                           float* dL_dmeans3D, void* stream);
+
+/* The BF16 path's activation as its kernels evaluate it, for every BF16
+ * input: out (device, 6 x 65536 uint16) = {act as the forward computes it,
+ * act as the adjoint computes it, act'} x {input in the low lane of a packed
+ * pair, in the high lane}, entry i of each table for the input whose BF16
+ * bit pattern is i. */
+GSPARC_API int gsparc_shared_mlp_bf16_act_table(int act, uint16_t* out, void* stream);
 
 /* ---- training loss ------------------------------------------------------ */
 
