@@ -500,17 +500,11 @@ int gsparc_shared_mlp_backward(int P, int R, int layers, int width, int act, int
   GeomView geo;
   carve_geom((char*)geom_state, (size_t)P, (size_t)R, &geo);
   if (precision == GSPARC_MLP_BF16) {
-    {   // the tensor-core adjoint and the feature adjoint, timed apart
-      Timed t(KID_SHARED_MLP_BWD, s);
-      GS_CHECK(launch_shared_mlp_bf16(false, P, R, layers, act, out, means3D, rx_pos, params, geo, workspace,
-                                      dL_dsignal, dL_dparams, nullptr, (ImageHeader*)image_state, s),
-               "shared mlp backward (bf16)");
-    }
-    Timed t(KID_MLP_FEAT_BWD, s);
-    GS_CHECK(launch_mlp_features_backward(P, R, means3D, rx_pos, geo.radii,
-                                          workspace + shared_mlp_layout_bf16(layers, (size_t)P * R, out).d0,
-                                          dL_dmeans3D, s),
-             "shared mlp feature adjoint (bf16)");
+    // the tensor-core adjoint, with the feature adjoint in its last step
+    Timed t(KID_SHARED_MLP_BWD, s);
+    GS_CHECK(launch_shared_mlp_bf16(false, P, R, layers, act, out, means3D, rx_pos, params, geo, workspace,
+                                    dL_dsignal, dL_dparams, dL_dmeans3D, (ImageHeader*)image_state, s),
+             "shared mlp backward (bf16)");
   } else {
     Timed t(KID_SHARED_MLP_BWD, s);
     GS_CHECK(launch_shared_mlp_backward(P, R, layers, width, act, out, means3D, rx_pos, params, geo, workspace,

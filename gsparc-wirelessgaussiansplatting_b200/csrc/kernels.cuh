@@ -124,7 +124,8 @@ cudaError_t launch_blend_channels_backward(int P, int R, int H, int W, int C, co
 
 // BF16 / tcgen05 path (shared_mlp_tc.cu): width 128, 1 or 64 outputs, 1-3 layers;
 // workspace: sigmoid outputs [rows][out] at s (offset 0), BF16 pre-activations
-// [layers][rows][128] at z[1], feature gradient [rows][32] at d0.
+// [layers][rows][128] at z[1] (whole 128-row tiles, tile-transposed); the
+// adjoint adds dL/dmeans3D through the features itself.
 SharedMlpLayout shared_mlp_layout_bf16(int layers, size_t rows, int out);
 cudaError_t launch_shared_mlp_bf16(bool fwd, int P, int R, int layers, int act, int out, const float* means3D,
                                    const float* rx_pos, const float* params, const GeomView& geo, float* work,

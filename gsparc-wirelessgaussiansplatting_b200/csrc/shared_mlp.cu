@@ -896,8 +896,7 @@ SharedMlpLayout shared_mlp_layout_bf16(int layers, size_t rows, int out) {
   L.z[1] = w;
   // BF16 pre-activations, two per float, for whole 128-row tiles (tile-transposed)
   w += a((size_t)layers * ((rows + 127) / 128 * 128) * 128 / 2);
-  L.d0 = w;
-  w += a(rows * kFeat);
+  L.d0 = w;   // no feature-gradient segment: the adjoint applies it in place
   L.work = w;
   return L;
 }

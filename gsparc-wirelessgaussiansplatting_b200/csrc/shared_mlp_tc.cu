@@ -209,6 +209,82 @@ __device__ __forceinline__ void pair_features(const float* __restrict__ means3D,
   x[31] = 0.0f;
 }
 
+// pair_features rounded to BF16 pairs, produced in feature order (octave by
+// octave, all three coordinates at once) so that each value is packed as soon
+// as it exists; the values are those of pair_features.
+__device__ __forceinline__ void pair_features_bf16(const float* __restrict__ means3D, const float* __restrict__ rx_pos,
+                                                   int g, int r, bool vis, uint4 (&xp)[kFin / 8]) {
+  if (!vis) {
+#pragma unroll
+    for (int q = 0; q < kFin / 8; ++q) xp[q] = make_uint4(0u, 0u, 0u, 0u);
+    return;
+  }
+  const float m[3] = {means3D[3 * g], means3D[3 * g + 1], means3D[3 * g + 2]};
+  float s[3], c[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) sincosf(kPiF * m[j], &s[j], &c[j]);
+  uint32_t w[16];
+  w[0] = pack2(m[0], m[1]);
+  // x[2] = m2, then per octave k: x[3 + 6k + 2j] = sin, x[4 + 6k + 2j] = cos
+  float carry = m[2];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    // the octave's six values x[3 + 6k .. 8 + 6k]; x[2 + 6k] is `carry`
+    w[1 + 3 * k] = pack2(carry, s[0]);
+    w[2 + 3 * k] = pack2(c[0], s[1]);
+    w[3 + 3 * k] = pack2(c[1], s[2]);
+    carry = c[2];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float s2 = 2.0f * s[j] * c[j], c2 = fmaf(c[j], c[j], -s[j] * s[j]);
+      s[j] = s2;
+      c[j] = c2;
+    }
+  }
+  const float v[3] = {m[0] - rx_pos[3 * r], m[1] - rx_pos[3 * r + 1], m[2] - rx_pos[3 * r + 2]};
+  const float d2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  const float d = sqrtf(d2);
+  w[13] = pack2(carry, v[0] / d);       // x[26], x[27]
+  w[14] = pack2(v[1] / d, v[2] / d);    // x[28], x[29]
+  w[15] = pack2(1.0f / d2, 0.0f);       // x[30], x[31]
+#pragma unroll
+  for (int q = 0; q < kFin / 8; ++q) xp[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+}
+
+// The chain rule of pair_features for one visible pair: its feature gradient
+// dx through the centre, added to dL_dmeans3D[g] by atomics (the rows of a
+// tile are distinct Gaussians; a Gaussian's receivers meet in the atomics).
+// The octaves' sines and cosines come from the same double-angle steps as in
+// pair_features.
+__device__ __forceinline__ void pair_features_adjoint(const float* __restrict__ means3D,
+                                                      const float* __restrict__ rx_pos, int g, int r,
+                                                      const float (&dx)[kFin], float* __restrict__ dL_dmeans3D) {
+  const float m[3] = {means3D[3 * g], means3D[3 * g + 1], means3D[3 * g + 2]};
+  const float v[3] = {m[0] - rx_pos[3 * r], m[1] - rx_pos[3 * r + 1], m[2] - rx_pos[3 * r + 2]};
+  const float d2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  const float d = sqrtf(d2);
+  const float u[3] = {v[0] / d, v[1] / d, v[2] / d};
+  // direction u = v / d: du_i/dv_j = (delta_ij - u_i u_j) / d;  1 / d^2: d/dv = -2 v / d^4
+  const float gu = dx[27] * u[0] + dx[28] * u[1] + dx[29] * u[2];
+  const float ga = dx[30] * (-2.0f / (d2 * d2));
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    float gj = dx[j] + (dx[27 + j] - gu * u[j]) / d + ga * v[j];
+    float s, c;
+    sincosf(kPiF * m[j], &s, &c);
+    float w = kPiF;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      gj += w * (c * dx[3 + 6 * k + 2 * j] - s * dx[4 + 6 * k + 2 * j]);
+      const float s2 = 2.0f * s * c, c2 = fmaf(c, c, -s * s);
+      s = s2;
+      c = c2;
+      w *= 2.0f;
+    }
+    atomicAdd(&dL_dmeans3D[3 * g + j], gj);
+  }
+}
+
 // Sum 32 per-lane values over the warp: returns, in lane j, the sum of value j.
 __device__ __forceinline__ float warp_transpose_sum32(float (&v)[32], int lane) {
 #pragma unroll
@@ -444,7 +520,7 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                          const float* __restrict__ rx_pos, const float* __restrict__ params,
                          const int* __restrict__ radii, const __nv_bfloat16* __restrict__ zb,
                          const float* __restrict__ S, const float* __restrict__ dL_dsignal,
-                         float* __restrict__ dX0, float* __restrict__ dparams, ImageHeader* __restrict__ hdr,
+                         float* __restrict__ dL_dmeans3D, float* __restrict__ dparams, ImageHeader* __restrict__ hdr,
                          uint32_t polls) {
   constexpr int kOutMma = out_mma_width(kOut);
   constexpr bool kBias0Cuda = bwd_bias0_on_cuda_cores(kLayers, kOut);
@@ -634,10 +710,25 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         z_pending = true;
       }
     };
-    if ((size_t)blockIdx.x * kBwdGroups + grp < ntiles) stage_slab(kLayers - 1, (size_t)blockIdx.x * kBwdGroups + grp);
-    for (size_t tile = (size_t)blockIdx.x * kBwdGroups + grp; tile < ntiles && ok; tile += tile_stride) {
+    // a row's visibility and (one output) its dO = dL/dsignal s (1 - s), loaded
+    // a step ahead (the next tile's during this tile's last MMAs)
+    auto load_row = [&](size_t rw, bool& vis_out) -> float {
+      vis_out = rw < rows && radii[rw] > 0;
+      if (kOut != 1 || hf != 0 || !vis_out) return 0.0f;
+      const float sg = S[rw];
+      return dL_dsignal[2 * rw] * sg * (1.0f - sg);
+    };
+    const size_t tile0 = (size_t)blockIdx.x * kBwdGroups + grp;
+    bool vis_n = false;
+    float dO_n = 0.0f;
+    if (tile0 < ntiles) {
+      stage_slab(kLayers - 1, tile0);
+      dO_n = load_row(tile0 * kRows + r, vis_n);
+    }
+    for (size_t tile = tile0; tile < ntiles && ok; tile += tile_stride) {
       const size_t row0 = tile * kRows, row = row0 + r;
       const bool valid = row < rows;
+      const bool vis = vis_n;
       if (t == 0 && tile + tile_stride < ntiles) {
         // the next tile's pre-activation slabs, outputs, radii and incoming gradients into L2
         for (int l = kLayers - 1; l >= 0; --l)
@@ -648,12 +739,10 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         tc::prefetch_l2(radii + r1, n1 * 4);
         tc::prefetch_l2(dL_dsignal + (kOut > 1 ? r1 * kOut : 2 * r1), n1 * (kOut > 1 ? 4 * kOut : 8));
       }
-      const bool vis = valid && radii[row] > 0;
-      // dO = dL/dsignal * s (1 - s) -> the dO row tile (BF16) in the dZ buffer; db_out sums it in FP32
+      // dO -> the dO row tile (BF16) in the dZ buffer; db_out sums it in FP32
       if constexpr (kOut == 1) {
         if (hf == 0) {
-          const float s = valid ? S[row] : 0.0f;
-          const float dO = vis ? dL_dsignal[2 * row] * s * (1.0f - s) : 0.0f;
+          const float dO = dO_n;
           *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(r, 0, kLbo, kSboO)) =
               make_uint4(pack2(dO, 0.0f), 0u, 0u, 0u);
           *reinterpret_cast<uint4*>(dZ + tc::kmajor_off(r, 8, kLbo, kSboO)) = make_uint4(0u, 0u, 0u, 0u);
@@ -691,21 +780,24 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         // act'(Z_{l-1}) of this row's columns as BF16 pairs, kept for dZ_{l-1}
         // after the MMAs
         uint32_t ad[kHc / 2];
-        // A_{l-1}: features (l == 0) or act(Z_{l-1}); the ones column sits at `in`
         if (l == 0) {
+          // A_{-1}: the row's features (BF16), then the ones column (not for the
+          // layer whose bias is summed on the CUDA cores).  Forming them while
+          // step 1's MMAs ran was slower (3.20 -> 3.72 ms at 6.4 M rows): the
+          // features' registers beside act' spilled in the per-step code.
           if (hf == 0) {
             int rr, g;
             row_pair(row0, r, P, rr, g);
-            float x[kFin];
-            pair_features(means3D, rx_pos, g, rr, vis, x);
+            uint4 xp[kFin / 8];
+            pair_features_bf16(means3D, rx_pos, g, rr, vis, xp);
 #pragma unroll
-            for (int kc = 0; kc < kFin / 8; ++kc)
-              *reinterpret_cast<uint4*>(Ab + slab_off(r, kc * 8)) = pack8(x + kc * 8);
+            for (int kc = 0; kc < kFin / 8; ++kc) *reinterpret_cast<uint4*>(Ab + slab_off(r, kc * 8)) = xp[kc];
           } else if constexpr (!kBias0Cuda) {
             *reinterpret_cast<uint4*>(Ab + slab_off(r, kFin)) = make_uint4(pack2(1.0f, 0.0f), 0u, 0u, 0u);
             *reinterpret_cast<uint4*>(Ab + slab_off(r, kFin + 8)) = make_uint4(0u, 0u, 0u, 0u);
           }
-        } else {
+        }
+        if (l > 0) {
           // Z_{l-1} of the tile, staged in the activation tile by a bulk copy:
           // activate it in place (rows past the end read as zero)
           const bool zgot = tc::mbar_wait(&bar_z[grp], ph_z, polls);
@@ -731,17 +823,17 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         // hand dZ_l (or dO) and A_{l-1} to the MMA warp
         tc::fence_async_smem();
         tc::mbar_arrive(&bar_ready[grp]);
-        // once the weight-gradient MMA has read the activation tile (before dA is
-        // computed), the group's first thread stages the slab the next step
-        // activates into it
         bool afree = true;
         if (t == 0 && (l >= 2 || (l == 0 && tile + tile_stride < ntiles))) {
+          // once the weight-gradient MMA has read the activation tile (before dA
+          // is computed), stage the slab the next step activates into it
           afree = tc::mbar_wait(&bar_afree[grp], ph_done, polls);
           if (afree) {
             if (l >= 2) stage_slab(l - 2, tile);
             else stage_slab(kLayers - 1, tile + tile_stride);
           }
         }
+        if (l == 0 && tile + tile_stride < ntiles) dO_n = load_row((tile + tile_stride) * kRows + r, vis_n);
         const bool got = tc::mbar_wait(&bar_done[grp], ph_done, polls);
         ph_done ^= 1u;
         tc::fence_after_sync();
@@ -751,15 +843,16 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         }
         if (l == 0) {
           if (hf == 0) {
+            // dL/dx of the row, then through the features into dL/dmeans3D
             float v[32];
             tc::tmem_ld32(tmem + lane_base + scratch, v);
             tc::fence_before_sync();
             tc::mbar_arrive(&bar_free);
-            if (valid)
-#pragma unroll
-              for (int q = 0; q < 8; ++q)
-                *reinterpret_cast<float4*>(dX0 + row * kFin + q * 4) =
-                    make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            if (vis && dL_dmeans3D != nullptr) {
+              int rr, g;
+              row_pair(row0, r, P, rr, g);
+              pair_features_adjoint(means3D, rx_pos, g, rr, v, dL_dmeans3D);
+            }
           } else {
             tc::fence_before_sync();
             tc::mbar_arrive(&bar_free);
@@ -904,8 +997,8 @@ size_t mlp_bf16_backward_smem(int layers, int out) {
 template <int L, int A, int O>
 static cudaError_t launch_bf16_layers(bool fwd, int P, size_t rows, const float* means3D, const float* rx_pos,
                                       const float* params, const GeomView& geo, const SharedMlpLayout& Lt,
-                                      float* work, const float* dL_dsignal, float* dparams, ImageHeader* hdr,
-                                      cudaStream_t s) {
+                                      float* work, const float* dL_dsignal, float* dparams, float* dL_dmeans3D,
+                                      ImageHeader* hdr, cudaStream_t s) {
   const size_t smem = fwd ? mlp_bf16_forward_smem(L, O) : mlp_bf16_backward_smem(L, O);
   static bool attr_done[2][64] = {};   // per instantiation
   static int sm_count[64] = {};
@@ -937,7 +1030,7 @@ static cudaError_t launch_bf16_layers(bool fwd, int P, size_t rows, const float*
                                                                           hdr, wait_polls(kPolls));
   else
     mlp_bf16_backward_kernel<L, A, O><<<grid, kBwdThreads, smem, s>>>(P, rows, means3D, rx_pos, params, geo.radii,
-                                                                      zb, work + Lt.s, dL_dsignal, work + Lt.d0,
+                                                                      zb, work + Lt.s, dL_dsignal, dL_dmeans3D,
                                                                       dparams, hdr, wait_polls(kPolls));
   return cudaGetLastError();
 }
@@ -946,17 +1039,17 @@ template <int L>
 static cudaError_t launch_bf16_act(bool fwd, int P, size_t rows, int act, int out, const float* means3D,
                                    const float* rx_pos, const float* params, const GeomView& geo,
                                    const SharedMlpLayout& Lt, float* work, const float* dL_dsignal, float* dparams,
-                                   ImageHeader* hdr, cudaStream_t s) {
+                                   float* dL_dmeans3D, ImageHeader* hdr, cudaStream_t s) {
   if (out == 64)
     return act == 1 ? launch_bf16_layers<L, 1, 64>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work,
-                                                   dL_dsignal, dparams, hdr, s)
+                                                   dL_dsignal, dparams, dL_dmeans3D, hdr, s)
                     : launch_bf16_layers<L, 2, 64>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work,
-                                                   dL_dsignal, dparams, hdr, s);
+                                                   dL_dsignal, dparams, dL_dmeans3D, hdr, s);
   if (out != 1) return cudaErrorInvalidValue;
   return act == 1 ? launch_bf16_layers<L, 1, 1>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work, dL_dsignal,
-                                                dparams, hdr, s)
+                                                dparams, dL_dmeans3D, hdr, s)
                   : launch_bf16_layers<L, 2, 1>(fwd, P, rows, means3D, rx_pos, params, geo, Lt, work, dL_dsignal,
-                                                dparams, hdr, s);
+                                                dparams, dL_dmeans3D, hdr, s);
 }
 
 cudaError_t launch_shared_mlp_bf16(bool fwd, int P, int R, int layers, int act, int out, const float* means3D,
@@ -971,13 +1064,12 @@ cudaError_t launch_shared_mlp_bf16(bool fwd, int P, int R, int layers, int act, 
     if (e != cudaSuccess) return e;
   }
   switch (layers) {
-    case 1: e = launch_bf16_act<1>(fwd, P, rows, act, out, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
-    case 2: e = launch_bf16_act<2>(fwd, P, rows, act, out, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
-    case 3: e = launch_bf16_act<3>(fwd, P, rows, act, out, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, hdr, s); break;
+    case 1: e = launch_bf16_act<1>(fwd, P, rows, act, out, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, dL_dmeans3D, hdr, s); break;
+    case 2: e = launch_bf16_act<2>(fwd, P, rows, act, out, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, dL_dmeans3D, hdr, s); break;
+    case 3: e = launch_bf16_act<3>(fwd, P, rows, act, out, means3D, rx_pos, params, geo, Lt, work, dL_dsignal, dparams, dL_dmeans3D, hdr, s); break;
     default: return cudaErrorInvalidValue;
   }
-  if (e != cudaSuccess || fwd || dL_dmeans3D == nullptr) return e;
-  return launch_mlp_features_backward(P, R, means3D, rx_pos, geo.radii, work + Lt.d0, dL_dmeans3D, s);
+  return e;
 }
 
 }  // namespace gsparc
