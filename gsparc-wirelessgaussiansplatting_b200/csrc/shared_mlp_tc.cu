@@ -111,24 +111,25 @@ __device__ __forceinline__ float2 bf2_unpack(uint32_t z) {
 constexpr uint32_t kBfOne = 0x3F803F80u;   // BF16 1.0 in both halves
 
 // GELU of BF16 pre-activations in the tanh form
-//   a = h (1 + t),  h = z / 2,  t = tanh v,  v = z (c1 + c3 z^2),
-// i.e. Phi(z) ~ (1 + t) / 2, evaluated in FP32 with the hardware tanh and
-// rounded to BF16 once.  c1 = 0.80078125 and c3 = 0.034423828125 are fitted to
-// the erf GELU z Phi(z): max |a - z Phi(z)| = 3.6e-4 over [-8, 8] (the classic
+//   a = z g,  g = (1 + t) / 2,  t = tanh v,  v = z (c1 + c3 z^2),
+// i.e. Phi(z) ~ g, evaluated in FP32 with the hardware tanh and rounded to
+// BF16 once.  c1 = 0.80078125 and c3 = 0.034423828125 are fitted to the erf
+// GELU z Phi(z): max |a - z Phi(z)| = 3.6e-4 over [-8, 8] (the classic
 // sqrt(2/pi), 0.044715 sqrt(2/pi) give 4.7e-4), below the BF16 spacing of the
 // activations it feeds.  The adjoint's derivative is the form's own:
-//   a' = (1 + t) / 2 + h (1 - t^2) (c1 + 3 c3 z^2),
+//   a' = g + z (1 - t^2) (c1 + 3 c3 z^2) / 2,
 // in FP32 (1 - t^2 needs FP32 where t is within a BF16 step of +-1).  One
 // special-function evaluation (the tanh) per element in both kernels.
 constexpr float kGeluC1 = 0.80078125f, kGeluC3 = 0.034423828125f;
+__device__ __forceinline__ float2 gelu_tanh_term(float2 z, float2 zz) {
+  const float2 v = fmul2(z, ffma2(zz, make_float2(kGeluC3, kGeluC3), make_float2(kGeluC1, kGeluC1)));
+  return make_float2(tanh_approx(v.x), tanh_approx(v.y));
+}
 __device__ __forceinline__ uint32_t act_fwd2(int act, uint32_t zb) {
   if (act == 1) return bf2_max(zb, 0u);
   const float2 z = bf2_unpack(zb);
-  const float2 zz = fmul2(z, z);
-  const float2 v = fmul2(z, ffma2(zz, make_float2(kGeluC3, kGeluC3), make_float2(kGeluC1, kGeluC1)));
-  const float2 t = make_float2(tanh_approx(v.x), tanh_approx(v.y));
-  const float2 h = fmul2(z, make_float2(0.5f, 0.5f));
-  const float2 a = ffma2(h, t, h);
+  const float2 t = gelu_tanh_term(z, fmul2(z, z));
+  const float2 a = fmul2(z, ffma2(t, make_float2(0.5f, 0.5f), make_float2(0.5f, 0.5f)));
   return pack2(a.x, a.y);
 }
 // act (the forward's, bit for bit) and act' of a pair, both rounded to BF16
@@ -140,14 +141,13 @@ __device__ __forceinline__ void act_bwd2(int act, uint32_t zb, uint32_t& a2, uin
   }
   const float2 z = bf2_unpack(zb);
   const float2 zz = fmul2(z, z);
-  const float2 v = fmul2(z, ffma2(zz, make_float2(kGeluC3, kGeluC3), make_float2(kGeluC1, kGeluC1)));
-  const float2 t = make_float2(tanh_approx(v.x), tanh_approx(v.y));
-  const float2 h = fmul2(z, make_float2(0.5f, 0.5f));
-  const float2 a = ffma2(h, t, h);
+  const float2 t = gelu_tanh_term(z, zz);
+  const float2 g = ffma2(t, make_float2(0.5f, 0.5f), make_float2(0.5f, 0.5f));
+  const float2 a = fmul2(z, g);
   const float2 s = ffma2(make_float2(-t.x, -t.y), t, make_float2(1.0f, 1.0f));   // 1 - t^2
-  const float2 w = ffma2(zz, make_float2(3.0f * kGeluC3, 3.0f * kGeluC3), make_float2(kGeluC1, kGeluC1));
-  // (h s) first: s is exactly 0 where t saturates, so w (~z^2) cannot make inf * 0
-  const float2 d = ffma2(fmul2(h, s), w, ffma2(t, make_float2(0.5f, 0.5f), make_float2(0.5f, 0.5f)));
+  const float2 w = ffma2(zz, make_float2(1.5f * kGeluC3, 1.5f * kGeluC3), make_float2(0.5f * kGeluC1, 0.5f * kGeluC1));
+  // (z s) first: s is exactly 0 where t saturates, so w (~z^2) cannot make inf * 0
+  const float2 d = ffma2(fmul2(z, s), w, g);
   a2 = pack2(a.x, a.y);
   d2 = pack2(d.x, d.y);
 }
@@ -858,17 +858,10 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
             tc::mbar_arrive(&bar_free);
           }
         } else {
-          // dZ_{l-1} = BF16(dA_{l-1}) * act'(Z_{l-1}) in BF16, 16 columns at a time; the MMAs
-          // that read dZ_l (or dO) are done
-#pragma unroll
-          for (int c = 0; c < kHc / 16; ++c) {
+          // dZ_{l-1} = BF16(dA_{l-1}) * act'(Z_{l-1}) in BF16, 32 columns (two TMEM loads, one
+          // wait) at a time; the MMAs that read dZ_l (or dO) are done
+          auto form_dz = [&](float (&v)[16], int c) {
             const int c0 = cb + 16 * c;
-            float v[16];
-            tc::tmem_ld16(tmem + lane_base + scratch + c0, v);
-            if (c + 1 == kHc / 16) {
-              tc::fence_before_sync();
-              tc::mbar_arrive(&bar_free);
-            }
             uint32_t p[8];
 #pragma unroll
             for (int i = 0; i < 8; ++i) p[i] = bf2_mul(pack2(v[2 * i], v[2 * i + 1]), ad[8 * c + i]);
@@ -886,6 +879,18 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
               const float sum = warp_transpose_sum16(v, lane);
               if (lane < 16) atomicAdd(&s_red[kOut + c0 + lane], sum);
             }
+          };
+#pragma unroll
+          for (int c = 0; c < kHc / 16; c += 2) {
+            float v0[16], v1[16];
+            tc::tmem_ld16x2(tmem + lane_base + scratch + cb + 16 * c, tmem + lane_base + scratch + cb + 16 * c + 16,
+                            v0, v1);
+            if (c + 2 == kHc / 16) {
+              tc::fence_before_sync();
+              tc::mbar_arrive(&bar_free);
+            }
+            form_dz(v0, c);
+            form_dz(v1, c + 1);
           }
         }
       }
