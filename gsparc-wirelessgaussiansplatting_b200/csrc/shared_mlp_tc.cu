@@ -423,16 +423,25 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
     // hidden layers, then the output layer (l == kLayers)
     for (int l = 0; l <= kLayers; ++l) {
       const bool out_layer = l == kLayers;
-      const int in = l == 0 ? kFin : kH;
       group_publish(bar_id);
-      if (t == 0) {
-        const uint32_t sbo = (uint32_t)(in / 8) * 128u;
+      if (t < 32) {
+        // the group's first warp issues the layer's MMAs (one elected lane, unrolled)
         const uint32_t a0 = tc::smem_u32(Hs), b0 = tc::smem_u32(out_layer ? Wo : Ws[l]);
         const uint32_t idesc = tc::idesc_bf16(kRows, out_layer ? kOutMma : kH, false, false);
-        for (int kk = 0; kk < in / 16; ++kk)
-          tc::mma_bf16(tmem, tc::smem_desc(a0 + kk * 2 * kLbo, kLbo, sbo),
-                       tc::smem_desc(b0 + kk * 2 * kLbo, kLbo, sbo), idesc, kk > 0 ? 1u : 0u);
-        tc::commit(&mbar[grp]);
+        if (l == 0) {
+          constexpr uint32_t sbo = (uint32_t)(kFin / 8) * 128u;
+#pragma unroll
+          for (int kk = 0; kk < kFin / 16; ++kk)
+            tc::mma_bf16_warp(tmem, tc::smem_desc(a0 + kk * 2 * kLbo, kLbo, sbo),
+                              tc::smem_desc(b0 + kk * 2 * kLbo, kLbo, sbo), idesc, kk > 0 ? 1u : 0u);
+        } else {
+          constexpr uint32_t sbo = (uint32_t)(kH / 8) * 128u;
+#pragma unroll
+          for (int kk = 0; kk < kH / 16; ++kk)
+            tc::mma_bf16_warp(tmem, tc::smem_desc(a0 + kk * 2 * kLbo, kLbo, sbo),
+                              tc::smem_desc(b0 + kk * 2 * kLbo, kLbo, sbo), idesc, kk > 0 ? 1u : 0u);
+        }
+        tc::commit_warp(&mbar[grp]);
       }
       const bool got = tc::mbar_wait(&mbar[grp], phase, polls);
       phase ^= 1u;
@@ -615,85 +624,86 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   const size_t tile_stride = (size_t)gridDim.x * kBwdGroups;
 
   if (grp == kBwdGroups) {
-    // ---- MMA warp: one thread issues every MMA of the CTA, in the order
-    // (tile round, step, group), so both groups' weight gradients accumulate
-    // into the same TMEM columns in issue order.
-    if (lane == 0) {
-      uint32_t ph_ready[kBwdGroups] = {};
-      bool first[kLayers + 1];
-      for (int l = 0; l <= kLayers; ++l) first[l] = true;
-      uint32_t n_da = 0;
-      bool ok = true;
-      for (size_t base = (size_t)blockIdx.x * kBwdGroups; base < ntiles && ok; base += tile_stride) {
+    // ---- MMA warp: the whole warp walks the schedule and one elected lane
+    // issues every MMA and commit of the CTA, in the order (tile round, step,
+    // group), so both groups' weight gradients accumulate into the same TMEM
+    // columns in issue order.  The K loops are unrolled (uniform descriptors).
+    constexpr uint32_t kAll = 0xffffffffu;
+    uint32_t ph_ready[kBwdGroups] = {};
+    bool first[kLayers + 1];
+    for (int l = 0; l <= kLayers; ++l) first[l] = true;
+    uint32_t n_da = 0;
+    bool ok = true;
+    for (size_t base = (size_t)blockIdx.x * kBwdGroups; base < ntiles && ok; base += tile_stride) {
 #pragma unroll 1
-        for (int l = kLayers; l >= 0 && ok; --l) {
-          const bool out_step = l == kLayers;
-          const int in = l == 0 ? kFin : kH;
+      for (int l = kLayers; l >= 0 && ok; --l) {
+        const bool out_step = l == kLayers;
+        const int in = l == 0 ? kFin : kH;
 #pragma unroll 1
-          for (int q = 0; q < kBwdGroups; ++q) {
-            if (base + q >= ntiles) break;
-            if (!tc::mbar_wait(&bar_ready[q], ph_ready[q], polls)) {
+        for (int q = 0; q < kBwdGroups; ++q) {
+          if (base + q >= ntiles) break;
+          if (!__all_sync(kAll, tc::mbar_wait(&bar_ready[q], ph_ready[q], polls))) {
+            ok = false;
+            break;
+          }
+          ph_ready[q] ^= 1u;
+          tc::fence_after_sync();
+          const uint32_t zq = tc::smem_u32(groups + (size_t)q * kGroupBytes);
+          const uint32_t aq = zq + (uint32_t)(kRows * kH * 2);
+          if (out_step) {
+            // dW_out^T += A_{L-1}^T dO: A operand A^T (M = hidden units, K = rows) and B operand
+            // dO^T (N = outputs, K = rows), MN-major views of the row tiles
+            const uint32_t id_o = tc::idesc_bf16(kH, kOutMma, true, true);
+#pragma unroll
+            for (int kk = 0; kk < kRows / 16; ++kk)
+              tc::mma_bf16_warp(tmem + dwo_col, tc::smem_desc(aq + kk * 256u, 128u, kChunkA),
+                                tc::smem_desc(zq + kk * 2 * kSboO, kSboO, 128u), id_o,
+                                (!first[kLayers] || kk > 0) ? 1u : 0u);
+            first[kLayers] = false;
+          } else {
+            // dW_l | db_l += dZ^T [A | 1]: A operand dZ^T (M = outputs, K = rows) and
+            // B operand [A | 1]^T (N = in (+ 16), K = rows), both MN-major views of the
+            // row tiles
+            const uint32_t id_w = tc::idesc_bf16(kH, dw_width(l), true, true);
+            const uint32_t dcol = tmem + dwcol(l);
+            const uint32_t acc0 = first[l] ? 0u : 1u;
+#pragma unroll
+            for (int kk = 0; kk < kRows / 16; ++kk)
+              tc::mma_bf16_warp(dcol, tc::smem_desc(zq + kk * 2 * kSboH, kSboH, 128u),
+                                tc::smem_desc(aq + kk * 256u, 128u, kChunkA), id_w, kk > 0 ? 1u : acc0);
+            first[l] = false;
+          }
+          // the activation tile is read: the group may stage the next slab into it
+          tc::commit_warp(&bar_afree[q]);
+          // dA = dZ_l W_l (or dO W_out) into the scratch, once its previous reader has drained it
+          if (n_da > 0) {
+            if (!__all_sync(kAll, tc::mbar_wait(&bar_free, (n_da - 1) & 1u, polls))) {
               ok = false;
               break;
             }
-            ph_ready[q] ^= 1u;
             tc::fence_after_sync();
-            const uint32_t zq = tc::smem_u32(groups + (size_t)q * kGroupBytes);
-            const uint32_t aq = zq + (uint32_t)(kRows * kH * 2);
-            if (out_step) {
-              // dW_out^T += A_{L-1}^T dO: A operand A^T (M = hidden units, K = rows) and B operand
-              // dO^T (N = outputs, K = rows), MN-major views of the row tiles
-              const uint32_t id_o = tc::idesc_bf16(kH, kOutMma, true, true);
-#pragma unroll 1
-              for (int kk = 0; kk < kRows / 16; ++kk)
-                tc::mma_bf16(tmem + dwo_col, tc::smem_desc(aq + kk * 256u, 128u, kChunkA),
-                             tc::smem_desc(zq + kk * 2 * kSboO, kSboO, 128u), id_o,
-                             (!first[kLayers] || kk > 0) ? 1u : 0u);
-              first[kLayers] = false;
-            } else {
-              // dW_l | db_l += dZ^T [A | 1]: A operand dZ^T (M = outputs, K = rows) and
-              // B operand [A | 1]^T (N = in (+ 16), K = rows), both MN-major views of the
-              // row tiles
-              const uint32_t id_w = tc::idesc_bf16(kH, dw_width(l), true, true);
-#pragma unroll 1
-              for (int kk = 0; kk < kRows / 16; ++kk)
-                tc::mma_bf16(tmem + dwcol(l), tc::smem_desc(zq + kk * 2 * kSboH, kSboH, 128u),
-                             tc::smem_desc(aq + kk * 256u, 128u, kChunkA), id_w,
-                             (!first[l] || kk > 0) ? 1u : 0u);
-              first[l] = false;
-            }
-            // the activation tile is read: the group may stage the next slab into it
-            tc::commit(&bar_afree[q]);
-            // dA = dZ_l W_l (or dO W_out) into the scratch, once its previous reader has drained it
-            if (n_da > 0) {
-              if (!tc::mbar_wait(&bar_free, (n_da - 1) & 1u, polls)) {
-                ok = false;
-                break;
-              }
-              tc::fence_after_sync();
-            }
-            if (out_step) {
-              const uint32_t id_x = tc::idesc_bf16(kRows, kH, false, true);
-              const uint32_t wo = tc::smem_u32(Wo);
-#pragma unroll 1
-              for (int kk = 0; kk < kOutMma / 16; ++kk)
-                tc::mma_bf16(tmem + scratch, tc::smem_desc(zq + kk * 2 * kLbo, kLbo, kSboO),
-                             tc::smem_desc(wo + kk * 2 * kLbo, kLbo, kSboO), id_x, kk > 0 ? 1u : 0u);
-            } else {
-              const uint32_t id_x = tc::idesc_bf16(kRows, in, false, true);
-              const uint32_t wb = tc::smem_u32(Wb[l]);
-#pragma unroll 1
-              for (int kk = 0; kk < kH / 16; ++kk)
-                tc::mma_bf16(tmem + scratch, tc::smem_desc(zq + kk * 2 * kLbo, kLbo, kSboH),
-                             tc::smem_desc(wb + kk * 2 * kLbo, kLbo, kSboH), id_x, kk > 0 ? 1u : 0u);
-            }
-            ++n_da;
-            tc::commit(&bar_done[q]);
           }
+          if (out_step) {
+            const uint32_t id_x = tc::idesc_bf16(kRows, kH, false, true);
+            const uint32_t wo = tc::smem_u32(Wo);
+#pragma unroll
+            for (int kk = 0; kk < kOutMma / 16; ++kk)
+              tc::mma_bf16_warp(tmem + scratch, tc::smem_desc(zq + kk * 2 * kLbo, kLbo, kSboO),
+                                tc::smem_desc(wo + kk * 2 * kLbo, kLbo, kSboO), id_x, kk > 0 ? 1u : 0u);
+          } else {
+            const uint32_t id_x = tc::idesc_bf16(kRows, in, false, true);
+            const uint32_t wb = tc::smem_u32(Wb[l]);
+#pragma unroll
+            for (int kk = 0; kk < kH / 16; ++kk)
+              tc::mma_bf16_warp(tmem + scratch, tc::smem_desc(zq + kk * 2 * kLbo, kLbo, kSboH),
+                                tc::smem_desc(wb + kk * 2 * kLbo, kLbo, kSboH), id_x, kk > 0 ? 1u : 0u);
+          }
+          ++n_da;
+          tc::commit_warp(&bar_done[q]);
         }
       }
-      if (!ok) s_fail = 1;
     }
+    if (!ok && lane == 0) s_fail = 1;
   } else {
     // ---- compute group: thread (r, hf) handles row r, columns [hf kHc, hf kHc + kHc)
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
@@ -946,10 +956,10 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
     }
   }
   if (s_fail && tid == 0 && hdr) atomic_or_error(hdr, kErrMlpWait);
-  if (s_fail && grp == kBwdGroups && lane == 0) {
-    // drain: every MMA the issuing thread started completes before the
-    // tensor memory is freed
-    tc::commit(&bar_drain);
+  if (s_fail && grp == kBwdGroups) {
+    // drain: every MMA the MMA warp's issuing lane started completes before
+    // the tensor memory is freed
+    tc::commit_warp(&bar_drain);
     tc::mbar_wait(&bar_drain, 0, kPolls);
   }
   tc::fence_before_sync();

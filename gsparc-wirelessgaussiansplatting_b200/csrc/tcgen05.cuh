@@ -60,6 +60,31 @@ __device__ __forceinline__ void commit(uint64_t* mbar) {
                : "memory");
 }
 
+// Warp-wide forms: called by all 32 lanes of a converged warp with warp-uniform
+// operands; elect.sync over the full mask picks the issuing lane, the same lane
+// every time, so a commit tracks the MMAs the same warp issued before it.
+// Issued from fully unrolled loops with uniform descriptors, one K = 16 MMA
+// costs about the tensor pipe's own time (M = 128: 72 cycles at N = 128, 131 at
+// N = 256, B200); from a rolled single-lane loop it cost about 160 cycles
+// whatever N was.
+__device__ __forceinline__ void mma_bf16_warp(uint32_t tmem_d, uint64_t desc_a, uint64_t desc_b, uint32_t idesc,
+                                              uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p, e;\n\t"
+      "elect.sync _|e, 0xffffffff;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(desc_a), "l"(desc_b), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void commit_warp(uint64_t* mbar) {
+  asm volatile(
+      "{\n\t.reg .pred e;\n\t"
+      "elect.sync _|e, 0xffffffff;\n\t"
+      "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}\n" ::"r"(smem_u32(mbar))
+      : "memory");
+}
+
 __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 // generic-proxy shared-memory writes -> visible to the tensor cores (async proxy)
