@@ -420,11 +420,23 @@ segment_place_kernel(int P, int T, const uint2* __restrict__ ranges, const Image
     if (w < words) {
       uint32_t pos = pre[w >> 3] + incl - c;
       const uint32_t* idw = ids + ((size_t)w << 5);
+      // up to eight set bits at a time: their id loads are issued together,
+      // then stored in bit order (one load latency per eight bits, not per bit)
       while (bits) {
-        const int b = __ffs(bits) - 1;
-        bits &= bits - 1u;
-        if (pos < (uint32_t)n) out[pos] = idw[b];
-        ++pos;
+        uint32_t v[8];
+        int m = 0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1u;
+            v[u] = idw[b];
+            m = u + 1;
+          }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (u < m && pos + u < (uint32_t)n) out[pos + u] = v[u];
+        pos += m;
       }
     }
   }
