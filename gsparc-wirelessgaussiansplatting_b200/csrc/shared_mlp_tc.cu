@@ -251,14 +251,66 @@ __device__ __forceinline__ void pair_features_bf16(const float* __restrict__ mea
   for (int q = 0; q < kFin / 8; ++q) xp[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
 }
 
+// pair_features of one pair written as BF16 straight into row r of the
+// adjoint's activation tile (the slab layout), split between the row's two
+// threads: part 0 -- the first two coordinates (x[j] and the sines and
+// cosines of their octaves), part 1 -- the third coordinate, the direction and
+// the attenuation (x[27..31]).  Every value comes from the FP32 arithmetic of
+// pair_features and is rounded to BF16 once; a culled pair's row is zero
+// (written by part 0).
+__device__ __forceinline__ void store_feature(unsigned char* Ab, int r, int c, float v) {
+  *reinterpret_cast<__nv_bfloat16*>(Ab + slab_off(r, c)) = __float2bfloat16_rn(v);
+}
+// x[j], then per octave k: x[3 + 6k + 2j] = sin, x[4 + 6k + 2j] = cos
+__device__ __forceinline__ void coord_features(unsigned char* Ab, int r, int j, float mj) {
+  store_feature(Ab, r, j, mj);
+  float s, c;
+  sincosf(kPiF * mj, &s, &c);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    store_feature(Ab, r, 3 + 6 * k + 2 * j, s);
+    store_feature(Ab, r, 4 + 6 * k + 2 * j, c);
+    const float s2 = 2.0f * s * c, c2 = fmaf(c, c, -s * s);
+    s = s2;
+    c = c2;
+  }
+}
+__device__ __forceinline__ void pair_features_tile(const float* __restrict__ means3D, const float* __restrict__ rx_pos,
+                                                   int g, int rr, bool vis, int part, unsigned char* Ab, int r) {
+  if (!vis) {
+    if (part == 0)
+#pragma unroll
+      for (int kc = 0; kc < kFin / 8; ++kc) *reinterpret_cast<uint4*>(Ab + slab_off(r, kc * 8)) = make_uint4(0u, 0u, 0u, 0u);
+    return;
+  }
+  const float m[3] = {means3D[3 * g], means3D[3 * g + 1], means3D[3 * g + 2]};
+  if (part == 0) {
+    coord_features(Ab, r, 0, m[0]);
+    coord_features(Ab, r, 1, m[1]);
+    return;
+  }
+  const float v[3] = {m[0] - rx_pos[3 * rr], m[1] - rx_pos[3 * rr + 1], m[2] - rx_pos[3 * rr + 2]};
+  coord_features(Ab, r, 2, m[2]);
+  const float d2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  const float d = sqrtf(d2);
+  store_feature(Ab, r, 27, v[0] / d);
+  store_feature(Ab, r, 28, v[1] / d);
+  store_feature(Ab, r, 29, v[2] / d);
+  store_feature(Ab, r, 30, 1.0f / d2);
+  store_feature(Ab, r, 31, 0.0f);
+}
+
 // The chain rule of pair_features for one visible pair: its feature gradient
 // dx through the centre, added to dL_dmeans3D[g] by atomics (the rows of a
 // tile are distinct Gaussians; a Gaussian's receivers meet in the atomics).
-// The octaves' sines and cosines come from the same double-angle steps as in
-// pair_features.
+// The coordinates are split between the row's two threads as in
+// pair_features_tile (part 0: x and y, part 1: z; part -1: all three, one
+// thread); the octaves' sines and cosines come from the same double-angle
+// steps as in pair_features.
 __device__ __forceinline__ void pair_features_adjoint(const float* __restrict__ means3D,
                                                       const float* __restrict__ rx_pos, int g, int r,
-                                                      const float (&dx)[kFin], float* __restrict__ dL_dmeans3D) {
+                                                      const float (&dx)[kFin], int part,
+                                                      float* __restrict__ dL_dmeans3D) {
   const float m[3] = {means3D[3 * g], means3D[3 * g + 1], means3D[3 * g + 2]};
   const float v[3] = {m[0] - rx_pos[3 * r], m[1] - rx_pos[3 * r + 1], m[2] - rx_pos[3 * r + 2]};
   const float d2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
@@ -267,8 +319,7 @@ __device__ __forceinline__ void pair_features_adjoint(const float* __restrict__ 
   // direction u = v / d: du_i/dv_j = (delta_ij - u_i u_j) / d;  1 / d^2: d/dv = -2 v / d^4
   const float gu = dx[27] * u[0] + dx[28] * u[1] + dx[29] * u[2];
   const float ga = dx[30] * (-2.0f / (d2 * d2));
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
+  auto coord = [&](int j) {
     float gj = dx[j] + (dx[27 + j] - gu * u[j]) / d + ga * v[j];
     float s, c;
     sincosf(kPiF * m[j], &s, &c);
@@ -282,7 +333,12 @@ __device__ __forceinline__ void pair_features_adjoint(const float* __restrict__ 
       w *= 2.0f;
     }
     atomicAdd(&dL_dmeans3D[3 * g + j], gj);
+  };
+  if (part != 1) {   // part 0 (or -1: all three coordinates)
+    coord(0);
+    coord(1);
   }
+  if (part != 0) coord(2);
 }
 
 // Sum 32 per-lane values over the warp: returns, in lane j, the sum of value j.
@@ -533,6 +589,10 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                          uint32_t polls) {
   constexpr int kOutMma = out_mma_width(kOut);
   constexpr bool kBias0Cuda = bwd_bias0_on_cuda_cores(kLayers, kOut);
+  // the last step's features and feature adjoint split between a row's two
+  // threads (one output: 2.84 -> 2.66 ms at 6.4 M rows); with 64 outputs one
+  // thread per row measured faster (1.20 against 1.28 ms at 1.6 M rows)
+  constexpr bool kSplitFeatures = kOut == 1;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar_ready[kBwdGroups];
   __shared__ __align__(8) uint64_t bar_done[kBwdGroups];
@@ -791,20 +851,28 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         // after the MMAs
         uint32_t ad[kHc / 2];
         if (l == 0) {
-          // A_{-1}: the row's features (BF16), then the ones column (not for the
-          // layer whose bias is summed on the CUDA cores).  Forming them while
+          // A_{-1}: the row's features (BF16; the row's two threads split them),
+          // then the ones column (not for the layer whose bias is summed on the
+          // CUDA cores).  Forming them while
           // step 1's MMAs ran was slower (3.20 -> 3.72 ms at 6.4 M rows): the
           // features' registers beside act' spilled in the per-step code.
-          if (hf == 0) {
+          if constexpr (kSplitFeatures) {
+            int rr, g;
+            row_pair(row0, r, P, rr, g);
+            pair_features_tile(means3D, rx_pos, g, rr, vis, hf, Ab, r);
+          } else if (hf == 0) {
             int rr, g;
             row_pair(row0, r, P, rr, g);
             uint4 xp[kFin / 8];
             pair_features_bf16(means3D, rx_pos, g, rr, vis, xp);
 #pragma unroll
             for (int kc = 0; kc < kFin / 8; ++kc) *reinterpret_cast<uint4*>(Ab + slab_off(r, kc * 8)) = xp[kc];
-          } else if constexpr (!kBias0Cuda) {
-            *reinterpret_cast<uint4*>(Ab + slab_off(r, kFin)) = make_uint4(pack2(1.0f, 0.0f), 0u, 0u, 0u);
-            *reinterpret_cast<uint4*>(Ab + slab_off(r, kFin + 8)) = make_uint4(0u, 0u, 0u, 0u);
+          }
+          if constexpr (!kBias0Cuda) {
+            if (hf == 1) {
+              *reinterpret_cast<uint4*>(Ab + slab_off(r, kFin)) = make_uint4(pack2(1.0f, 0.0f), 0u, 0u, 0u);
+              *reinterpret_cast<uint4*>(Ab + slab_off(r, kFin + 8)) = make_uint4(0u, 0u, 0u, 0u);
+            }
           }
         }
         if (l > 0) {
@@ -852,8 +920,10 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
           break;
         }
         if (l == 0) {
-          if (hf == 0) {
-            // dL/dx of the row, then through the features into dL/dmeans3D
+          // dL/dx of the row, then through the features into dL/dmeans3D
+          // (with kSplitFeatures the coordinates are split between the row's
+          // two threads, else the first takes all three)
+          if (kSplitFeatures || hf == 0) {
             float v[32];
             tc::tmem_ld32(tmem + lane_base + scratch, v);
             tc::fence_before_sync();
@@ -861,7 +931,7 @@ mlp_bf16_backward_kernel(int P, size_t rows, const float* __restrict__ means3D,
             if (vis && dL_dmeans3D != nullptr) {
               int rr, g;
               row_pair(row0, r, P, rr, g);
-              pair_features_adjoint(means3D, rx_pos, g, rr, v, dL_dmeans3D);
+              pair_features_adjoint(means3D, rx_pos, g, rr, v, kSplitFeatures ? hf : -1, dL_dmeans3D);
             }
           } else {
             tc::fence_before_sync();
