@@ -405,12 +405,53 @@ class FusedTrainer:
     def step(self, views, rxs, targets):
         """Copy a batch of R receivers (device or pinned host tensors) into the
         graph's inputs and replay the captured step; returns the loss (a
-        device tensor that the next step overwrites)."""
-        self._s_views.copy_(views.reshape(self._s_views.shape), non_blocking=True)
-        self._s_rxs.copy_(rxs.reshape(self._s_rxs.shape), non_blocking=True)
-        self._s_targets.copy_(targets.reshape(self._s_targets.shape), non_blocking=True)
+        device tensor that the next step overwrites).
+
+        Host inputs are copied on a side stream into one of two staging
+        buffers, so the host-to-device transfer of this step overlaps the
+        previous step's kernels; a device-to-device copy then moves them into
+        the graph's inputs just before the replay.  As with any non-blocking
+        copy, the host tensors must stay unchanged until that copy is done
+        (one step later at most)."""
+        if views.is_cuda or rxs.is_cuda or targets.is_cuda:
+            self._s_views.copy_(views.reshape(self._s_views.shape), non_blocking=True)
+            self._s_rxs.copy_(rxs.reshape(self._s_rxs.shape), non_blocking=True)
+            self._s_targets.copy_(targets.reshape(self._s_targets.shape), non_blocking=True)
+        else:
+            self._stage_host_inputs(views, rxs, targets)
         self.graph.replay()
         return self._s_loss
+
+    def _stage_host_inputs(self, views, rxs, targets):
+        """Host inputs -> staging buffer (side stream) -> the graph's inputs
+        (current stream, after the transfer and the previous step)."""
+        if getattr(self, "_stage", None) is None:
+            inputs = (self._s_views, self._s_rxs, self._s_targets)
+            self._stage = [tuple(torch.empty_like(x) for x in inputs) for _ in range(2)]
+            self._stage_ready = [torch.cuda.Event(), torch.cuda.Event()]
+            self._stage_free = [torch.cuda.Event(), torch.cuda.Event()]
+            self._stage_used = [False, False]
+            self._stage_i = 0
+            self._copy_stream = torch.cuda.Stream(device=self._s_views.device)
+            for b in self._stage:
+                for x in b:
+                    x.record_stream(self._copy_stream)
+        k = self._stage_i
+        self._stage_i ^= 1
+        buf = self._stage[k]
+        cur = torch.cuda.current_stream(self._s_views.device)
+        cs = self._copy_stream
+        if self._stage_used[k]:
+            cs.wait_event(self._stage_free[k])   # the device copy of two steps ago has read it
+        with torch.cuda.stream(cs):
+            for dst, src in zip(buf, (views, rxs, targets)):
+                dst.copy_(src.reshape(dst.shape), non_blocking=True)
+            self._stage_ready[k].record(cs)
+        cur.wait_event(self._stage_ready[k])
+        for dst, src in zip((self._s_views, self._s_rxs, self._s_targets), buf):
+            dst.copy_(src, non_blocking=True)
+        self._stage_free[k].record(cur)
+        self._stage_used[k] = True
 
     def step_eager(self, views, rxs, tx, targets):
         """The same step without a graph (plan must exist)."""
