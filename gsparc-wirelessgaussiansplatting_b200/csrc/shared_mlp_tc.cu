@@ -72,6 +72,10 @@ __host__ __device__ constexpr uint32_t slab_off(int r, int c) {
 constexpr uint32_t kPolls = 1u << 24;
 // N of the output layer's MMA: one output is padded to the smallest N (16)
 constexpr int out_mma_width(int out) { return out < 16 ? 16 : out; }
+// The forward adds the hidden biases inside the MMAs (a K = 16 tile of ones
+// times a hi/lo BF16 split of the bias) where shared memory has room: one
+// output (the 64-output W_out takes the space).
+constexpr bool fwd_bias_in_mma(int out) { return out == 1; }
 // Adjoint TMEM plan: the weight-gradient accumulators with their ones (bias)
 // columns, dW_out^T and the 128-column dA scratch must fit 512 columns; when
 // they do not, the first layer's bias gradient is summed on the CUDA cores.
@@ -387,7 +391,11 @@ __device__ __forceinline__ void group_publish(uint32_t bar_id) {
 // k = input), then per warpgroup an activation tile H [128 x 128] K-major bf16
 // whose first 8 KB also hold the feature tile X [128 x 32]; the hidden biases
 // and the output biases in fp32; W_out K-major [kOutMma x 128] bf16 (rows past
-// the real outputs zero).
+// the real outputs zero).  With one output the hidden biases also enter the
+// MMAs: a shared K = 16 tile of ones [128 x 16] (columns 0 and 1 one) times a
+// bias tile per layer [128 x 16] (column 0 the bias rounded to BF16, column 1
+// the BF16 remainder), so the epilogue adds nothing (64 outputs leave no
+// room for the 16 KB).
 template <int kLayers, int act, int kOut>
 __global__ void __launch_bounds__(128 * kFwdGroups, 1)
 mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
@@ -395,6 +403,8 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
                         const int* __restrict__ radii, __nv_bfloat16* __restrict__ zb, float* __restrict__ S,
                         float2* __restrict__ signal, ImageHeader* __restrict__ hdr, uint32_t polls) {
   constexpr int kOutMma = out_mma_width(kOut);
+  constexpr bool kBiasMma = fwd_bias_in_mma(kOut);
+  constexpr uint32_t kSboK16 = 2u * 128u;   // [rows x 16] K-major
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar[kFwdGroups];
   __shared__ uint32_t tbase;
@@ -407,6 +417,9 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   }
   unsigned char* Hs = smem + off + (size_t)grp * kRows * kH * 2;
   off += (size_t)kFwdGroups * kRows * kH * 2;
+  unsigned char* ones = smem + off;                      // kBiasMma: [128 x 16], then the bias tiles
+  unsigned char* Bt = ones + kRows * 16 * 2;
+  if (kBiasMma) off += (size_t)kRows * 16 * 2 + (size_t)kLayers * kH * 16 * 2;
   float* bias = reinterpret_cast<float*>(smem + off);   // [kLayers][128], then b_out[kOut]
   float* bout = bias + kLayers * kH;
   off += (size_t)(kLayers * kH + kH + 4) * sizeof(float);
@@ -425,9 +438,25 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
       *reinterpret_cast<uint4*>(Ws[l] + tc::kmajor_off(n, kc * 8, kLbo, sbo)) = pack8(v);
     }
     poff += (size_t)kH * in;
-    for (int j = tid; j < kH; j += blockDim.x) bias[l * kH + j] = params[poff + j];
+    for (int j = tid; j < kH; j += blockDim.x) {
+      const float b = params[poff + j];
+      bias[l * kH + j] = b;
+      if (kBiasMma) {
+        const __nv_bfloat16 hi = __float2bfloat16_rn(b);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(b - __bfloat162float(hi));
+        unsigned char* bt = Bt + (size_t)l * kH * 16 * 2;
+        const uint32_t row2 = (uint32_t)__bfloat16_as_ushort(hi) | ((uint32_t)__bfloat16_as_ushort(lo) << 16);
+        *reinterpret_cast<uint4*>(bt + tc::kmajor_off(j, 0, kLbo, kSboK16)) = make_uint4(row2, 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(bt + tc::kmajor_off(j, 8, kLbo, kSboK16)) = make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
     poff += kH;
   }
+  if (kBiasMma)
+    for (int r = tid; r < kRows; r += blockDim.x) {
+      *reinterpret_cast<uint4*>(ones + tc::kmajor_off(r, 0, kLbo, kSboK16)) = make_uint4(pack2(1.0f, 1.0f), 0u, 0u, 0u);
+      *reinterpret_cast<uint4*>(ones + tc::kmajor_off(r, 8, kLbo, kSboK16)) = make_uint4(0u, 0u, 0u, 0u);
+    }
   for (int c = tid; c < kOutMma * (kH / 8); c += blockDim.x) {
     const int n = c / (kH / 8), kc = c % (kH / 8);
     float v[8];
@@ -497,6 +526,9 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
             tc::mma_bf16_warp(tmem, tc::smem_desc(a0 + kk * 2 * kLbo, kLbo, sbo),
                               tc::smem_desc(b0 + kk * 2 * kLbo, kLbo, sbo), idesc, kk > 0 ? 1u : 0u);
         }
+        if (kBiasMma && !out_layer)   // + 1 * b_hi + 1 * b_lo
+          tc::mma_bf16_warp(tmem, tc::smem_desc(tc::smem_u32(ones), kLbo, kSboK16),
+                            tc::smem_desc(tc::smem_u32(Bt) + (uint32_t)(l * kH * 16 * 2), kLbo, kSboK16), idesc, 1u);
         tc::commit_warp(&mbar[grp]);
       }
       const bool got = tc::mbar_wait(&mbar[grp], phase, polls);
@@ -517,12 +549,16 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
         tc::tmem_ld32(tmem + lane_base + c0, v);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const float4 b0 = *reinterpret_cast<const float4*>(bl + c0 + q * 8);
-          const float4 b1 = *reinterpret_cast<const float4*>(bl + c0 + q * 8 + 4);
-          const float2 z0 = fadd2(make_float2(v[q * 8 + 0], v[q * 8 + 1]), make_float2(b0.x, b0.y));
-          const float2 z1 = fadd2(make_float2(v[q * 8 + 2], v[q * 8 + 3]), make_float2(b0.z, b0.w));
-          const float2 z2 = fadd2(make_float2(v[q * 8 + 4], v[q * 8 + 5]), make_float2(b1.x, b1.y));
-          const float2 z3 = fadd2(make_float2(v[q * 8 + 6], v[q * 8 + 7]), make_float2(b1.z, b1.w));
+          float2 z0 = make_float2(v[q * 8 + 0], v[q * 8 + 1]), z1 = make_float2(v[q * 8 + 2], v[q * 8 + 3]);
+          float2 z2 = make_float2(v[q * 8 + 4], v[q * 8 + 5]), z3 = make_float2(v[q * 8 + 6], v[q * 8 + 7]);
+          if constexpr (!kBiasMma) {
+            const float4 b0 = *reinterpret_cast<const float4*>(bl + c0 + q * 8);
+            const float4 b1 = *reinterpret_cast<const float4*>(bl + c0 + q * 8 + 4);
+            z0 = fadd2(z0, make_float2(b0.x, b0.y));
+            z1 = fadd2(z1, make_float2(b0.z, b0.w));
+            z2 = fadd2(z2, make_float2(b1.x, b1.y));
+            z3 = fadd2(z3, make_float2(b1.z, b1.w));
+          }
           const uint4 zp = make_uint4(pack2(z0.x, z0.y), pack2(z1.x, z1.y), pack2(z2.x, z2.y), pack2(z3.x, z3.y));
           if (valid) *reinterpret_cast<uint4*>(z_out + (size_t)((c0 + q * 8) / 8) * kZChunk) = zp;
           const uint4 ap = make_uint4(act_fwd2(act, zp.x), act_fwd2(act, zp.y), act_fwd2(act, zp.z),
@@ -1070,7 +1106,8 @@ cudaError_t launch_bf16_act_table(int act, uint16_t* out, cudaStream_t s) {
 
 size_t mlp_bf16_forward_smem(int layers, int out) {
   const size_t base = (size_t)kH * kFin * 2 + (size_t)(layers - 1) * kH * kH * 2 +
-                      (size_t)kFwdGroups * kRows * kH * 2 + (size_t)(layers * kH + kH + 4) * sizeof(float);
+                      (size_t)kFwdGroups * kRows * kH * 2 + (size_t)(layers * kH + kH + 4) * sizeof(float) +
+                      (fwd_bias_in_mma(out) ? (size_t)kRows * 16 * 2 + (size_t)layers * kH * 16 * 2 : 0);
   return (base + 127) / 128 * 128 + (size_t)out_mma_width(out) * kH * 2;
 }
 size_t mlp_bf16_backward_smem(int layers, int out) {
