@@ -411,8 +411,8 @@ class FusedTrainer:
         buffers, so the host-to-device transfer of this step overlaps the
         previous step's kernels; a device-to-device copy then moves them into
         the graph's inputs just before the replay.  As with any non-blocking
-        copy, the host tensors must stay unchanged until that copy is done
-        (one step later at most)."""
+        copy, the host tensors must stay unchanged until the step has run on
+        the device (for example, until its loss has been read)."""
         if views.is_cuda or rxs.is_cuda or targets.is_cuda:
             self._s_views.copy_(views.reshape(self._s_views.shape), non_blocking=True)
             self._s_rxs.copy_(rxs.reshape(self._s_rxs.shape), non_blocking=True)
