@@ -11,8 +11,9 @@
 // Gaussian) rows, one row per thread of a 128-thread warpgroup:
 //
 //   forward:  four warpgroups per CTA, each with its own tile in flight and
-//             its own 128 TMEM columns; per layer the group's leader issues
-//             the MMA, the group runs the +bias/activation epilogue.  The
+//             its own 128 TMEM columns; per layer the group's first warp
+//             issues the MMAs (one elected lane), the group runs the
+//             +bias/activation epilogue.  The
 //             weights are staged in shared memory once per CTA; only the BF16
 //             pre-activations (for the adjoint) and the signal go to HBM.
 //   backward: two compute groups of 256 threads (two per row, 64 columns
@@ -376,7 +377,7 @@ __device__ __forceinline__ float warp_transpose_sum16(float (&v)[16], int lane) 
 }
 
 // Warpgroup-local ordering of generic shared-memory writes and TMEM reads
-// before the group's leader issues MMAs that read / overwrite them.
+// before the group's first warp issues MMAs that read / overwrite them.
 __device__ __forceinline__ void group_publish(uint32_t bar_id) {
   tc::fence_async_smem();
   tc::fence_before_sync();
@@ -593,8 +594,8 @@ mlp_bf16_forward_kernel(int P, size_t rows, const float* __restrict__ means3D,
   }
   if (!ok && t == 0) {
     if (hdr) atomic_or_error(hdr, kErrMlpWait);
-    // drain: the MMAs this group's leader committed last (the phase the group
-    // gave up on) complete before the tensor memory is freed
+    // drain: the MMAs the group's issuing lane committed last (the phase the
+    // group gave up on) complete before the tensor memory is freed
     tc::mbar_wait(&mbar[grp], phase ^ 1u, kPolls);
   }
   tc::fence_before_sync();

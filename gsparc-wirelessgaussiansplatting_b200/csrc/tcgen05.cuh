@@ -41,28 +41,11 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool a_mn, bool 
          (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
 }
 
-// D (+)= A * B^T, issued by one thread.
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t desc_a, uint64_t desc_b, uint32_t idesc,
-                                         uint32_t accumulate) {
-  const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-      :
-      : "r"(tmem_d), "l"(desc_a), "l"(desc_b), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2),
-        "r"(mask3));
-}
-
-// Arrive on an mbarrier when every MMA issued so far by this thread is done.
-__device__ __forceinline__ void commit(uint64_t* mbar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
-               : "memory");
-}
-
-// Warp-wide forms: called by all 32 lanes of a converged warp with warp-uniform
-// operands; elect.sync over the full mask picks the issuing lane, the same lane
-// every time, so a commit tracks the MMAs the same warp issued before it.
+// D (+)= A * B^T and the commit that tracks it, in warp-wide form: called by
+// all 32 lanes of a converged warp with warp-uniform operands; elect.sync over
+// the full mask picks the issuing lane, the same lane every time, so a commit
+// tracks the MMAs the same warp issued before it (tcgen05.commit covers the
+// asynchronous operations of the thread that executes it).
 // Issued from fully unrolled loops with uniform descriptors, one K = 16 MMA
 // costs about the tensor pipe's own time (M = 128: 72 cycles at N = 128, 131 at
 // N = 256, B200); from a rolled single-lane loop it cost about 160 cycles
