@@ -151,6 +151,21 @@ def test_adam_step_rejects_partial_activation_outputs():
     assert b"all three" in L.gsparc_last_error_detail()
 
 
+def test_bf16_shared_mlp_workspace_layout():
+    """The BF16 shared MLP's workspace: the sigmoid outputs [rows][out], then
+    the BF16 pre-activations of every hidden layer for whole 128-row tiles,
+    each segment rounded up to 64 floats (256 bytes); no feature-gradient
+    segment (the adjoint applies it in place)."""
+    L = _lib.lib()
+    a = lambda x: (x + 63) // 64 * 64
+    for P, R, layers, out in [(1, 1, 1, 1), (20000, 1, 3, 1), (4097, 3, 2, 1), (100000, 16, 3, 64),
+                              (200000, 32, 3, 1)]:
+        rows = P * R
+        zrows = (rows + 127) // 128 * 128
+        want = a(rows * out) + a(layers * zrows * 128 // 2)
+        assert L.gsparc_shared_mlp_workspace_floats(P, R, layers, 128, out, 1) == want, (P, R, layers, out)
+
+
 def test_static_ssim_rejects_sizes_whose_product_wraps():
     """B = CH = H = W = 65536 multiplies to 2^64, i.e. 0 in 64 bits; the
     allocation-free SSIM entry point must reject it (each factor is checked
